@@ -1,0 +1,126 @@
+// Device-side building blocks shared by the IGA kernels: PTX wrappers for the
+// bulk-copy engine (TMA, cp.async.bulk) with mbarrier completion, Ampere-style
+// cp.async for small ragged rows, bounded waits, and strip geometry.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace iga {
+
+// Upper bound on mbarrier polls before a wait gives up and reports
+// IGA_ERR_TIMEOUT; each try_wait suspends for a hardware-defined interval, so
+// this is seconds of wall time, far beyond any legitimate copy latency.
+constexpr long long kWaitLimit = 1LL << 24;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// 1-D bulk copy global -> shared through the async (TMA) proxy; completion is
+// signalled on *bar as transaction bytes. dst, src 16-byte aligned, bytes % 16 == 0.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for phase `parity` of *bar; returns false on timeout.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+{
+    for (long long it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// cp.async (LDGSTS) of 4 or 8 bytes with zero fill when `valid` is false.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void *dst, const void *src, bool valid)
+{
+    const int src_size = valid ? BYTES : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES),
+                 "r"(src_size)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// ---------------------------------------------------------------- strips
+// The element grid is cut into warp strips of 32 element columns by TY
+// element rows (nominal sizes; strips that overhang the mesh are padded with
+// empty elements). A control-point row R (or column C) is covered by the
+// strips whose element range, widened by p to the right/top, contains it:
+// strip R/TY (if it exists) and strip R/TY - 1 when R % TY < p.
+struct StripGrid {
+    int m, n;       // control points per direction
+    int nex, ney;
+    int TY;         // element rows per strip
+    int NSX, NSY;   // strips per direction
+    int P;
+    int FS;         // frame slots per strip
+};
+
+__host__ __device__ __forceinline__ int frame_size(int P, int TY) { return 2 * P * (TY + P) + 2 * P * (32 - P); }
+
+// Number of strips covering coordinate c along a direction of strip width w
+// with NS strips, and the first (lowest) of them.
+__host__ __device__ __forceinline__ int cover(int c, int w, int NS, int P, int &first)
+{
+    const int s = c / w;
+    const bool has_s = s < NS;
+    const bool has_prev = (c - s * w) < P && s >= 1 && (s - 1) < NS;
+    first = has_prev ? s - 1 : s;
+    return (int)has_s + (int)has_prev;
+}
+
+// Slot of footprint position (lr, lc) in a strip's frame (only positions that
+// can be covered by another strip: lc < P, lc >= 32, lr < P or lr >= TY).
+__host__ __device__ __forceinline__ int frame_index(int lr, int lc, int P, int TY)
+{
+    if (lc < P) return lr * P + lc;
+    if (lc >= 32) return P * (TY + P) + lr * P + (lc - 32);
+    if (lr < P) return 2 * P * (TY + P) + lr * (32 - P) + (lc - P);
+    return 2 * P * (TY + P) + P * (32 - P) + (lr - TY) * (32 - P) + (lc - P);
+}
+
+}  // namespace iga

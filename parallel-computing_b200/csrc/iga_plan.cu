@@ -1,0 +1,634 @@
+// Plans and the C ABI of the matrix-free operator (include/iga_mf.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "iga_apply.cuh"
+#include "iga_host.hpp"
+#include "iga_plan.hpp"
+
+namespace iga {
+
+// ---------------------------------------------------------------- setup kernels
+// Precomputed geometry (the mult_sf path): G = w kappa det(J) J^-1 J^-T at
+// every quadrature point, in the order apply_kernel streams it:
+// [gx][gy][s][qp][3][lane]. Padding elements get G = 0.
+template <typename T>
+__global__ void geom_setup_kernel(T *__restrict__ G, const double *__restrict__ tabX64,
+                                  const double *__restrict__ tabY64, const double *__restrict__ CP,
+                                  const double *__restrict__ qw, const double *__restrict__ kappa, StripGrid g,
+                                  int *err)
+{
+    const int P = g.P, NB = P + 1, NQ = P + 1, NQ2 = NQ * NQ;
+    const long long total = (long long)g.NSX * g.NSY * g.TY * NQ2 * 32;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int lane = (int)(t % 32);
+        long long r = t / 32;
+        const int qp = (int)(r % NQ2);
+        r /= NQ2;
+        const int s = (int)(r % g.TY);
+        r /= g.TY;
+        const int gy = (int)(r % g.NSY);
+        const int gx = (int)(r / g.NSY);
+        const int ex = 32 * gx + lane, ey = g.TY * gy + s;
+        const int qx = qp % NQ, qy = qp / NQ;
+        double g00 = 0, g01 = 0, g11 = 0;
+        if (ex < g.nex && ey < g.ney) {
+            double x_xi = 0, x_eta = 0, y_xi = 0, y_eta = 0;
+            for (int jl = 0; jl < NB; ++jl) {
+                const double n2 = tabY64[((size_t)(ey * 2 + 0) * NQ + qy) * NB + jl];
+                const double d2 = tabY64[((size_t)(ey * 2 + 1) * NQ + qy) * NB + jl];
+                for (int il = 0; il < NB; ++il) {
+                    const double n1 = tabX64[((size_t)(ex * 2 + 0) * NQ + qx) * NB + il];
+                    const double d1 = tabX64[((size_t)(ex * 2 + 1) * NQ + qx) * NB + il];
+                    const size_t A = (size_t)(ey + jl) * g.m + (ex + il);
+                    const double cx = CP[2 * A], cy = CP[2 * A + 1];
+                    x_xi += cx * d1 * n2;
+                    x_eta += cx * n1 * d2;
+                    y_xi += cy * d1 * n2;
+                    y_eta += cy * n1 * d2;
+                }
+            }
+            const double det = x_xi * y_eta - x_eta * y_xi;
+            if (!(det > 0.0)) atomicExch(err, 1 /* IGA_ERR_ARG: non-positive Jacobian */);
+            double wgt = qw[qx] * qw[qy];
+            if (kappa) wgt *= kappa[((size_t)ey * g.nex + ex) * NQ2 + qp];
+            const double f = wgt / det;
+            g00 = f * (x_eta * x_eta + y_eta * y_eta);
+            g01 = -f * (x_xi * x_eta + y_xi * y_eta);
+            g11 = f * (x_xi * x_xi + y_xi * y_xi);
+        }
+        const size_t base = ((((size_t)gx * g.NSY + gy) * g.TY + s) * NQ2 + qp) * 3 * 32 + lane;
+        G[base] = (T)g00;
+        G[base + 32] = (T)g01;
+        G[base + 64] = (T)g11;
+    }
+}
+
+__device__ double load_f(int fkind, double x, double y)
+{
+    const double pi = 3.141592653589793238462643383279;
+    if (fkind == 0) return x * (1 - x) * y * (1 - y);
+    if (fkind == 1) return 2.0 * pi * pi * sin(pi * x) * sin(pi * y);
+    const double r = sqrt(x * x + y * y), th = atan2(y, x);
+    return (pi * pi * sin(pi * r) - pi * cos(pi * r) / r + 4.0 * sin(pi * r) / (r * r)) * sin(2.0 * th);
+}
+
+// Load vector F = int R f (matrix_free/src/LocalAssemblyMF.cpp:3-29), gathered
+// per control point over its supporting elements in a fixed order (the
+// atomic-free scheme of matrix_free_gpu_dbd/src/mult.cu:233-340), F[Dir] = 0.
+__global__ void rhs_kernel(double *__restrict__ F, const double *__restrict__ tabX64,
+                           const double *__restrict__ tabY64, const double *__restrict__ CP,
+                           const double *__restrict__ qw, int fkind, StripGrid g)
+{
+    const int P = g.P, NB = P + 1, NQ = P + 1;
+    const long long N = (long long)g.m * g.n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int C = (int)(t % g.m), R = (int)(t / g.m);
+        if (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1) {
+            F[t] = 0.0;
+            continue;
+        }
+        double v = 0.0;
+        for (int ey = max(0, R - P); ey <= min(R, g.ney - 1); ++ey)
+            for (int ex = max(0, C - P); ex <= min(C, g.nex - 1); ++ex) {
+                const int il0 = C - ex, jl0 = R - ey;
+                for (int qy = 0; qy < NQ; ++qy)
+                    for (int qx = 0; qx < NQ; ++qx) {
+                        double xq = 0, yq = 0, x_xi = 0, x_eta = 0, y_xi = 0, y_eta = 0;
+                        for (int jl = 0; jl < NB; ++jl) {
+                            const double n2 = tabY64[((size_t)(ey * 2 + 0) * NQ + qy) * NB + jl];
+                            const double d2 = tabY64[((size_t)(ey * 2 + 1) * NQ + qy) * NB + jl];
+                            for (int il = 0; il < NB; ++il) {
+                                const double n1 = tabX64[((size_t)(ex * 2 + 0) * NQ + qx) * NB + il];
+                                const double d1 = tabX64[((size_t)(ex * 2 + 1) * NQ + qx) * NB + il];
+                                const size_t A = (size_t)(ey + jl) * g.m + (ex + il);
+                                const double cx = CP[2 * A], cy = CP[2 * A + 1];
+                                xq += cx * n1 * n2;
+                                yq += cy * n1 * n2;
+                                x_xi += cx * d1 * n2;
+                                x_eta += cx * n1 * d2;
+                                y_xi += cy * d1 * n2;
+                                y_eta += cy * n1 * d2;
+                            }
+                        }
+                        const double det = x_xi * y_eta - x_eta * y_xi;
+                        const double Ra = tabX64[((size_t)(ex * 2) * NQ + qx) * NB + il0] *
+                                          tabY64[((size_t)(ey * 2) * NQ + qy) * NB + jl0];
+                        v += Ra * load_f(fkind, xq, yq) * qw[qx] * qw[qy] * det;
+                    }
+            }
+        F[t] = v;
+    }
+}
+
+// ---------------------------------------------------------------- helpers
+#define IGA_CUDA_TRY(call)                                  \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) {                            \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+            return e_ == cudaErrorMemoryAllocation ? IGA_ERR_NOMEM : IGA_ERR_CUDA; \
+        }                                                   \
+    } while (0)
+
+static thread_local std::string g_last_error;
+void set_error(const std::string &s) { g_last_error = s; }
+const std::string &last_error() { return g_last_error; }
+
+template <typename T>
+static int upload(T **dst, const void *src, size_t bytes)
+{
+    IGA_CUDA_TRY(cudaMalloc((void **)dst, std::max<size_t>(bytes, 16)));
+    if (src && bytes) IGA_CUDA_TRY(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    return IGA_OK;
+}
+
+static int nst_for(int prec) { return prec == IGA_FP64 ? 2 : 3; }
+
+template <int P, typename T>
+static size_t smem_for(int W, int NST)
+{
+    return NST == 2 ? apply_smem_bytes<P, T, 2>(W) : apply_smem_bytes<P, T, 3>(W);
+}
+
+template <typename T>
+static size_t smem_dispatch(int P, int W, int NST)
+{
+    switch (P) {
+    case 1: return smem_for<1, T>(W, NST);
+    case 2: return smem_for<2, T>(W, NST);
+    case 3: return smem_for<3, T>(W, NST);
+    case 4: return smem_for<4, T>(W, NST);
+    default: return smem_for<5, T>(W, NST);
+    }
+}
+
+static constexpr size_t kSmemBudget = 220 * 1024;
+
+// Warps per CTA: as many as fit in shared memory, at most 8.
+static int warps_for(int P, int prec)
+{
+    const int NST = nst_for(prec);
+    for (int W = 8; W >= 1; --W) {
+        const size_t b = prec == IGA_FP64 ? smem_dispatch<double>(P, W, NST) : smem_dispatch<float>(P, W, NST);
+        if (b <= kSmemBudget) return W;
+    }
+    return 1;
+}
+
+// Rows per strip: the candidate whose CTA count fills the SMs best, with a
+// small penalty on short strips (more seam traffic).
+static int rows_for(int nex, int ney, int W, int nsm)
+{
+    const int NSX = (nex + 31) / 32;
+    int best = 64;
+    double best_cost = 1e300;
+    for (int TY : {64, 48, 32, 24, 16}) {
+        const int NSY = (ney + TY - 1) / TY;
+        const long long ctas = (long long)NSX * ((NSY + W - 1) / W);
+        const long long waves = (ctas + nsm - 1) / nsm;
+        const double work = (double)waves * W * (TY + 2.0);   // per-SM time in strip-row units
+        const double cost = work * (1.0 + 0.5 * 3.0 / TY);
+        if (cost < best_cost - 1e-9) {
+            best_cost = cost;
+            best = TY;
+        }
+    }
+    return best;
+}
+
+}  // namespace iga
+
+using namespace iga;
+
+// ---------------------------------------------------------------- plan
+template <typename T>
+static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const Tables1D &tx, const Tables1D &ty)
+{
+    const int p = P.p, NB = p + 1, NQ = p + 1, NQ2 = NQ * NQ;
+    const StripGrid &g = pl->grid;
+    // x tables regrouped per column strip: [gx][kind][qx][il][lane]
+    std::vector<T> hx((size_t)g.NSX * 2 * NQ * NB * 32, T(0));
+    for (int gx = 0; gx < g.NSX; ++gx)
+        for (int kind = 0; kind < 2; ++kind)
+            for (int qx = 0; qx < NQ; ++qx)
+                for (int il = 0; il < NB; ++il)
+                    for (int lane = 0; lane < 32; ++lane) {
+                        const int ex = 32 * gx + lane;
+                        double v = 0.0;
+                        if (ex < P.nex) v = (kind ? tx.der : tx.val)[((size_t)ex * NQ + qx) * NB + il];
+                        hx[((((size_t)gx * 2 + kind) * NQ + qx) * NB + il) * 32 + lane] = (T)v;
+                    }
+    std::vector<T> hy((size_t)P.ney * 2 * NQ * NB);
+    for (int ey = 0; ey < P.ney; ++ey)
+        for (int kind = 0; kind < 2; ++kind)
+            for (int k = 0; k < NQ * NB; ++k)
+                hy[((size_t)ey * 2 + kind) * NQ * NB + k] = (T)(kind ? ty.der : ty.val)[(size_t)ey * NQ * NB + k];
+    int st;
+    if ((st = upload((T **)&op.tabX, hx.data(), hx.size() * sizeof(T)))) return st;
+    if ((st = upload((T **)&op.tabY, hy.data(), hy.size() * sizeof(T)))) return st;
+    std::vector<T> hw(NQ2);
+    std::vector<double> qx(NQ), qw(NQ);
+    gauss01(NQ, qx.data(), qw.data());
+    for (int a = 0; a < NQ; ++a)
+        for (int b = 0; b < NQ; ++b) hw[a * NQ + b] = (T)(qw[a] * qw[b]);
+    if ((st = upload((T **)&op.wq, hw.data(), hw.size() * sizeof(T)))) return st;
+    if (!P.kappa.empty() && pl->geometry == IGA_GEOM_ON_THE_FLY) {
+        std::vector<T> hk(P.kappa.begin(), P.kappa.end());
+        if ((st = upload((T **)&op.kappa, hk.data(), hk.size() * sizeof(T)))) return st;
+    }
+    size_t fbytes = (size_t)g.NSX * g.NSY * g.FS * sizeof(T);
+    if ((st = upload((T **)&op.frame, nullptr, fbytes))) return st;
+    if (pl->geometry == IGA_GEOM_PRECOMPUTED) {
+        const size_t gelems = (size_t)g.NSX * g.NSY * g.TY * NQ2 * 3 * 32;
+        op.geom_bytes = gelems * sizeof(T);
+        if ((st = upload((T **)&op.G, nullptr, op.geom_bytes))) return st;
+        double *kap = nullptr;
+        if (!P.kappa.empty())
+            if ((st = upload(&kap, P.kappa.data(), P.kappa.size() * sizeof(double)))) return st;
+        geom_setup_kernel<T><<<1184, 256>>>((T *)op.G, pl->tabX64, pl->tabY64, pl->CP, pl->qw, kap, g, pl->d_err);
+        cudaError_t e = cudaDeviceSynchronize();
+        if (kap) cudaFree(kap);
+        if (e != cudaSuccess) {
+            set_error(std::string("geometry setup: ") + cudaGetErrorString(e));
+            return IGA_ERR_CUDA;
+        }
+    }
+    op.ready = true;
+    return IGA_OK;
+}
+
+template <int P, typename T, int GEOM, int NST>
+static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s)
+{
+    ApplyParams<T> a;
+    a.x = x;
+    a.y = y;
+    a.G = (const T *)op.G;
+    a.tabX = (const T *)op.tabX;
+    a.tabY = (const T *)op.tabY;
+    a.CP = pl->CP;
+    a.wq = (const T *)op.wq;
+    a.kappa = (const T *)op.kappa;
+    a.frame = (T *)op.frame;
+    a.g = pl->grid;
+    a.sign = (T)pl->sign;
+    a.bc = pl->bc;
+    a.err = pl->d_err;
+    const int W = op.warps;
+    const size_t smem = apply_smem_bytes<P, T, NST>(W);
+    auto kern = apply_kernel<P, T, GEOM, NST>;
+    static bool attr_set = false;   // per template instance
+    if (!attr_set) {
+        IGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    dim3 grid(pl->grid.NSX, (pl->grid.NSY + W - 1) / W), block(32, W);
+    kern<<<grid, block, smem, s>>>(a);
+    const StripGrid &g = pl->grid;
+    const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
+    if (nseam > 0) {
+        const int blocks = (int)std::min<long long>((nseam + 255) / 256, 4 * 148);
+        seam_fixup_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)pl->sign, pl->bc);
+    }
+    IGA_CUDA_TRY(cudaGetLastError());
+    return IGA_OK;
+}
+
+template <int P, typename T>
+static int launch_apply_p(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s)
+{
+    constexpr int NST = sizeof(T) == 8 ? 2 : 3;
+    if (pl->geometry == IGA_GEOM_PRECOMPUTED) return launch_apply_t<P, T, 0, NST>(pl, op, x, y, s);
+    return launch_apply_t<P, T, 1, NST>(pl, op, x, y, s);
+}
+
+template <typename T>
+static int launch_apply(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s)
+{
+    switch (pl->p) {
+    case 1: return launch_apply_p<1, T>(pl, op, x, y, s);
+    case 2: return launch_apply_p<2, T>(pl, op, x, y, s);
+    case 3: return launch_apply_p<3, T>(pl, op, x, y, s);
+    case 4: return launch_apply_p<4, T>(pl, op, x, y, s);
+    case 5: return launch_apply_p<5, T>(pl, op, x, y, s);
+    default: return IGA_ERR_UNSUPPORTED;
+    }
+}
+
+int iga_apply_internal(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s)
+{
+    if (prec == IGA_FP64) {
+        if (!pl->op64.ready) return IGA_ERR_ARG;
+        return launch_apply<double>(pl, pl->op64, (const double *)x, (double *)y, s);
+    }
+    if (!pl->op32.ready) return IGA_ERR_ARG;
+    return launch_apply<float>(pl, pl->op32, (const float *)x, (float *)y, s);
+}
+
+int iga_check_error_flag(iga_plan *pl)
+{
+    int h = 0;
+    IGA_CUDA_TRY(cudaMemcpy(&h, pl->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        cudaMemset(pl->d_err, 0, sizeof(int));
+        return h;
+    }
+    return IGA_OK;
+}
+
+static void free_op(OperatorData &op)
+{
+    for (void *p : {op.tabX, op.tabY, op.G, op.frame, op.wq, op.kappa})
+        if (p) cudaFree(p);
+    op = OperatorData{};
+}
+
+extern "C" {
+
+void iga_opts_default(iga_opts *o)
+{
+    if (!o) return;
+    o->precision = IGA_FP64;
+    o->geometry = IGA_GEOM_PRECOMPUTED;
+    o->sign = IGA_SIGN_REFERENCE;
+    o->bc = IGA_BC_REFERENCE;
+    o->device = 0;
+    o->rows_per_strip = 0;
+}
+
+const char *iga_status_str(int s)
+{
+    switch (s) {
+    case IGA_OK: return "ok";
+    case IGA_ERR_ARG: return "invalid argument";
+    case IGA_ERR_UNSUPPORTED: return "unsupported input";
+    case IGA_ERR_CUDA: return "CUDA error";
+    case IGA_ERR_NOMEM: return "out of device memory";
+    case IGA_ERR_NOT_CONVERGED: return "not converged";
+    case IGA_ERR_BREAKDOWN: return "Krylov breakdown";
+    case IGA_ERR_NONFINITE: return "non-finite value";
+    case IGA_ERR_TIMEOUT: return "bounded device wait timed out";
+    default: return "unknown status";
+    }
+}
+
+const char *iga_last_error(void) { return last_error().c_str(); }
+
+int iga_mesh_unit_square(int p, int nex, int ney, double Lx, double Ly, double *CP, double *C1, double *C2)
+{
+    if (p < 1 || p > 8 || nex < 1 || ney < 1 || !CP || !C1 || !C2 || !(Lx > 0) || !(Ly > 0)) return IGA_ERR_ARG;
+    const std::vector<double> S = open_knots(p, nex, Lx), T = open_knots(p, ney, Ly);
+    const std::vector<double> gx = greville(p, S), gy = greville(p, T);
+    const std::vector<double> c1 = extraction(p, S), c2 = extraction(p, T);
+    const int m = nex + p, n = ney + p;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) {
+            CP[2 * ((size_t)j * m + i)] = gx[i];
+            CP[2 * ((size_t)j * m + i) + 1] = gy[j];
+        }
+    std::memcpy(C1, c1.data(), c1.size() * sizeof(double));
+    std::memcpy(C2, c2.data(), c2.size() * sizeof(double));
+    return IGA_OK;
+}
+
+int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **out)
+{
+    if (!d || !out) return IGA_ERR_ARG;
+    *out = nullptr;
+    iga_opts opts;
+    iga_opts_default(&opts);
+    if (opts_in) opts = *opts_in;
+    if (opts.precision < IGA_FP64 || opts.precision > IGA_MIXED) return IGA_ERR_ARG;
+    if (opts.geometry != IGA_GEOM_PRECOMPUTED && opts.geometry != IGA_GEOM_ON_THE_FLY) return IGA_ERR_ARG;
+    if (opts.sign != IGA_SIGN_REFERENCE && opts.sign != IGA_SIGN_SPD) return IGA_ERR_ARG;
+    if (opts.bc != IGA_BC_REFERENCE && opts.bc != IGA_BC_IDENTITY) return IGA_ERR_ARG;
+    Patch P;
+    MeshDescView v{d->p, d->q, d->nElemX, d->nElemY, d->CP, d->weights, d->C1, d->C2, d->IEN, d->ID, d->Dir,
+                   d->nDir, d->kappa};
+    std::string err = build_patch(v, P);
+    if (!err.empty()) {
+        set_error(err);
+        return (err.find("requires") != std::string::npos || err.find("must be in") != std::string::npos)
+                   ? IGA_ERR_UNSUPPORTED
+                   : IGA_ERR_ARG;
+    }
+    IGA_CUDA_TRY(cudaSetDevice(opts.device));
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opts.device);
+
+    iga_plan *pl = new iga_plan();
+    pl->p = P.p;
+    pl->nex = P.nex;
+    pl->ney = P.ney;
+    pl->m = P.m;
+    pl->n = P.n;
+    pl->nfunc = (long long)P.m * P.n;
+    pl->precision = opts.precision;
+    pl->geometry = opts.geometry;
+    pl->sign = opts.sign;
+    pl->bc = opts.bc;
+    pl->device = opts.device;
+    pl->patch = P;
+    const int Wmin = std::min(opts.precision == IGA_FP32 ? 8 : warps_for(P.p, IGA_FP64), warps_for(P.p, IGA_FP32));
+    const int TY = opts.rows_per_strip > 0 ? opts.rows_per_strip : rows_for(P.nex, P.ney, Wmin, nsm);
+    if (TY < P.p || TY > 1024) {
+        delete pl;
+        set_error("rows_per_strip must be in [p, 1024]");
+        return IGA_ERR_ARG;
+    }
+    StripGrid &g = pl->grid;
+    g.m = P.m;
+    g.n = P.n;
+    g.nex = P.nex;
+    g.ney = P.ney;
+    g.TY = TY;
+    g.NSX = (P.nex + 31) / 32;
+    g.NSY = (P.ney + TY - 1) / TY;
+    g.P = P.p;
+    g.FS = frame_size(P.p, TY);
+
+    int st = IGA_OK;
+    auto fail = [&](int code) {
+        iga_plan_destroy(pl);
+        return code;
+    };
+    const Tables1D tx = tables_1d(P.p, P.nex, P.C1.data(), P.w1.empty() ? nullptr : P.w1.data());
+    const Tables1D ty = tables_1d(P.q, P.ney, P.C2.data(), P.w2.empty() ? nullptr : P.w2.data());
+    {
+        const int NB = P.p + 1, NQ = NB;
+        std::vector<double> h64x((size_t)P.nex * 2 * NQ * NB), h64y((size_t)P.ney * 2 * NQ * NB);
+        for (int e = 0; e < P.nex; ++e)
+            for (int k = 0; k < NQ * NB; ++k) {
+                h64x[((size_t)e * 2 + 0) * NQ * NB + k] = tx.val[(size_t)e * NQ * NB + k];
+                h64x[((size_t)e * 2 + 1) * NQ * NB + k] = tx.der[(size_t)e * NQ * NB + k];
+            }
+        for (int e = 0; e < P.ney; ++e)
+            for (int k = 0; k < NQ * NB; ++k) {
+                h64y[((size_t)e * 2 + 0) * NQ * NB + k] = ty.val[(size_t)e * NQ * NB + k];
+                h64y[((size_t)e * 2 + 1) * NQ * NB + k] = ty.der[(size_t)e * NQ * NB + k];
+            }
+        std::vector<double> qx(NQ), qw(NQ);
+        gauss01(NQ, qx.data(), qw.data());
+        if ((st = upload(&pl->tabX64, h64x.data(), h64x.size() * 8))) return fail(st);
+        if ((st = upload(&pl->tabY64, h64y.data(), h64y.size() * 8))) return fail(st);
+        if ((st = upload(&pl->CP, P.CP.data(), P.CP.size() * 8))) return fail(st);
+        if ((st = upload(&pl->qw, qw.data(), qw.size() * 8))) return fail(st);
+        if ((st = upload(&pl->d_err, nullptr, sizeof(int)))) return fail(st);
+        cudaMemset(pl->d_err, 0, sizeof(int));
+    }
+    if (opts.precision != IGA_FP32) {
+        pl->op64.warps = warps_for(P.p, IGA_FP64);
+        if ((st = build_operator<double>(pl, pl->op64, P, tx, ty))) return fail(st);
+    }
+    if (opts.precision != IGA_FP64) {
+        pl->op32.warps = warps_for(P.p, IGA_FP32);
+        if ((st = build_operator<float>(pl, pl->op32, P, tx, ty))) return fail(st);
+    }
+    int herr = 0;
+    cudaMemcpy(&herr, pl->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (herr) {
+        set_error("geometry has a non-positive Jacobian determinant");
+        return fail(IGA_ERR_ARG);
+    }
+    *out = pl;
+    return IGA_OK;
+}
+
+int iga_plan_destroy(iga_plan *pl)
+{
+    if (!pl) return IGA_OK;
+    cudaSetDevice(pl->device);
+    cudaDeviceSynchronize();
+    free_op(pl->op64);
+    free_op(pl->op32);
+    for (void *p : {(void *)pl->tabX64, (void *)pl->tabY64, (void *)pl->CP, (void *)pl->qw, (void *)pl->d_err,
+                    (void *)pl->h_stage_x, (void *)pl->d_stage_x, (void *)pl->d_stage_y})
+        if (p) cudaFree(p);
+    if (pl->h_pinned) cudaFreeHost(pl->h_pinned);
+    iga_solver_release(pl);
+    delete pl;
+    return IGA_OK;
+}
+
+int iga_plan_get_info(const iga_plan *pl, iga_plan_info *info)
+{
+    if (!pl || !info) return IGA_ERR_ARG;
+    info->nfunc = pl->nfunc;
+    info->nelem = (long long)pl->nex * pl->ney;
+    const int NQ2 = (pl->p + 1) * (pl->p + 1);
+    info->geom_bytes = pl->op64.ready ? pl->op64.geom_bytes : pl->op32.geom_bytes;
+    // Algorithmic bytes: read x, write y, plus geometry (3 values per
+    // quadrature point precomputed, or control points + 1-D tables on the fly).
+    for (int k = 0; k < 2; ++k) {
+        const long long s = k == 0 ? 8 : 4;
+        long long b = 2 * s * pl->nfunc;
+        if (pl->geometry == IGA_GEOM_PRECOMPUTED) b += 3 * s * NQ2 * info->nelem;
+        else b += 16LL * pl->nfunc + 8LL * 2 * NQ2 * (pl->nex + pl->ney);
+        (k == 0 ? info->algo_bytes_f64 : info->algo_bytes_f32) = b;
+    }
+    info->rows_per_strip = pl->grid.TY;
+    info->warps_per_cta = pl->op64.ready ? pl->op64.warps : pl->op32.warps;
+    return IGA_OK;
+}
+
+int iga_apply(iga_plan *pl, const void *x, void *y, void *stream)
+{
+    if (!pl || !x || !y) return IGA_ERR_ARG;
+    return iga_apply_internal(pl, pl->precision == IGA_FP32 ? IGA_FP32 : IGA_FP64, x, y, (cudaStream_t)stream);
+}
+
+int iga_apply_prec(iga_plan *pl, int prec, const void *x, void *y, void *stream)
+{
+    if (!pl || !x || !y || (prec != IGA_FP64 && prec != IGA_FP32)) return IGA_ERR_ARG;
+    return iga_apply_internal(pl, prec, x, y, (cudaStream_t)stream);
+}
+
+int iga_apply_host(iga_plan *pl, const double *xh, double *yh)
+{
+    if (!pl || !xh || !yh || !pl->op64.ready) return IGA_ERR_ARG;
+    const size_t bytes = (size_t)pl->nfunc * sizeof(double);
+    IGA_CUDA_TRY(cudaSetDevice(pl->device));
+    if (!pl->d_stage_x) {
+        IGA_CUDA_TRY(cudaMalloc((void **)&pl->d_stage_x, bytes));
+        IGA_CUDA_TRY(cudaMalloc((void **)&pl->d_stage_y, bytes));
+    }
+    IGA_CUDA_TRY(cudaMemcpyAsync(pl->d_stage_x, xh, bytes, cudaMemcpyHostToDevice, 0));
+    int st = iga_apply_internal(pl, IGA_FP64, pl->d_stage_x, pl->d_stage_y, 0);
+    if (st) return st;
+    IGA_CUDA_TRY(cudaMemcpyAsync(yh, pl->d_stage_y, bytes, cudaMemcpyDeviceToHost, 0));
+    IGA_CUDA_TRY(cudaStreamSynchronize(0));
+    return iga_check_error_flag(pl);
+}
+
+int iga_rhs(iga_plan *pl, int fkind, double *F, void *stream)
+{
+    if (!pl || !F || fkind < 0 || fkind > 2) return IGA_ERR_ARG;
+    rhs_kernel<<<2 * 148, 256, 0, (cudaStream_t)stream>>>(F, pl->tabX64, pl->tabY64, pl->CP, pl->qw, fkind,
+                                                         pl->grid);
+    IGA_CUDA_TRY(cudaGetLastError());
+    return IGA_OK;
+}
+
+// ------------------------------------------------- reference-shaped entry point
+namespace {
+struct CachedPlan {
+    iga_plan *plan;
+};
+std::mutex g_cache_mu;
+std::map<std::tuple<int, int, int, int, const void *, const void *, const void *>, CachedPlan> g_cache;
+}  // namespace
+
+int iga_MatrixFreeMatMultCUDA(int p, int q, int nex, int ney, const double *, const double *, const double *,
+                              const double *, const double *d_C1, const double *d_C2, const double *,
+                              const double *, const int *, const int *, const double *d_CP, const double *,
+                              const double *, const double *d_in, double *d_out)
+{
+    if (!d_C1 || !d_C2 || !d_CP || !d_in || !d_out || nex < 1 || ney < 1) return IGA_ERR_ARG;
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    auto key = std::make_tuple(p, q, nex, ney, (const void *)d_CP, (const void *)d_C1, (const void *)d_C2);
+    auto it = g_cache.find(key);
+    if (it == g_cache.end()) {
+        const long long nf = (long long)(nex + p) * (ney + q);
+        std::vector<double> CP(2 * nf), C1((size_t)nex * (p + 1) * (p + 1)), C2((size_t)ney * (q + 1) * (q + 1));
+        IGA_CUDA_TRY(cudaMemcpy(CP.data(), d_CP, CP.size() * 8, cudaMemcpyDeviceToHost));
+        IGA_CUDA_TRY(cudaMemcpy(C1.data(), d_C1, C1.size() * 8, cudaMemcpyDeviceToHost));
+        IGA_CUDA_TRY(cudaMemcpy(C2.data(), d_C2, C2.size() * 8, cudaMemcpyDeviceToHost));
+        iga_mesh_desc d{};
+        d.p = p;
+        d.q = q;
+        d.nElemX = nex;
+        d.nElemY = ney;
+        d.CP = CP.data();
+        d.C1 = C1.data();
+        d.C2 = C2.data();
+        iga_opts o;
+        iga_opts_default(&o);
+        cudaGetDevice(&o.device);
+        o.geometry = IGA_GEOM_ON_THE_FLY;   // the reference kernel recomputes geometry too
+        iga_plan *pl = nullptr;
+        const int st = iga_plan_create(&d, &o, &pl);
+        if (st) return st;
+        it = g_cache.emplace(key, CachedPlan{pl}).first;
+    }
+    return iga_apply_internal(it->second.plan, IGA_FP64, d_in, d_out, 0);
+}
+
+int iga_MatrixFreeMatMultCUDA_release(void)
+{
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (auto &kv : g_cache) iga_plan_destroy(kv.second.plan);
+    g_cache.clear();
+    return IGA_OK;
+}
+
+}  // extern "C"

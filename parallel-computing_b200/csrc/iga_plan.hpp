@@ -1,0 +1,50 @@
+// Internal plan layout shared by the operator and solver translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/iga_mf.h"
+#include "iga_device.cuh"
+#include "iga_host.hpp"
+
+namespace iga {
+
+// Device data of one operator precision.
+struct OperatorData {
+    bool ready = false;
+    int warps = 8;
+    void *tabX = nullptr;   // [NSX][2][NQ][NB][32]
+    void *tabY = nullptr;   // [ney][2][NQ][NB]
+    void *G = nullptr;      // precomputed geometry (may be null)
+    void *frame = nullptr;  // seam frames
+    void *wq = nullptr;     // [NQ*NQ] quadrature weight products
+    void *kappa = nullptr;  // on-the-fly coefficient
+    size_t geom_bytes = 0;
+};
+
+struct SolverState;   // defined by the solver translation unit
+
+void set_error(const std::string &s);
+const std::string &last_error();
+
+}  // namespace iga
+
+struct iga_plan {
+    int p = 0, nex = 0, ney = 0, m = 0, n = 0;
+    long long nfunc = 0;
+    int precision = IGA_FP64, geometry = IGA_GEOM_PRECOMPUTED, sign = IGA_SIGN_REFERENCE, bc = IGA_BC_REFERENCE;
+    int device = 0;
+    iga::StripGrid grid{};
+    iga::Patch patch;
+    iga::OperatorData op64, op32;
+    double *tabX64 = nullptr, *tabY64 = nullptr, *CP = nullptr, *qw = nullptr;
+    int *d_err = nullptr;
+    double *h_stage_x = nullptr, *d_stage_x = nullptr, *d_stage_y = nullptr;
+    void *h_pinned = nullptr;
+    iga::SolverState *solver = nullptr;
+};
+
+int iga_apply_internal(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s);
+int iga_check_error_flag(iga_plan *pl);
+void iga_solver_release(iga_plan *pl);

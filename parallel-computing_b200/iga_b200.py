@@ -1,0 +1,199 @@
+"""Python binding (ctypes) of the C ABI in include/iga_mf.h and include/iga_solve.h.
+
+A thin layer for tests, the benchmark and Python users: it loads the in-tree
+libiga_b200.so (built by `make -C parallel-computing_b200`) and fails loudly if
+it is missing. There is no fallback path: every operator call runs the CUDA
+kernels of that library.
+
+Device arrays are passed as torch CUDA tensors (or raw integer pointers);
+torch is used only for device memory and streams.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libiga_b200.so")
+VP = ctypes.c_void_p
+
+IGA_OK = 0
+FP64, FP32, MIXED = 0, 1, 2
+GEOM_PRECOMPUTED, GEOM_ON_THE_FLY = 0, 1
+SIGN_REFERENCE, SIGN_SPD = -1, 1
+BC_REFERENCE, BC_IDENTITY = 0, 1
+F_REFERENCE, F_SINSIN, F_ANNULUS = 0, 1, 2
+
+
+class IgaError(RuntimeError):
+    def __init__(self, status, what):
+        self.status = status
+        super().__init__(f"{what}: {_lib().iga_status_str(status).decode()} ({status}): "
+                         f"{_lib().iga_last_error().decode()}")
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_int), ("q", ctypes.c_int), ("nElemX", ctypes.c_int), ("nElemY", ctypes.c_int),
+                ("CP", VP), ("weights", VP), ("C1", VP), ("C2", VP), ("h1", VP), ("h2", VP),
+                ("IEN", VP), ("ID", VP), ("Dir", VP), ("nDir", ctypes.c_int), ("kappa", VP)]
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("geometry", ctypes.c_int), ("sign", ctypes.c_int),
+                ("bc", ctypes.c_int), ("device", ctypes.c_int), ("rows_per_strip", ctypes.c_int)]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [("nfunc", ctypes.c_int64), ("nelem", ctypes.c_int64), ("geom_bytes", ctypes.c_int64),
+                ("algo_bytes_f64", ctypes.c_int64), ("algo_bytes_f32", ctypes.c_int64),
+                ("rows_per_strip", ctypes.c_int), ("warps_per_cta", ctypes.c_int)]
+
+
+_LIB = None
+
+# (name, restype, argtypes) of every exported C entry point.
+SIGNATURES = [
+    ("iga_status_str", ctypes.c_char_p, [ctypes.c_int]),
+    ("iga_last_error", ctypes.c_char_p, []),
+    ("iga_opts_default", None, [ctypes.POINTER(Opts)]),
+    ("iga_mesh_unit_square", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, VP, VP, VP]),
+    ("iga_plan_create", ctypes.c_int, [ctypes.POINTER(MeshDesc), ctypes.POINTER(Opts), ctypes.POINTER(VP)]),
+    ("iga_plan_destroy", ctypes.c_int, [VP]),
+    ("iga_plan_get_info", ctypes.c_int, [VP, ctypes.POINTER(PlanInfo)]),
+    ("iga_apply", ctypes.c_int, [VP, VP, VP, VP]),
+    ("iga_apply_prec", ctypes.c_int, [VP, ctypes.c_int, VP, VP, VP]),
+    ("iga_apply_host", ctypes.c_int, [VP, VP, VP]),
+    ("iga_rhs", ctypes.c_int, [VP, ctypes.c_int, VP, VP]),
+    ("iga_MatrixFreeMatMultCUDA", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 15),
+    ("iga_MatrixFreeMatMultCUDA_release", ctypes.c_int, []),
+]
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIBPATH):
+            raise RuntimeError(f"{LIBPATH} is missing: build it with `make -C {HERE}` "
+                               "(there is no CPU fallback for the operator)")
+        L = ctypes.CDLL(LIBPATH)
+        for name, res, args in SIGNATURES:
+            if hasattr(L, name):
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def lib():
+    return _lib()
+
+
+def _check(status, what):
+    if status != IGA_OK:
+        raise IgaError(status, what)
+
+
+def _ptr(a):
+    """Device/host pointer of a torch tensor, numpy array or int."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def unit_square(p, nex, ney=None, Lx=1.0, Ly=1.0):
+    """Patch arrays of the reference preprocessor (host numpy): dict(p, q, nex, ney, CP, C1, C2)."""
+    ney = nex if ney is None else ney
+    m, n = nex + p, ney + p
+    CP = np.empty(2 * m * n)
+    C1 = np.empty(nex * (p + 1) ** 2)
+    C2 = np.empty(ney * (p + 1) ** 2)
+    _check(_lib().iga_mesh_unit_square(p, nex, ney, Lx, Ly, _ptr(CP), _ptr(C1), _ptr(C2)),
+           "iga_mesh_unit_square")
+    return dict(p=p, q=p, nex=nex, ney=ney, CP=CP, C1=C1, C2=C2, W=None, kappa=None,
+                h1=np.full(nex, Lx / nex), h2=np.full(ney, Ly / ney))
+
+
+class Plan:
+    """Owns an iga_plan (device tables, precomputed geometry)."""
+
+    def __init__(self, mesh, precision=FP64, geometry=GEOM_PRECOMPUTED, sign=SIGN_REFERENCE,
+                 bc=BC_REFERENCE, device=0, rows_per_strip=0, IEN=None, ID=None, Dir=None):
+        L = _lib()
+        self._keep = []
+
+        def arr(v, dt=np.float64):
+            if v is None:
+                return None
+            a = np.ascontiguousarray(v, dtype=dt)
+            self._keep.append(a)
+            return a.ctypes.data
+
+        d = MeshDesc()
+        d.p, d.q, d.nElemX, d.nElemY = mesh["p"], mesh.get("q", mesh["p"]), mesh["nex"], mesh["ney"]
+        d.CP = arr(mesh["CP"])
+        d.weights = arr(mesh.get("W"))
+        d.C1 = arr(mesh.get("C1"))
+        d.C2 = arr(mesh.get("C2"))
+        d.h1 = arr(mesh.get("h1"))
+        d.h2 = arr(mesh.get("h2"))
+        d.IEN = arr(IEN, np.int32)
+        d.ID = arr(ID, np.int32)
+        d.Dir = arr(Dir, np.int32)
+        d.nDir = 0 if Dir is None else len(Dir)
+        d.kappa = arr(mesh.get("kappa"))
+        o = Opts()
+        L.iga_opts_default(ctypes.byref(o))
+        o.precision, o.geometry, o.sign, o.bc, o.device, o.rows_per_strip = (
+            precision, geometry, sign, bc, device, rows_per_strip)
+        h = VP()
+        _check(L.iga_plan_create(ctypes.byref(d), ctypes.byref(o), ctypes.byref(h)), "iga_plan_create")
+        self.h = h
+        self._keep = []
+        self.mesh = mesh
+        self.precision = precision
+        info = PlanInfo()
+        _check(L.iga_plan_get_info(h, ctypes.byref(info)), "iga_plan_get_info")
+        self.info = info
+        self.nfunc = info.nfunc
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().iga_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def apply(self, x, y, stream=None, precision=None):
+        if precision is None:
+            _check(_lib().iga_apply(self.h, _ptr(x), _ptr(y), _stream(stream)), "iga_apply")
+        else:
+            _check(_lib().iga_apply_prec(self.h, precision, _ptr(x), _ptr(y), _stream(stream)), "iga_apply_prec")
+
+    def apply_host(self, x, y=None):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if y is None:
+            y = np.empty_like(x)
+        _check(_lib().iga_apply_host(self.h, _ptr(x), _ptr(y)), "iga_apply_host")
+        return y
+
+    def rhs(self, F, fkind=F_REFERENCE, stream=None):
+        _check(_lib().iga_rhs(self.h, fkind, _ptr(F), _stream(stream)), "iga_rhs")
+        return F

@@ -205,3 +205,51 @@ def golden_mesh(g, name):
     p, q, nex, ney = (int(v) for v in g[f"{name}_dims"])
     return dict(p=p, q=q, nex=nex, ney=ney, CP=g[f"{name}_CP"], C1=g[f"{name}_C1"], C2=g[f"{name}_C2"],
                 h1=g[f"{name}_h1"], h2=g[f"{name}_h2"], W=None, kappa=None)
+
+
+def load_binding():
+    import sys
+    pkg = os.path.join(ROOT, "parallel-computing_b200")
+    if pkg not in sys.path:
+        sys.path.insert(0, pkg)
+    import iga_b200
+    return iga_b200
+
+
+def distorted(mesh, ax=0.01, ay=0.02):
+    """Smoothly distorted copy of a unit-square patch (non-affine geometry)."""
+    p, nex, ney = mesh["p"], mesh["nex"], mesh["ney"]
+    m, n = nex + p, ney + mesh.get("q", p)
+    cp = np.asarray(mesh["CP"]).reshape(n, m, 2).copy()
+    x0, y0 = cp[..., 0].copy(), cp[..., 1].copy()
+    cp[..., 0] = x0 + ax * np.sin(3 * y0) * x0 * (1 - x0)
+    cp[..., 1] = y0 + ay * np.sin(2 * x0) * y0 * (1 - y0)
+    out = dict(mesh)
+    out["CP"] = cp.ravel()
+    return out
+
+
+def window(mesh, ex_a, ex_b, ey_a, ey_b):
+    """Sub-patch of elements [ex_a, ex_b) x [ey_a, ey_b) with its control points and tables."""
+    p, q = mesh["p"], mesh.get("q", mesh["p"])
+    m = mesh["nex"] + p
+    n = mesh["ney"] + q
+    cp = np.asarray(mesh["CP"]).reshape(n, m, 2)[ey_a:ey_b + q, ex_a:ex_b + p]
+    nb1, nb2 = (p + 1) ** 2, (q + 1) ** 2
+    w = dict(p=p, q=q, nex=ex_b - ex_a, ney=ey_b - ey_a, CP=np.ascontiguousarray(cp).ravel(),
+             C1=np.asarray(mesh["C1"])[ex_a * nb1:ex_b * nb1], C2=np.asarray(mesh["C2"])[ey_a * nb2:ey_b * nb2],
+             h1=np.full(ex_b - ex_a, 1.0 / mesh["nex"]), h2=np.full(ey_b - ey_a, 1.0 / mesh["ney"]),
+             W=None, kappa=None)
+    return w
+
+
+def window_rows(mesh, ex_a, ex_b, ey_a, ey_b):
+    """Global (R, C) index arrays of the window's rows whose support lies inside it."""
+    p, q = mesh["p"], mesh.get("q", mesh["p"])
+    m = mesh["nex"] + p
+    n = mesh["ney"] + q
+    c0 = 0 if ex_a == 0 else ex_a + p
+    c1 = m if ex_b == mesh["nex"] else ex_b
+    r0 = 0 if ey_a == 0 else ey_a + q
+    r1 = n if ey_b == mesh["ney"] else ey_b
+    return (r0, r1, c0, c1)
