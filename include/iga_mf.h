@@ -147,6 +147,33 @@ int iga_MatrixFreeMatMultCUDA(int p, int q, int nlocalelemx, int nlocalelemy,
 /* Drop every plan cached by iga_MatrixFreeMatMultCUDA. */
 int iga_MatrixFreeMatMultCUDA_release(void);
 
+/* Allocation-free MatMult. No counterpart in the reference: added for callers
+ * that cannot allocate device memory when they need a MatMult (their own memory
+ * pool owns the GPU, or a cudaMalloc/cudaFree device synchronisation inside a
+ * solver loop is not acceptable). Arguments are those of
+ * iga_MatrixFreeMatMultCUDA plus a stream; every array is a caller-owned device
+ * array, and d_B1/d_dB1 (d_B2/d_dB2) must hold the Bernstein values/derivatives
+ * at the p+1 (q+1) Gauss points on [0,1], point-major, and qw1/qw2 the Gauss
+ * weights (the arrays the reference uploads). Geometry is computed on the fly
+ * from d_CP (no NURBS weights). Computes y = A_ref x with y[Dir] = 0.
+ * This entry point calls no cudaMalloc, cudaFree or other allocating routine:
+ * its scratch (basis tables and seam frames) is a fixed 16 MiB device array
+ * held by every GPU that loads the library until the process exits. Meshes whose
+ * scratch would exceed 16 MiB are rejected with IGA_ERR_UNSUPPORTED (p = 3 up to
+ * about 2048 x 2048 elements fits). The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and sets the kernel's shared
+ * memory limit; make that first call before any stream capture. All calls share
+ * the one array, so calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
+int iga_MatrixFreeMatMultCUDA_noalloc(int p, int q, int nlocalelemx, int nlocalelemy,
+                                      const double *d_B1, const double *d_B2,
+                                      const double *d_dB1, const double *d_dB2,
+                                      const double *d_nurbs_extraction1, const double *d_nurbs_extraction2,
+                                      const double *d_elem_size1, const double *d_elem_size2,
+                                      const int *d_IEN, const int *d_ID, const double *d_CP,
+                                      const double *qw1, const double *qw2,
+                                      const double *d_F_array_in, double *d_F_array_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

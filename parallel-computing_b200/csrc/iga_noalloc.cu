@@ -1,0 +1,222 @@
+// Allocation-free variant of the reference-shaped MatMult entry point.
+//
+// Some callers cannot allocate device memory at the moment they need a
+// MatMult: a host application whose memory pool already owns the whole GPU
+// (a framework caching allocator, a solver library with its own pool), or a
+// Krylov loop that must not hit the implicit device synchronisation of
+// cudaMalloc/cudaFree. iga_MatrixFreeMatMultCUDA_noalloc serves them: the
+// caller passes every input and output as device arrays (the argument list of
+// the reference's MatrixFreeMatMultCUDA plus a stream), and the only scratch
+// the kernels need - the per-element-column / per-element-row basis tables and
+// the seam frames of the atomic-free reduction - lives in the fixed array
+// g_noalloc_scratch below, which every GPU that loads this library holds until
+// the process exits.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <mutex>
+
+#include "iga_apply.cuh"
+#include "iga_plan.hpp"
+
+namespace {
+
+constexpr size_t kScratchBytes = size_t(16) << 20;   // 16 MiB per device
+constexpr int kMaxDevices = 64;
+
+// File-scope device scratch. In host code this name is only a stand-in for
+// the symbol, never a device address: the address comes from
+// cudaGetSymbolAddress, per device, in scratch_on_current_device().
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+std::mutex g_mu;
+void *g_addr[kMaxDevices] = {};
+bool g_attr[kMaxDevices][6] = {};
+
+// One-time set-up per device (first call on that device, under a lock): fetch
+// the scratch address with the device current. Returns null on failure.
+void *scratch_on_current_device(int &dev)
+{
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return nullptr;
+        g_addr[dev] = p;
+    }
+    return g_addr[dev];
+}
+
+// Basis tables of the apply kernel from the caller's Bernstein tables
+// (B[k][i]: quadrature point k, Bernstein function i, the layout of
+// matrix_free_gpu/src/GlobalAssemblyMF.cu:156-169) and extraction operators:
+// N = C_e B (matrix_free/src/RefElement.cpp:20-57), in reference-element
+// coordinates (no division by the element size).
+__global__ void noalloc_tables_kernel(double *__restrict__ tabX, double *__restrict__ tabY,
+                                      double *__restrict__ wq, int *__restrict__ err,
+                                      const double *__restrict__ B1, const double *__restrict__ dB1,
+                                      const double *__restrict__ B2, const double *__restrict__ dB2,
+                                      const double *__restrict__ C1, const double *__restrict__ C2,
+                                      const double *__restrict__ qw1, const double *__restrict__ qw2, int P,
+                                      int nex, int ney, int NSX)
+{
+    const int NB = P + 1, NQ = P + 1;
+    const long long nX = (long long)NSX * 2 * NQ * NB * 32;
+    const long long nY = (long long)ney * 2 * NQ * NB;
+    const long long tid0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (tid0 == 0) *err = 0;
+    for (long long t = tid0; t < nX + nY + NQ * NQ; t += (long long)gridDim.x * blockDim.x) {
+        if (t < nX) {   // [gx][kind][qx][il][lane]
+            const int lane = (int)(t % 32);
+            long long r = t / 32;
+            const int il = (int)(r % NB);
+            r /= NB;
+            const int qx = (int)(r % NQ);
+            r /= NQ;
+            const int kind = (int)(r % 2);
+            const int gx = (int)(r / 2);
+            const int ex = 32 * gx + lane;
+            double v = 0.0;
+            if (ex < nex) {
+                const double *Ce = C1 + (size_t)ex * NB * NB + il * NB;
+                const double *Bq = (kind ? dB1 : B1) + qx * NB;
+                for (int k = 0; k < NB; ++k) v += Ce[k] * Bq[k];
+            }
+            tabX[t] = v;
+        } else if (t < nX + nY) {   // [ey][kind][qy][jl]
+            const long long u = t - nX;
+            const int jl = (int)(u % NB);
+            long long r = u / NB;
+            const int qy = (int)(r % NQ);
+            r /= NQ;
+            const int kind = (int)(r % 2);
+            const int ey = (int)(r / 2);
+            const double *Ce = C2 + (size_t)ey * NB * NB + jl * NB;
+            const double *Bq = (kind ? dB2 : B2) + qy * NB;
+            double v = 0.0;
+            for (int k = 0; k < NB; ++k) v += Ce[k] * Bq[k];
+            tabY[u] = v;
+        } else {
+            const int k = (int)(t - nX - nY);
+            wq[k] = qw1[k % NQ] * qw2[k / NQ];
+        }
+    }
+}
+
+struct Layout {
+    size_t off_err, off_wq, off_tabX, off_tabY, off_frame, total;
+};
+
+size_t up256(size_t v) { return (v + 255) & ~size_t(255); }
+
+Layout layout_for(int P, int nex, int ney, int TY)
+{
+    const int NB = P + 1, NQ = P + 1;
+    const long long NSX = (nex + 31) / 32, NSY = (ney + TY - 1) / TY;
+    Layout L;
+    L.off_err = 0;
+    L.off_wq = 256;
+    L.off_tabX = L.off_wq + up256(sizeof(double) * NQ * NQ);
+    L.off_tabY = L.off_tabX + up256(sizeof(double) * NSX * 2 * NQ * NB * 32);
+    L.off_frame = L.off_tabY + up256(sizeof(double) * (size_t)ney * 2 * NQ * NB);
+    L.total = L.off_frame + up256(sizeof(double) * NSX * NSY * iga::frame_size(P, TY));
+    return L;
+}
+
+template <int P>
+int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int ney, const double *d_CP,
+           const double *d_in, double *d_out, cudaStream_t s)
+{
+    using namespace iga;
+    int W = 8;
+    while (W > 1 && apply_smem_bytes<P, double, 2>(W) > 220 * 1024) --W;
+    const size_t smem = apply_smem_bytes<P, double, 2>(W);
+    auto kern = apply_kernel<P, double, 1, 2>;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (!g_attr[dev][P]) {
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+                return IGA_ERR_CUDA;
+            g_attr[dev][P] = true;
+        }
+    }
+    StripGrid g;
+    g.m = nex + P;
+    g.n = ney + P;
+    g.nex = nex;
+    g.ney = ney;
+    g.TY = TY;
+    g.NSX = (nex + 31) / 32;
+    g.NSY = (ney + TY - 1) / TY;
+    g.P = P;
+    g.FS = frame_size(P, TY);
+    ApplyParams<double> a;
+    a.x = d_in;
+    a.y = d_out;
+    a.G = nullptr;
+    a.tabX = reinterpret_cast<const double *>(base + Ly.off_tabX);
+    a.tabY = reinterpret_cast<const double *>(base + Ly.off_tabY);
+    a.CP = d_CP;
+    a.wq = reinterpret_cast<const double *>(base + Ly.off_wq);
+    a.kappa = nullptr;
+    a.frame = reinterpret_cast<double *>(base + Ly.off_frame);
+    a.g = g;
+    a.sign = -1.0;   // the reference operator A_ref = -K
+    a.bc = IGA_BC_REFERENCE;
+    a.err = reinterpret_cast<int *>(base + Ly.off_err);
+    dim3 grid(g.NSX, (g.NSY + W - 1) / W), block(32, W);
+    kern<<<grid, block, smem, s>>>(a);
+    const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
+    if (nseam > 0)
+        seam_fixup_kernel<P, double><<<(int)std::min<long long>((nseam + 255) / 256, 592), 256, 0, s>>>(
+            a.frame, d_in, d_out, g, -1.0, IGA_BC_REFERENCE);
+    return cudaGetLastError() == cudaSuccess ? IGA_OK : IGA_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int iga_MatrixFreeMatMultCUDA_noalloc(int p, int q, int nex, int ney, const double *d_B1,
+                                                 const double *d_B2, const double *d_dB1, const double *d_dB2,
+                                                 const double *d_C1, const double *d_C2, const double *,
+                                                 const double *, const int *, const int *, const double *d_CP,
+                                                 const double *qw1, const double *qw2, const double *d_in,
+                                                 double *d_out, void *stream)
+{
+    if (p < 1 || p > 5 || q != p || nex < 1 || ney < 1) return p == q ? IGA_ERR_ARG : IGA_ERR_UNSUPPORTED;
+    if (!d_B1 || !d_B2 || !d_dB1 || !d_dB2 || !d_C1 || !d_C2 || !d_CP || !qw1 || !qw2 || !d_in || !d_out)
+        return IGA_ERR_ARG;
+    // Strip height: the smallest of these whose tables and frames fit the scratch.
+    int TY = 0;
+    Layout Ly{};
+    for (int cand : {32, 64, 128, 256, 512, 1024}) {
+        if (cand < p) continue;
+        Ly = layout_for(p, nex, ney, cand);
+        if (Ly.total <= kScratchBytes) {
+            TY = cand;
+            break;
+        }
+    }
+    if (!TY) {
+        iga::set_error("mesh too large for the fixed 16 MiB scratch of iga_MatrixFreeMatMultCUDA_noalloc");
+        return IGA_ERR_UNSUPPORTED;
+    }
+    int dev = 0;
+    unsigned char *base = static_cast<unsigned char *>(scratch_on_current_device(dev));
+    if (!base) {
+        iga::set_error("cudaGetSymbolAddress of the no-alloc scratch failed");
+        return IGA_ERR_CUDA;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int NSX = (nex + 31) / 32;
+    noalloc_tables_kernel<<<148, 256, 0, s>>>(
+        reinterpret_cast<double *>(base + Ly.off_tabX), reinterpret_cast<double *>(base + Ly.off_tabY),
+        reinterpret_cast<double *>(base + Ly.off_wq), reinterpret_cast<int *>(base + Ly.off_err), d_B1, d_dB1, d_B2,
+        d_dB2, d_C1, d_C2, qw1, qw2, p, nex, ney, NSX);
+    switch (p) {
+    case 1: return launch<1>(dev, base, Ly, TY, nex, ney, d_CP, d_in, d_out, s);
+    case 2: return launch<2>(dev, base, Ly, TY, nex, ney, d_CP, d_in, d_out, s);
+    case 3: return launch<3>(dev, base, Ly, TY, nex, ney, d_CP, d_in, d_out, s);
+    case 4: return launch<4>(dev, base, Ly, TY, nex, ney, d_CP, d_in, d_out, s);
+    default: return launch<5>(dev, base, Ly, TY, nex, ney, d_CP, d_in, d_out, s);
+    }
+}

@@ -67,6 +67,7 @@ SIGNATURES = [
     ("iga_rhs", ctypes.c_int, [VP, ctypes.c_int, VP, VP]),
     ("iga_MatrixFreeMatMultCUDA", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 15),
     ("iga_MatrixFreeMatMultCUDA_release", ctypes.c_int, []),
+    ("iga_MatrixFreeMatMultCUDA_noalloc", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 16),
 ]
 
 
