@@ -220,8 +220,9 @@ def our_arm(args):
     sys.path.insert(0, PKG)
     import iga_b200 as ib
 
-    mesh = ib.unit_square(P, NE, NE)
-    N = (NE + P) ** 2
+    ne = args.ne
+    mesh = ib.unit_square(P, ne, ne)
+    N = (ne + P) ** 2
     x_host = splitmix_uniform(SEED + rank, -1.0, 1.0, N)
     xd = torch.from_numpy(x_host).cuda()
     yd = torch.empty_like(xd)
@@ -266,18 +267,19 @@ def our_arm(args):
 
     peak, peak_kind = measured_peaks()
     variants = {}
-    # on-the-fly geometry (mult_mf): its inputs (x, control points) fit in L2,
-    # so L2 is flushed between timed applies.
-    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
-    plan_mf = ib.Plan(mesh, geometry=ib.GEOM_ON_THE_FLY)
-    k_mf = max(1, min(args.steps, 200))
-    ms_mf = timed_loop(plan_mf, k_mf, args.warmup, flush=flush)
-    variants["on_the_fly_geometry"] = {
-        "value": ws * N * k_mf / (ms_mf * 1e-3) / 1e9, "unit": "GDOF/s", "ms_per_step": ms_mf / k_mf,
-        "algo_bytes_per_step": plan_mf.info.algo_bytes_f64, "l2": "flushed between timed applies"}
-    plan_mf.close()
-    del flush
-    torch.cuda.empty_cache()
+    if not args.skip_variants:
+        # on-the-fly geometry (mult_mf): its inputs (x, control points) fit in
+        # L2, so L2 is flushed between timed applies.
+        flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device="cuda")
+        plan_mf = ib.Plan(mesh, geometry=ib.GEOM_ON_THE_FLY)
+        k_mf = max(1, min(args.steps, 200))
+        ms_mf = timed_loop(plan_mf, k_mf, args.warmup, flush=flush)
+        variants["on_the_fly_geometry"] = {
+            "value": ws * N * k_mf / (ms_mf * 1e-3) / 1e9, "unit": "GDOF/s", "ms_per_step": ms_mf / k_mf,
+            "algo_bytes_per_step": plan_mf.info.algo_bytes_f64, "l2": "flushed between timed applies"}
+        plan_mf.close()
+        del flush
+        torch.cuda.empty_cache()
 
     plan = ib.Plan(mesh, geometry=ib.GEOM_PRECOMPUTED)
     algo = plan.info.algo_bytes_f64
@@ -289,20 +291,22 @@ def our_arm(args):
     achieved = algo / (ms_step * 1e-3) / 1e9
 
     # e2e through the host-buffer C ABI call (pinned host memory).
-    xh = torch.from_numpy(x_host).pin_memory()
-    yh = torch.empty_like(xh).pin_memory()
-    xh_np, yh_np = xh.numpy(), yh.numpy()
-    for _ in range(max(3, args.warmup // 4)):
-        plan.apply_host(xh_np, yh_np)
-    barrier()
-    k_e2e = max(3, min(args.steps, 100))
-    t0 = time.perf_counter()
-    for _ in range(k_e2e):
-        plan.apply_host(xh_np, yh_np)
-    barrier()
-    t_e2e = max_over_ranks(time.perf_counter() - t0)
-    e2e = {"value": ws * N * k_e2e / t_e2e / 1e9, "unit": "GDOF/s", "h2d_bytes_per_step": 8 * N,
-           "d2h_bytes_per_step": 8 * N, "call": "iga_apply_host (MATSHELL MatMult on host vectors)"}
+    e2e = None
+    if not args.no_e2e:
+        xh = torch.from_numpy(x_host).pin_memory()
+        yh = torch.empty_like(xh).pin_memory()
+        xh_np, yh_np = xh.numpy(), yh.numpy()
+        for _ in range(max(3, args.warmup // 4)):
+            plan.apply_host(xh_np, yh_np)
+        barrier()
+        k_e2e = max(3, min(args.steps, 100))
+        t0 = time.perf_counter()
+        for _ in range(k_e2e):
+            plan.apply_host(xh_np, yh_np)
+        barrier()
+        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": ws * N * k_e2e / t_e2e / 1e9, "unit": "GDOF/s", "h2d_bytes_per_step": 8 * N,
+               "d2h_bytes_per_step": 8 * N, "call": "iga_apply_host (MATSHELL MatMult on host vectors)"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -314,10 +318,10 @@ def our_arm(args):
         out = {"metric": METRIC, "value": value, "unit": "GDOF/s", "n_gpus": ws, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": "matmul_c2_p3_2048x2048_fp64_precomputed_geometry", "p": P,
-                          "nElem": [NE, NE], "dofs_per_gpu": N, "quadrature_points_per_element": 16,
+               "config": {"workload": f"matmul_p3_{ne}x{ne}_fp64_precomputed_geometry", "p": P,
+                          "nElem": [ne, ne], "dofs_per_gpu": N, "quadrature_points_per_element": 16,
                           "geometry_bytes": plan.info.geom_bytes, "parallelism": f"replicas{ws}",
-                          "l2": "inputs larger than L2 (1.61 GB of geometry streamed per apply)",
+                          "l2": f"inputs larger than L2 ({plan.info.geom_bytes / 1e9:.2f} GB of geometry streamed per apply)",
                           "rows_per_strip": plan.info.rows_per_strip, "warps_per_cta": plan.info.warps_per_cta},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": profiled_traffic("apply_c2_p3_fp64_precomputed"),
@@ -341,6 +345,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ne", type=int, default=NE, help="elements per direction (profiling runs use smaller cases)")
+    ap.add_argument("--skip-variants", action="store_true", help="skip the on-the-fly-geometry timing")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer timing")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
