@@ -1,0 +1,96 @@
+/* iga_solve.h - device-resident Krylov solve of the IGA Poisson system with
+ * the bilinear-FEM preconditioner, and the FEM preconditioner's assembly.
+ *
+ * Replaces the reference's solve loop: PETSc KSPSolve on the MATSHELL with a
+ * PCSHELL whose apply is an inner KSPCG + PCJACOBI solve of the bilinear FEM
+ * matrix (matrix_free/iteration_number_fempc_mf.cpp:11-17,199-233), and the
+ * GPU driver's FEM assembly (elem2coo + MATAIJCUSPARSE COO assembly:
+ * matrix_free_gpu/src/Elem2COOGenerator.cpp:3-69, matrix_free_gpu/src/assembly.cu:41-99,
+ * matrix_free_gpu/src/GlobalAssembly.cu:3-108).
+ *
+ * The system solved is the SPD form K u = b (boundary rows identity, b[Dir]
+ * expected 0). The reference solves A_ref u = F with A_ref = -K, whose
+ * solution is the negative of this one; pass -F to get the reference's
+ * vector. Iteration counts are not strictly comparable with the reference:
+ * it runs GMRES with a preconditioned-residual test; this runs flexible PCG
+ * to a relative TRUE residual ||b - K u|| / ||b|| <= rtol.
+ */
+#ifndef IGA_SOLVE_H
+#define IGA_SOLVE_H
+
+#include <stdint.h>
+
+#include "iga_mf.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    IGA_PC_NONE = 0,      /* unpreconditioned CG */
+    IGA_PC_FEM_CG = 1,    /* reference: inner Jacobi-CG on the bilinear FEM matrix */
+    IGA_PC_FEM_EXACT = 2  /* the same FEM matrix inverted exactly (tensor-product fast diagonalisation) */
+};
+
+typedef struct {
+    int precision;     /* IGA_FP64: FP64 PCG. IGA_MIXED: FP32 PCG sweeps (FP32 operator and
+                          preconditioner) wrapped in FP64 iterative refinement. */
+    int pc;            /* IGA_PC_* */
+    double rtol;       /* target relative true residual (FP64) */
+    int max_it;        /* outer PCG iterations per solve / per FP32 sweep */
+    double pc_rtol;    /* IGA_PC_FEM_CG inner tolerance (reference: 1e-10) */
+    int pc_max_it;     /* IGA_PC_FEM_CG inner iteration cap (reference: 10000) */
+    double sweep_rtol; /* IGA_MIXED: residual reduction asked of each FP32 sweep */
+    int max_sweeps;    /* IGA_MIXED: refinement sweeps */
+    int x0_nonzero;    /* 1: use x as the initial guess, 0: start from x = 0 */
+} iga_solve_opts;
+
+typedef struct {
+    int status;            /* IGA_OK or IGA_ERR_NOT_CONVERGED / BREAKDOWN / NONFINITE */
+    int iterations;        /* outer PCG iterations (all sweeps) */
+    int64_t pc_iterations; /* inner FEM-CG iterations (IGA_PC_FEM_CG) */
+    int sweeps;            /* refinement sweeps (IGA_MIXED) */
+    double relres;         /* final ||b - K x|| / ||b||, FP64 */
+    double seconds;        /* wall time of the solve (device synchronised) */
+} iga_solve_stats;
+
+void iga_solve_opts_default(iga_solve_opts *opts);
+
+/* Solve K x = b on the device (b, x: nfunc doubles, caller-owned). The plan
+ * must hold the FP64 operator; IGA_MIXED needs a plan created with
+ * precision IGA_MIXED (both operators). */
+int iga_solve(iga_plan *plan, const double *b_dev, double *x_dev, const iga_solve_opts *opts,
+              iga_solve_stats *stats, void *stream);
+
+/* z = M^-1 r for one preconditioner (the PCSHELL apply MyPCApply,
+ * matrix_free/iteration_number_fempc_mf.cpp:11-17): IGA_PC_FEM_CG runs the inner
+ * Jacobi-CG to pc_rtol (at most pc_max_it iterations), IGA_PC_FEM_EXACT applies
+ * K_fem^-1 exactly, IGA_PC_NONE copies. precision: IGA_FP64 (double arrays) or
+ * IGA_FP32 (float arrays; FEM_EXACT then uses TF32 tensor-core GEMMs). */
+int iga_pc_apply(iga_plan *plan, int pc, int precision, const void *r_dev, void *z_dev, double pc_rtol,
+                 int pc_max_it, void *stream);
+
+/* y = K_fem x, the SPD bilinear-FEM matrix of the preconditioner (boundary
+ * rows identity), matrix-free from its 1-D tensor factors; precision of x/y
+ * as for iga_apply_prec. */
+int iga_fem_apply(iga_plan *plan, int precision, const void *x_dev, void *y_dev, void *stream);
+
+/* The FEM preconditioner matrix assembled on the device in CSR form, one
+ * thread per row, no atomics (replaces Elem2COOGenerator + the COO atomicAdd
+ * assembly). sign = -1 gives the reference's matrix (-K_fem on free rows,
+ * +1 on Dirichlet diagonals), +1 the SPD one. Call with NULL arrays to get
+ * nnz; rowptr has nfunc+1 entries. */
+int iga_fem_assemble_csr(iga_plan *plan, int sign, int32_t *rowptr_dev, int32_t *colidx_dev, double *vals_dev,
+                         int64_t *nnz, void *stream);
+
+/* 1-D node coordinates of the FEM preconditioner grid (host arrays of
+ * nElemX+p and nElemY+q entries): degree p-2 Greville abscissae of the
+ * shortened knot vector (matrix_free/preprocess_fem.cpp:38-60) for p >= 3; the
+ * reference divides by zero for p = 2, replaced by the degree-2 Greville
+ * abscissae of the IGA knot vector. */
+int iga_fem_nodes(const iga_plan *plan, double *gx, double *gy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* IGA_SOLVE_H */

@@ -268,7 +268,7 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
 }
 
 template <int P, typename T, int GEOM, int NST>
-static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s)
+static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s, int sign, int bc)
 {
     ApplyParams<T> a;
     a.x = x;
@@ -281,8 +281,8 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
     a.kappa = (const T *)op.kappa;
     a.frame = (T *)op.frame;
     a.g = pl->grid;
-    a.sign = (T)pl->sign;
-    a.bc = pl->bc;
+    a.sign = (T)sign;
+    a.bc = bc;
     a.err = pl->d_err;
     const int W = op.warps;
     const size_t smem = apply_smem_bytes<P, T, NST>(W);
@@ -298,41 +298,46 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
     const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
     if (nseam > 0) {
         const int blocks = (int)std::min<long long>((nseam + 255) / 256, 4 * 148);
-        seam_fixup_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)pl->sign, pl->bc);
+        seam_fixup_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)sign, bc);
     }
     IGA_CUDA_TRY(cudaGetLastError());
     return IGA_OK;
 }
 
 template <int P, typename T>
-static int launch_apply_p(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s)
+static int launch_apply_p(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s, int sign, int bc)
 {
     constexpr int NST = sizeof(T) == 8 ? 2 : 3;
-    if (pl->geometry == IGA_GEOM_PRECOMPUTED) return launch_apply_t<P, T, 0, NST>(pl, op, x, y, s);
-    return launch_apply_t<P, T, 1, NST>(pl, op, x, y, s);
+    if (pl->geometry == IGA_GEOM_PRECOMPUTED) return launch_apply_t<P, T, 0, NST>(pl, op, x, y, s, sign, bc);
+    return launch_apply_t<P, T, 1, NST>(pl, op, x, y, s, sign, bc);
 }
 
 template <typename T>
-static int launch_apply(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s)
+static int launch_apply(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s, int sign, int bc)
 {
     switch (pl->p) {
-    case 1: return launch_apply_p<1, T>(pl, op, x, y, s);
-    case 2: return launch_apply_p<2, T>(pl, op, x, y, s);
-    case 3: return launch_apply_p<3, T>(pl, op, x, y, s);
-    case 4: return launch_apply_p<4, T>(pl, op, x, y, s);
-    case 5: return launch_apply_p<5, T>(pl, op, x, y, s);
+    case 1: return launch_apply_p<1, T>(pl, op, x, y, s, sign, bc);
+    case 2: return launch_apply_p<2, T>(pl, op, x, y, s, sign, bc);
+    case 3: return launch_apply_p<3, T>(pl, op, x, y, s, sign, bc);
+    case 4: return launch_apply_p<4, T>(pl, op, x, y, s, sign, bc);
+    case 5: return launch_apply_p<5, T>(pl, op, x, y, s, sign, bc);
     default: return IGA_ERR_UNSUPPORTED;
     }
 }
 
-int iga_apply_internal(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s)
+int iga_apply_internal_sb(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s, int sign, int bc)
 {
     if (prec == IGA_FP64) {
         if (!pl->op64.ready) return IGA_ERR_ARG;
-        return launch_apply<double>(pl, pl->op64, (const double *)x, (double *)y, s);
+        return launch_apply<double>(pl, pl->op64, (const double *)x, (double *)y, s, sign, bc);
     }
     if (!pl->op32.ready) return IGA_ERR_ARG;
-    return launch_apply<float>(pl, pl->op32, (const float *)x, (float *)y, s);
+    return launch_apply<float>(pl, pl->op32, (const float *)x, (float *)y, s, sign, bc);
+}
+
+int iga_apply_internal(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s)
+{
+    return iga_apply_internal_sb(pl, prec, x, y, s, pl->sign, pl->bc);
 }
 
 int iga_check_error_flag(iga_plan *pl)

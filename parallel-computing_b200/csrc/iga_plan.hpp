@@ -46,5 +46,7 @@ struct iga_plan {
 };
 
 int iga_apply_internal(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s);
+// Operator with explicit sign / boundary rule (the solver applies +K with identity rows).
+int iga_apply_internal_sb(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s, int sign, int bc);
 int iga_check_error_flag(iga_plan *pl);
 void iga_solver_release(iga_plan *pl);

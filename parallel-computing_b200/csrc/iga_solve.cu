@@ -1,0 +1,1099 @@
+// Device-resident flexible PCG for K u = b with the bilinear-FEM
+// preconditioner (include/iga_solve.h).
+//
+// Reference loop (matrix_free/iteration_number_fempc_mf.cpp:193-233): PETSc
+// KSPSolve on the MATSHELL operator, PCSHELL apply = inner KSPCG + PCJACOBI on
+// the FEM matrix to rtol = abstol = 1e-10 (:210-224). Here every vector, every
+// scalar (alpha, beta, dot products) and every convergence test lives on the
+// device; the host only reads one flag per outer iteration. All reductions
+// are deterministic (fixed-order block partials, summed by the last block).
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/iga_solve.h"
+#include "iga_fastdiag.hpp"
+#include "iga_plan.hpp"
+
+namespace iga {
+
+constexpr int kRedBlocks = 296;   // fixed grid of every reduction kernel (2 x 148 SMs)
+constexpr int kThreads = 256;
+constexpr int kChunk = 16;        // inner CG iterations per captured graph
+
+struct DevScalars {
+    double alpha, beta, rz, rr, rr0, tol2, bb;      // outer PCG
+    double ialpha, ibeta, irz, irr, itol2;          // inner FEM-CG
+    int done, breakdown, idone, iiters, ibreak, imax;
+};
+
+// ------------------------------------------------------------ reductions
+// Block sums of K values; the last block to finish sums the per-block
+// partials in block order and returns true (thread 0 holds the totals).
+template <int K>
+__device__ bool reduce_last(double (&v)[K], double *partials, unsigned *counter, double (&tot)[K])
+{
+    __shared__ double sh[K][kThreads / 32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = v[k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) sh[k][wid] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = 0.0;
+            for (int w = 0; w < kThreads / 32; ++w) s += sh[k][w];
+            partials[blockIdx.x * K + k] = s;
+        }
+        __threadfence();
+        const unsigned t = atomicAdd(counter, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    // Last block: every thread sums a fixed subset of the partials in block
+    // order, then a fixed-shape tree (warp shuffles, then warp 0) combines them.
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads) s += ((volatile double *)partials)[b * K + k];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) sh[k][wid] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double s = 0.0;
+            for (int w = 0; w < kThreads / 32; ++w) s += sh[k][w];
+            tot[k] = s;
+        }
+        *counter = 0u;
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool bnd(int i, int j, int m, int n) { return i == 0 || j == 0 || i == m - 1 || j == n - 1; }
+
+// ------------------------------------------------------------ FEM stencil
+// K_fem = Kx (x) My + Mx (x) Ky on the free nodes (1-D linear-element
+// stiffness K and mass M from the node coordinates; the 2x2-Gauss bilinear
+// element matrices of matrix_free/src/ElementFEM.cpp:3-117 are exactly these
+// tensor products), identity rows on the boundary.
+template <typename T>
+struct FemCoef {
+    const T *kd, *ko, *md, *mo;   // x: diag / off-diagonal (i,i+1)
+    const T *ld, *lo, *nd, *no;   // y: stiffness diag / off, mass diag / off
+    int m, n;
+};
+
+template <typename T>
+__device__ __forceinline__ T fem_row(const T *__restrict__ p, int i, int j, const FemCoef<T> &c)
+{
+    const T kx[3] = {c.ko[i - 1], c.kd[i], c.ko[i]}, mx[3] = {c.mo[i - 1], c.md[i], c.mo[i]};
+    const T ky[3] = {c.lo[j - 1], c.ld[j], c.lo[j]}, my[3] = {c.no[j - 1], c.nd[j], c.no[j]};
+    const bool xl = i - 1 >= 1, xr = i + 1 <= c.m - 2, yl = j - 1 >= 1, yr = j + 1 <= c.n - 2;
+    T s = 0;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        if ((b == 0 && !yl) || (b == 2 && !yr)) continue;
+        const T *row = p + (size_t)(j + b - 1) * c.m;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if ((a == 0 && !xl) || (a == 2 && !xr)) continue;
+            s += (kx[a] * my[b] + mx[a] * ky[b]) * row[i + a - 1];
+        }
+    }
+    return s;
+}
+
+template <typename T>
+__device__ __forceinline__ T fem_diag(int i, int j, const FemCoef<T> &c)
+{
+    return c.kd[i] * c.nd[j] + c.md[i] * c.ld[j];
+}
+
+template <typename T>
+__global__ void fem_apply_kernel(const T *__restrict__ x, T *__restrict__ y, FemCoef<T> c)
+{
+    const long long N = (long long)c.m * c.n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % c.m), j = (int)(t / c.m);
+        y[t] = bnd(i, j, c.m, c.n) ? x[t] : fem_row(x, i, j, c);
+    }
+}
+
+// CSR rows of the FEM matrix (sorted columns); rowptr precomputed on the host.
+__global__ void fem_csr_kernel(const int32_t *__restrict__ rowptr, int32_t *__restrict__ col, double *__restrict__ val,
+                               FemCoef<double> c, double sign)
+{
+    const long long N = (long long)c.m * c.n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % c.m), j = (int)(t / c.m);
+        int k = rowptr[t];
+        if (bnd(i, j, c.m, c.n)) {
+            col[k] = (int32_t)t;
+            val[k] = 1.0;
+            continue;
+        }
+        const double kx[3] = {c.ko[i - 1], c.kd[i], c.ko[i]}, mx[3] = {c.mo[i - 1], c.md[i], c.mo[i]};
+        const double ky[3] = {c.lo[j - 1], c.ld[j], c.lo[j]}, my[3] = {c.no[j - 1], c.nd[j], c.no[j]};
+        for (int b = 0; b < 3; ++b) {
+            const int jj = j + b - 1;
+            if (jj < 1 || jj > c.n - 2) continue;
+            for (int a = 0; a < 3; ++a) {
+                const int ii = i + a - 1;
+                if (ii < 1 || ii > c.m - 2) continue;
+                col[k] = (int32_t)((long long)jj * c.m + ii);
+                val[k] = sign * (kx[a] * my[b] + mx[a] * ky[b]);
+                ++k;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ inner FEM-CG (the PC apply)
+// Jacobi-preconditioned CG on K_fem z = r_in to ||r|| <= pc_rtol ||r_in||.
+template <typename T>
+struct InnerCG {
+    T *z, *r, *p, *q;
+    const T *rhs;
+    FemCoef<T> c;
+    DevScalars *s;
+    double *partials;
+    unsigned *counter;
+};
+
+template <typename T>
+__global__ void icg_init_kernel(InnerCG<T> a, const T *__restrict__ rhs, double rtol, int maxit)
+{
+    const long long N = (long long)a.c.m * a.c.n;
+    double v[2] = {0.0, 0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % a.c.m), j = (int)(t / a.c.m);
+        const T r = rhs[t];
+        const T d = bnd(i, j, a.c.m, a.c.n) ? T(1) : fem_diag(i, j, a.c);
+        const T zz = r / d;
+        a.z[t] = 0;
+        a.r[t] = r;
+        a.p[t] = zz;
+        v[0] += (double)r * (double)zz;
+        v[1] += (double)r * (double)r;
+    }
+    double tot[2];
+    if (reduce_last<2>(v, a.partials, a.counter, tot) && threadIdx.x == 0) {
+        a.s->irz = tot[0];
+        a.s->irr = tot[1];
+        a.s->itol2 = rtol * rtol * tot[1];
+        a.s->iiters = 0;
+        a.s->imax = maxit;
+        a.s->ibreak = 0;
+        a.s->idone = (tot[1] == 0.0) ? 1 : 0;
+    }
+}
+
+template <typename T>
+__global__ void icg_q_kernel(InnerCG<T> a)
+{
+    if (a.s->idone) return;
+    const long long N = (long long)a.c.m * a.c.n;
+    double v[1] = {0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % a.c.m), j = (int)(t / a.c.m);
+        const T pv = a.p[t];
+        const T qv = bnd(i, j, a.c.m, a.c.n) ? pv : fem_row(a.p, i, j, a.c);
+        a.q[t] = qv;
+        v[0] += (double)pv * (double)qv;
+    }
+    double tot[1];
+    if (reduce_last<1>(v, a.partials, a.counter, tot) && threadIdx.x == 0) {
+        if (!(tot[0] > 0.0)) {
+            a.s->ibreak = 1;
+            a.s->idone = 1;
+        } else {
+            a.s->ialpha = a.s->irz / tot[0];
+        }
+    }
+}
+
+template <typename T>
+__global__ void icg_update_kernel(InnerCG<T> a)
+{
+    if (a.s->idone) return;
+    const long long N = (long long)a.c.m * a.c.n;
+    const T al = (T)a.s->ialpha;
+    double v[2] = {0.0, 0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % a.c.m), j = (int)(t / a.c.m);
+        a.z[t] += al * a.p[t];
+        const T r = a.r[t] - al * a.q[t];
+        a.r[t] = r;
+        const T d = bnd(i, j, a.c.m, a.c.n) ? T(1) : fem_diag(i, j, a.c);
+        v[0] += (double)r * (double)(r / d);
+        v[1] += (double)r * (double)r;
+    }
+    double tot[2];
+    if (reduce_last<2>(v, a.partials, a.counter, tot) && threadIdx.x == 0) {
+        a.s->ibeta = tot[0] / a.s->irz;
+        a.s->irz = tot[0];
+        a.s->irr = tot[1];
+        a.s->iiters += 1;
+        if (tot[1] <= a.s->itol2 || a.s->iiters >= a.s->imax || !(tot[1] == tot[1])) a.s->idone = 1;
+    }
+}
+
+template <typename T>
+__global__ void icg_p_kernel(InnerCG<T> a)
+{
+    if (a.s->idone) return;
+    const long long N = (long long)a.c.m * a.c.n;
+    const T be = (T)a.s->ibeta;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % a.c.m), j = (int)(t / a.c.m);
+        const T d = bnd(i, j, a.c.m, a.c.n) ? T(1) : fem_diag(i, j, a.c);
+        a.p[t] = a.r[t] / d + be * a.p[t];
+    }
+}
+
+// ------------------------------------------------------------ outer PCG vector kernels
+template <typename T>
+__global__ void dot_kernel(const T *__restrict__ a, const T *__restrict__ b, long long N, double *out, double *partials,
+                           unsigned *counter)
+{
+    double v[1] = {0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        v[0] += (double)a[t] * (double)b[t];
+    double tot[1];
+    if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) *out = tot[0];
+}
+
+// alpha = rz / (p.q) from the device scalars, x += alpha p, r -= alpha q, rr = r.r
+template <typename T>
+__global__ void pcg_pq_kernel(const T *__restrict__ p, const T *__restrict__ q, long long N, DevScalars *s,
+                              double *partials, unsigned *counter)
+{
+    double v[1] = {0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        v[0] += (double)p[t] * (double)q[t];
+    double tot[1];
+    if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) {
+        if (!(tot[0] > 0.0)) {
+            s->breakdown = 1;
+            s->alpha = 0.0;
+        } else {
+            s->alpha = s->rz / tot[0];
+        }
+    }
+}
+
+template <typename T>
+__global__ void pcg_xr_kernel(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p, const T *__restrict__ q,
+                              long long N, DevScalars *s, double *partials, unsigned *counter)
+{
+    const T al = (T)s->alpha;
+    double v[1] = {0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        x[t] += al * p[t];
+        const T rv = r[t] - al * q[t];
+        r[t] = rv;
+        v[0] += (double)rv * (double)rv;
+    }
+    double tot[1];
+    if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) s->rr = tot[0];
+}
+
+// Flexible (Polak-Ribiere) beta = r.(z - z_old) / rz_old; rz = r.z.
+template <typename T>
+__global__ void pcg_beta_kernel(const T *__restrict__ r, const T *__restrict__ z, const T *__restrict__ zo, long long N,
+                                DevScalars *s, double *partials, unsigned *counter)
+{
+    double v[2] = {0.0, 0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        v[0] += (double)r[t] * (double)z[t];
+        v[1] += (double)r[t] * (double)zo[t];
+    }
+    double tot[2];
+    if (reduce_last<2>(v, partials, counter, tot) && threadIdx.x == 0) {
+        s->beta = (tot[0] - tot[1]) / s->rz;
+        s->rz = tot[0];
+    }
+}
+
+template <typename T>
+__global__ void pcg_p_kernel(T *__restrict__ p, const T *__restrict__ z, long long N, const DevScalars *s, int first)
+{
+    const T be = first ? T(0) : (T)s->beta;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        p[t] = first ? z[t] : z[t] + be * p[t];   // the first direction never reads stale p
+}
+
+// r = b - Ax (FP64), rr = r.r, bb = b.b
+__global__ void residual_kernel(const double *__restrict__ b, const double *__restrict__ Ax, double *__restrict__ r,
+                                long long N, DevScalars *s, double *partials, unsigned *counter)
+{
+    double v[2] = {0.0, 0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const double rv = b[t] - Ax[t];
+        r[t] = rv;
+        v[0] += rv * rv;
+        v[1] += b[t] * b[t];
+    }
+    double tot[2];
+    if (reduce_last<2>(v, partials, counter, tot) && threadIdx.x == 0) {
+        s->rr = tot[0];
+        s->bb = tot[1];
+    }
+}
+
+// r = b - q, rr = r.r
+template <typename T>
+__global__ void sub_kernel(const T *__restrict__ b, const T *__restrict__ q, T *__restrict__ r, long long N,
+                           DevScalars *s, double *partials, unsigned *counter)
+{
+    double v[1] = {0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const T rv = b[t] - q[t];
+        r[t] = rv;
+        v[0] += (double)rv * (double)rv;
+    }
+    double tot[1];
+    if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) s->rr = tot[0];
+}
+
+template <typename T>
+__global__ void copy_kernel(T *__restrict__ dst, const T *__restrict__ src, long long N)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        dst[t] = src[t];
+}
+
+template <typename T>
+__global__ void zero_kernel(T *__restrict__ dst, long long N)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        dst[t] = 0;
+}
+
+// FP32 sweep right-hand side r32 = r64 / scale.
+__global__ void scale_down_kernel(const double *__restrict__ r, float *__restrict__ r32, long long N, const DevScalars *s)
+{
+    const double inv = s->rr > 0.0 ? 1.0 / sqrt(s->rr) : 0.0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        r32[t] = (float)(r[t] * inv);
+}
+
+// Refinement update x64 += scale * d32 (scale = ||r64|| of the sweep's rhs).
+__global__ void refine_update_kernel(double *__restrict__ x, const float *__restrict__ d, long long N, double scale)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        x[t] += scale * (double)d[t];
+}
+
+// ------------------------------------------------------------ exact FEM inverse (fast diagonalisation)
+// W(a, b) /= (lx[a] + ly[b]) on the nx x ny interior transform (column-major, ld nx).
+template <typename T>
+__global__ void fd_scale_kernel(T *__restrict__ W, const T *__restrict__ lx, const T *__restrict__ ly, int nx, int ny)
+{
+    const long long N = (long long)nx * ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(t % nx), b = (int)(t / nx);
+        W[t] /= (lx[a] + ly[b]);   // padding rows/columns: 0 / (1 + 1)
+    }
+}
+
+// Interior block of r (m x n grid, x fastest) into a zero-padded nxp x nyp
+// column-major matrix (rows = x), and back: GEMM-friendly leading dimensions.
+template <typename T>
+__global__ void fd_gather_kernel(const T *__restrict__ r, T *__restrict__ U, int m, int nx, int ny, int nxp, int nyp)
+{
+    const long long N = (long long)nxp * nyp;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(t % nxp), b = (int)(t / nxp);
+        U[t] = (a < nx && b < ny) ? r[(size_t)(b + 1) * m + (a + 1)] : T(0);
+    }
+}
+
+template <typename T>
+__global__ void fd_scatter_kernel(const T *__restrict__ Z, T *__restrict__ z, int m, int nx, int ny, int nxp)
+{
+    const long long N = (long long)nx * ny;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(t % nx), b = (int)(t / nx);
+        z[(size_t)(b + 1) * m + (a + 1)] = Z[(size_t)b * nxp + a];
+    }
+}
+
+// z = r on the boundary ring (identity rows of K_fem).
+template <typename T>
+__global__ void boundary_copy_kernel(T *__restrict__ z, const T *__restrict__ r, int m, int n)
+{
+    const long long nb = 2LL * m + 2LL * (n - 2);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb; t += (long long)gridDim.x * blockDim.x) {
+        long long idx;
+        if (t < m) idx = t;
+        else if (t < 2LL * m) idx = (long long)(n - 1) * m + (t - m);
+        else {
+            const long long u = t - 2LL * m;
+            const long long j = 1 + u / 2;
+            idx = j * m + ((u % 2) ? (m - 1) : 0);
+        }
+        z[idx] = r[idx];
+    }
+}
+
+// ------------------------------------------------------------ host state
+template <typename T>
+struct PrecState {
+    bool ready = false;
+    T *kd = nullptr, *ko = nullptr, *md = nullptr, *mo = nullptr;
+    T *ld = nullptr, *lo = nullptr, *nd = nullptr, *no = nullptr;
+    T *x = nullptr, *r = nullptr, *z = nullptr, *zo = nullptr, *p = nullptr, *q = nullptr, *b = nullptr;
+    T *iz = nullptr, *ir = nullptr, *ip = nullptr, *iq = nullptr;
+    cudaGraphExec_t chunk = nullptr;
+    // exact FEM inverse: eigenvectors (column-major), eigenvalues, two work matrices
+    T *Vx = nullptr, *Vy = nullptr, *lx = nullptr, *ly = nullptr, *W1 = nullptr, *W2 = nullptr;
+    int nxp = 0, nyp = 0;   // transform sizes padded to multiples of 64
+    FemCoef<T> coef() const
+    {
+        FemCoef<T> c;
+        c.kd = kd; c.ko = ko; c.md = md; c.mo = mo;
+        c.ld = ld; c.lo = lo; c.nd = nd; c.no = no;
+        return c;
+    }
+};
+
+struct SolverState {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cublasHandle_t blas = nullptr;
+    bool fd_host = false;
+    std::vector<double> lamx, lamy, Vx, Vy;   // host eigenpairs (built once)
+    DevScalars *s = nullptr;
+    DevScalars *h = nullptr;   // pinned mirror
+    double *partials = nullptr;
+    unsigned *counter = nullptr;
+    double *r64 = nullptr, *q64 = nullptr;   // refinement residual / operator output
+    PrecState<double> d;
+    PrecState<float> f;
+    std::vector<double> gx, gy;
+};
+
+}  // namespace iga
+
+using namespace iga;
+
+static void fem_1d(const std::vector<double> &g, std::vector<double> &kd, std::vector<double> &ko,
+                   std::vector<double> &md, std::vector<double> &mo)
+{
+    const int n = (int)g.size();
+    kd.assign(n, 0.0);
+    md.assign(n, 0.0);
+    ko.assign(n, 0.0);
+    mo.assign(n, 0.0);
+    for (int e = 0; e + 1 < n; ++e) {   // linear element [g_e, g_e+1], 2-point Gauss is exact
+        const double h = g[e + 1] - g[e];
+        kd[e] += 1.0 / h;
+        kd[e + 1] += 1.0 / h;
+        ko[e] = -1.0 / h;
+        md[e] += h / 3.0;
+        md[e + 1] += h / 3.0;
+        mo[e] = h / 6.0;
+    }
+}
+
+static std::vector<double> fem_nodes_1d(int p, int ne, double L)
+{
+    if (p >= 3) {   // matrix_free/preprocess_fem.cpp:38-60
+        std::vector<double> S;
+        const double h = L / (ne + 2);
+        for (int i = 0; i < p - 1; ++i) S.push_back(0.0);
+        for (int i = 1; i < ne + 2; ++i) S.push_back(i * h);
+        for (int i = 0; i < p - 1; ++i) S.push_back(L);
+        return greville(p - 2, S);
+    }
+    return greville(p, open_knots(p, ne, L));
+}
+
+// Lengths of the FEM grid: mean polyline length of the control-net rows
+// (x direction) and columns (y direction); 1 x 1 on the unit square.
+static void net_lengths(const Patch &P, double &Lx, double &Ly)
+{
+    double sx = 0.0, sy = 0.0;
+    for (int j = 0; j < P.n; ++j)
+        for (int i = 0; i + 1 < P.m; ++i) {
+            const size_t a = (size_t)j * P.m + i;
+            sx += std::hypot(P.CP[2 * (a + 1)] - P.CP[2 * a], P.CP[2 * (a + 1) + 1] - P.CP[2 * a + 1]);
+        }
+    for (int j = 0; j + 1 < P.n; ++j)
+        for (int i = 0; i < P.m; ++i) {
+            const size_t a = (size_t)j * P.m + i, b = a + P.m;
+            sy += std::hypot(P.CP[2 * b] - P.CP[2 * a], P.CP[2 * b + 1] - P.CP[2 * a + 1]);
+        }
+    Lx = sx / P.n;
+    Ly = sy / P.m;
+}
+
+#define SOLVE_TRY(call)                                                              \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess) {                                                     \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));          \
+            return e_ == cudaErrorMemoryAllocation ? IGA_ERR_NOMEM : IGA_ERR_CUDA;   \
+        }                                                                            \
+    } while (0)
+
+template <typename T>
+static int alloc_prec(PrecState<T> &ps, const iga_plan *pl, const SolverState &S)
+{
+    if (ps.ready) return IGA_OK;
+    const size_t N = (size_t)pl->nfunc;
+    std::vector<double> kd, ko, md, mo, ld, lo, nd, no;
+    fem_1d(S.gx, kd, ko, md, mo);
+    fem_1d(S.gy, ld, lo, nd, no);
+    auto up = [&](T **dst, const std::vector<double> &v) -> int {
+        std::vector<T> h(v.begin(), v.end());
+        SOLVE_TRY(cudaMalloc((void **)dst, sizeof(T) * h.size()));
+        SOLVE_TRY(cudaMemcpy(*dst, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+        return IGA_OK;
+    };
+    int st;
+    if ((st = up(&ps.kd, kd)) || (st = up(&ps.ko, ko)) || (st = up(&ps.md, md)) || (st = up(&ps.mo, mo)) ||
+        (st = up(&ps.ld, ld)) || (st = up(&ps.lo, lo)) || (st = up(&ps.nd, nd)) || (st = up(&ps.no, no)))
+        return st;
+    for (T **v : {&ps.x, &ps.r, &ps.z, &ps.zo, &ps.p, &ps.q, &ps.b, &ps.iz, &ps.ir, &ps.ip, &ps.iq})
+        SOLVE_TRY(cudaMalloc((void **)v, sizeof(T) * N));
+    ps.ready = true;
+    return IGA_OK;
+}
+
+static int ensure_state(iga_plan *pl, SolverState **out)
+{
+    if (pl->solver) {
+        *out = pl->solver;
+        return IGA_OK;
+    }
+    SolverState *S = new SolverState();
+    pl->solver = S;
+    S->device = pl->device;
+    SOLVE_TRY(cudaSetDevice(pl->device));
+    SOLVE_TRY(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+    SOLVE_TRY(cudaMalloc((void **)&S->s, sizeof(DevScalars)));
+    SOLVE_TRY(cudaMemset(S->s, 0, sizeof(DevScalars)));
+    SOLVE_TRY(cudaMallocHost((void **)&S->h, sizeof(DevScalars)));
+    SOLVE_TRY(cudaMalloc((void **)&S->partials, sizeof(double) * kRedBlocks * 4));
+    SOLVE_TRY(cudaMalloc((void **)&S->counter, sizeof(unsigned)));
+    SOLVE_TRY(cudaMemset(S->counter, 0, sizeof(unsigned)));
+    SOLVE_TRY(cudaMalloc((void **)&S->r64, sizeof(double) * pl->nfunc));
+    SOLVE_TRY(cudaMalloc((void **)&S->q64, sizeof(double) * pl->nfunc));
+    double Lx, Ly;
+    net_lengths(pl->patch, Lx, Ly);
+    S->gx = fem_nodes_1d(pl->p, pl->nex, Lx);
+    S->gy = fem_nodes_1d(pl->p, pl->ney, Ly);
+    *out = S;
+    return IGA_OK;
+}
+
+template <typename T>
+static void free_prec(PrecState<T> &ps)
+{
+    T *bufs[] = {ps.kd, ps.ko, ps.md, ps.mo, ps.ld, ps.lo, ps.nd, ps.no, ps.x, ps.r, ps.z, ps.zo, ps.p,
+                 ps.q, ps.b, ps.iz, ps.ir, ps.ip, ps.iq, ps.Vx, ps.Vy, ps.lx, ps.ly, ps.W1, ps.W2};
+    for (T *v : bufs)
+        if (v) cudaFree(v);
+    if (ps.chunk) cudaGraphExecDestroy(ps.chunk);
+    ps = PrecState<T>{};
+}
+
+void iga_solver_release(iga_plan *pl)
+{
+    SolverState *S = pl->solver;
+    if (!S) return;
+    cudaSetDevice(S->device);
+    free_prec(S->d);
+    free_prec(S->f);
+    for (void *v : {(void *)S->s, (void *)S->partials, (void *)S->counter, (void *)S->r64, (void *)S->q64})
+        if (v) cudaFree(v);
+    if (S->h) cudaFreeHost(S->h);
+    if (S->blas) cublasDestroy(S->blas);
+    if (S->stream) cudaStreamDestroy(S->stream);
+    delete S;
+    pl->solver = nullptr;
+}
+
+template <typename T>
+static FemCoef<T> coef_of(const PrecState<T> &ps, const iga_plan *pl)
+{
+    FemCoef<T> c = ps.coef();
+    c.m = pl->m;
+    c.n = pl->n;
+    return c;
+}
+
+template <typename T>
+static InnerCG<T> inner_of(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
+{
+    InnerCG<T> a;
+    a.z = ps.iz;
+    a.r = ps.ir;
+    a.p = ps.ip;
+    a.q = ps.iq;
+    a.rhs = nullptr;
+    a.c = coef_of(ps, pl);
+    a.s = S->s;
+    a.partials = S->partials;
+    a.counter = S->counter;
+    return a;
+}
+
+// One captured graph of kChunk inner iterations (3 kernels each, no-ops once done).
+template <typename T>
+static int inner_chunk_graph(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
+{
+    if (ps.chunk) return IGA_OK;
+    InnerCG<T> a = inner_of(ps, pl, S);
+    cudaGraph_t g;
+    SOLVE_TRY(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kChunk; ++k) {
+        icg_q_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(a);
+        icg_update_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(a);
+        icg_p_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(a);
+    }
+    SOLVE_TRY(cudaStreamEndCapture(S->stream, &g));
+    SOLVE_TRY(cudaGraphInstantiate(&ps.chunk, g, 0));
+    cudaGraphDestroy(g);
+    return IGA_OK;
+}
+
+static void interior_pencil(const std::vector<double> &g, std::vector<double> &Kd, std::vector<double> &Ko,
+                            std::vector<double> &Md, std::vector<double> &Mo)
+{
+    std::vector<double> kd, ko, md, mo;
+    fem_1d(g, kd, ko, md, mo);
+    const int n = (int)g.size() - 2;
+    Kd.assign(kd.begin() + 1, kd.begin() + 1 + n);
+    Md.assign(md.begin() + 1, md.begin() + 1 + n);
+    Ko.assign(ko.begin() + 1, ko.begin() + 1 + n);
+    Mo.assign(mo.begin() + 1, mo.begin() + 1 + n);
+}
+
+// Eigenpairs of the 1-D FEM pencils on the free nodes, built once per plan.
+static int fd_setup(PrecState<double> &, const iga_plan *pl, SolverState *S)
+{
+    (void)pl;
+    if (S->fd_host) return IGA_OK;
+    for (int dir = 0; dir < 2; ++dir) {
+        const std::vector<double> &g = dir == 0 ? S->gx : S->gy;
+        std::vector<double> Kd, Ko, Md, Mo;
+        interior_pencil(g, Kd, Ko, Md, Mo);
+        const int n = (int)Kd.size();
+        std::vector<double> &lam = dir == 0 ? S->lamx : S->lamy;
+        std::vector<double> &V = dir == 0 ? S->Vx : S->Vy;
+        lam.assign(n, 0.0);
+        V.assign((size_t)n * n, 0.0);
+        pencil_eig(n, Kd.data(), Ko.data(), Md.data(), Mo.data(), lam.data(), V.data());
+    }
+    S->fd_host = true;
+    return IGA_OK;
+}
+
+template <typename T>
+static int fd_upload(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
+{
+    if (ps.Vx) return IGA_OK;
+    PrecState<double> dummy;
+    fd_setup(dummy, pl, S);
+    const int nx = pl->m - 2, ny = pl->n - 2;
+    const int nxp = (nx + 63) / 64 * 64, nyp = (ny + 63) / 64 * 64;
+    ps.nxp = nxp;
+    ps.nyp = nyp;
+    // zero-padded eigenvector matrices; padded eigenvalues 1 keep the scaling finite
+    auto up_mat = [&](T **dst, const std::vector<double> &V, int n, int np) -> int {
+        std::vector<T> h((size_t)np * np, T(0));
+        for (int k = 0; k < n; ++k)
+            for (int i = 0; i < n; ++i) h[(size_t)k * np + i] = (T)V[(size_t)k * n + i];
+        SOLVE_TRY(cudaMalloc((void **)dst, sizeof(T) * h.size()));
+        SOLVE_TRY(cudaMemcpy(*dst, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+        return IGA_OK;
+    };
+    auto up_vec = [&](T **dst, const std::vector<double> &v, int np) -> int {
+        std::vector<T> h(np, T(1));
+        for (size_t i = 0; i < v.size(); ++i) h[i] = (T)v[i];
+        SOLVE_TRY(cudaMalloc((void **)dst, sizeof(T) * h.size()));
+        SOLVE_TRY(cudaMemcpy(*dst, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+        return IGA_OK;
+    };
+    int st;
+    if ((st = up_mat(&ps.Vx, S->Vx, nx, nxp)) || (st = up_mat(&ps.Vy, S->Vy, ny, nyp)) ||
+        (st = up_vec(&ps.lx, S->lamx, nxp)) || (st = up_vec(&ps.ly, S->lamy, nyp)))
+        return st;
+    SOLVE_TRY(cudaMalloc((void **)&ps.W1, sizeof(T) * (size_t)nxp * nyp));
+    SOLVE_TRY(cudaMalloc((void **)&ps.W2, sizeof(T) * (size_t)nxp * nyp));
+    if (!S->blas) {
+        if (cublasCreate(&S->blas) != CUBLAS_STATUS_SUCCESS) {
+            set_error("cublasCreate failed");
+            return IGA_ERR_CUDA;
+        }
+    }
+    return IGA_OK;
+}
+
+static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
+                           const double *A, int lda, const double *B, int ldb, double *C, int ldc)
+{
+    const double one = 1.0, zero = 0.0;
+    return cublasDgemm(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc);
+}
+
+// FP32 preconditioner GEMMs run on the TF32 tensor cores: the preconditioner
+// only has to be a close SPD approximation of K_fem^-1.
+static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
+                           const float *A, int lda, const float *B, int ldb, float *C, int ldc)
+{
+    const float one = 1.0f, zero = 0.0f;
+    return cublasGemmEx(h, ta, tb, m, n, k, &one, A, CUDA_R_32F, lda, B, CUDA_R_32F, ldb, &zero, C, CUDA_R_32F, ldc,
+                        CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT);
+}
+
+// z = K_fem^-1 r: Z = Vx [(Vx^T R Vy) ./ (lx_a + ly_b)] Vy^T on the free nodes
+// (R, Z: the interior blocks of r, z, zero-padded to multiples of 64 so the
+// GEMMs run with aligned leading dimensions).
+template <typename T>
+static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const T *r, T *z)
+{
+    const int m = pl->m, n = pl->n, nx = m - 2, ny = n - 2;
+    boundary_copy_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(z, r, m, n);
+    if (nx <= 0 || ny <= 0) return IGA_OK;
+    const int nxp = ps.nxp, nyp = ps.nyp;
+    cublasSetStream(S->blas, S->stream);
+    fd_gather_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(r, ps.W2, m, nx, ny, nxp, nyp);
+    cublasStatus_t e = gemm(S->blas, CUBLAS_OP_T, CUBLAS_OP_N, nxp, nyp, nxp, ps.Vx, nxp, ps.W2, nxp, ps.W1, nxp);
+    if (e == CUBLAS_STATUS_SUCCESS)
+        e = gemm(S->blas, CUBLAS_OP_N, CUBLAS_OP_N, nxp, nyp, nyp, ps.W1, nxp, ps.Vy, nyp, ps.W2, nxp);
+    if (e == CUBLAS_STATUS_SUCCESS)
+        fd_scale_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(ps.W2, ps.lx, ps.ly, nxp, nyp);
+    if (e == CUBLAS_STATUS_SUCCESS)
+        e = gemm(S->blas, CUBLAS_OP_N, CUBLAS_OP_N, nxp, nyp, nxp, ps.Vx, nxp, ps.W2, nxp, ps.W1, nxp);
+    if (e == CUBLAS_STATUS_SUCCESS)
+        e = gemm(S->blas, CUBLAS_OP_N, CUBLAS_OP_T, nxp, nyp, nyp, ps.W1, nxp, ps.Vy, nyp, ps.W2, nxp);
+    if (e != CUBLAS_STATUS_SUCCESS) {
+        set_error("cuBLAS GEMM failed in the FEM preconditioner");
+        return IGA_ERR_CUDA;
+    }
+    fd_scatter_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(ps.W2, z, m, nx, ny, nxp);
+    return IGA_OK;
+}
+
+// z = M^-1 r for the configured preconditioner.
+template <typename T>
+static int pc_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const iga_solve_opts &o, const T *r, T *z,
+                    double pc_rtol, int64_t &pc_iters)
+{
+    const long long N = pl->nfunc;
+    if (o.pc == IGA_PC_NONE) {
+        copy_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(z, r, N);
+        return IGA_OK;
+    }
+    int st;
+    if (o.pc == IGA_PC_FEM_EXACT) {
+        if ((st = fd_upload(ps, pl, S))) return st;
+        return fd_apply(ps, pl, S, r, z);
+    }
+    if ((st = inner_chunk_graph(ps, pl, S))) return st;
+    InnerCG<T> a = inner_of(ps, pl, S);
+    icg_init_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(a, r, pc_rtol, o.pc_max_it);
+    // Keep one chunk in flight ahead of the completion check.
+    SOLVE_TRY(cudaGraphLaunch(ps.chunk, S->stream));
+    int launched = 1;
+    for (;;) {
+        SOLVE_TRY(cudaMemcpyAsync(S->h, S->s, sizeof(DevScalars), cudaMemcpyDeviceToHost, S->stream));
+        cudaEvent_t ev;
+        SOLVE_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        SOLVE_TRY(cudaEventRecord(ev, S->stream));
+        if ((long long)launched * kChunk < (long long)o.pc_max_it + kChunk) {
+            SOLVE_TRY(cudaGraphLaunch(ps.chunk, S->stream));
+            ++launched;
+        }
+        SOLVE_TRY(cudaEventSynchronize(ev));
+        cudaEventDestroy(ev);
+        if (S->h->idone) break;
+        if ((long long)launched * kChunk >= (long long)o.pc_max_it + 2 * kChunk) break;
+    }
+    SOLVE_TRY(cudaStreamSynchronize(S->stream));
+    pc_iters += S->h->iiters;
+    if (S->h->ibreak) return IGA_ERR_BREAKDOWN;
+    copy_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(z, ps.iz, N);
+    return IGA_OK;
+}
+
+static int sync_scalars(SolverState *S)
+{
+    SOLVE_TRY(cudaMemcpyAsync(S->h, S->s, sizeof(DevScalars), cudaMemcpyDeviceToHost, S->stream));
+    SOLVE_TRY(cudaStreamSynchronize(S->stream));
+    return IGA_OK;
+}
+
+// Flexible PCG on K x = b in precision T, from the current x; stops when the
+// recurrence residual satisfies ||r|| <= rtol ||b_ref||. Returns iterations.
+template <typename T>
+static int pcg(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_solve_opts &o, const T *b, T *x, double rtol,
+               double bnorm, double pc_rtol, int prec, int &its, int64_t &pc_iters)
+{
+    const long long N = pl->nfunc;
+    const cudaStream_t s = S->stream;
+    int st;
+    // r = b - K x, rr = r.r
+    if ((st = iga_apply_internal_sb(pl, prec, x, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY))) return st;
+    sub_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(b, ps.q, ps.r, N, S->s, S->partials, S->counter);
+    if ((st = sync_scalars(S))) return st;
+    if (std::sqrt(S->h->rr) <= rtol * bnorm) return IGA_OK;
+    if ((st = pc_apply(ps, pl, S, o, ps.r, ps.z, pc_rtol, pc_iters))) return st;
+    dot_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, N, &S->s->rz, S->partials, S->counter);
+    pcg_p_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.z, N, S->s, 1);
+    cudaMemsetAsync(&S->s->breakdown, 0, sizeof(int), s);
+    for (int it = 0; it < o.max_it; ++it) {
+        if ((st = iga_apply_internal_sb(pl, prec, ps.p, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY))) return st;
+        pcg_pq_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.q, N, S->s, S->partials, S->counter);
+        pcg_xr_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(x, ps.r, ps.p, ps.q, N, S->s, S->partials, S->counter);
+        ++its;
+        if ((st = sync_scalars(S))) return st;
+        if (S->h->breakdown) return IGA_ERR_BREAKDOWN;
+        if (!std::isfinite(S->h->rr)) return IGA_ERR_NONFINITE;
+        if (std::sqrt(S->h->rr) <= rtol * bnorm) return IGA_OK;
+        std::swap(ps.z, ps.zo);
+        if ((st = pc_apply(ps, pl, S, o, ps.r, ps.z, pc_rtol, pc_iters))) return st;
+        pcg_beta_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, ps.zo, N, S->s, S->partials, S->counter);
+        pcg_p_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.z, N, S->s, 0);
+    }
+    return IGA_ERR_NOT_CONVERGED;
+}
+
+// ||b - K x|| (FP64 operator), into S->h->rr and S->h->bb.
+static int true_residual(iga_plan *pl, SolverState *S, const double *b, const double *x)
+{
+    int st;
+    if ((st = iga_apply_internal_sb(pl, IGA_FP64, x, S->q64, S->stream, IGA_SIGN_SPD, IGA_BC_IDENTITY))) return st;
+    residual_kernel<<<kRedBlocks, kThreads, 0, S->stream>>>(b, S->q64, S->r64, pl->nfunc, S->s, S->partials,
+                                                          S->counter);
+    return sync_scalars(S);
+}
+
+extern "C" {
+
+void iga_solve_opts_default(iga_solve_opts *o)
+{
+    if (!o) return;
+    o->precision = IGA_FP64;
+    o->pc = IGA_PC_FEM_CG;
+    o->rtol = 1e-10;
+    o->max_it = 10000;
+    o->pc_rtol = 1e-10;
+    o->pc_max_it = 10000;
+    o->sweep_rtol = 1e-5;
+    o->max_sweeps = 10;
+    o->x0_nonzero = 0;
+}
+
+int iga_fem_nodes(const iga_plan *pl, double *gx, double *gy)
+{
+    if (!pl || !gx || !gy) return IGA_ERR_ARG;
+    double Lx, Ly;
+    net_lengths(pl->patch, Lx, Ly);
+    const std::vector<double> a = fem_nodes_1d(pl->p, pl->nex, Lx), b = fem_nodes_1d(pl->p, pl->ney, Ly);
+    std::memcpy(gx, a.data(), a.size() * sizeof(double));
+    std::memcpy(gy, b.data(), b.size() * sizeof(double));
+    return IGA_OK;
+}
+
+int iga_pc_apply(iga_plan *pl, int pc, int prec, const void *r, void *z, double pc_rtol, int pc_max_it,
+                 void *stream)
+{
+    if (!pl || !r || !z || (prec != IGA_FP64 && prec != IGA_FP32)) return IGA_ERR_ARG;
+    if (pc != IGA_PC_NONE && pc != IGA_PC_FEM_CG && pc != IGA_PC_FEM_EXACT) return IGA_ERR_ARG;
+    SolverState *S;
+    int st;
+    if ((st = ensure_state(pl, &S))) return st;
+    cudaEvent_t ev;
+    SOLVE_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    SOLVE_TRY(cudaEventRecord(ev, (cudaStream_t)stream));
+    SOLVE_TRY(cudaStreamWaitEvent(S->stream, ev, 0));
+    iga_solve_opts o;
+    iga_solve_opts_default(&o);
+    o.pc = pc;
+    o.pc_max_it = pc_max_it;
+    int64_t its = 0;
+    if (prec == IGA_FP64) {
+        if ((st = alloc_prec(S->d, pl, *S))) return st;
+        st = pc_apply<double>(S->d, pl, S, o, (const double *)r, (double *)z, pc_rtol, its);
+    } else {
+        if ((st = alloc_prec(S->f, pl, *S))) return st;
+        st = pc_apply<float>(S->f, pl, S, o, (const float *)r, (float *)z, pc_rtol, its);
+    }
+    SOLVE_TRY(cudaEventRecord(ev, S->stream));
+    SOLVE_TRY(cudaStreamWaitEvent((cudaStream_t)stream, ev, 0));
+    cudaEventDestroy(ev);
+    return st;
+}
+
+int iga_fem_apply(iga_plan *pl, int prec, const void *x, void *y, void *stream)
+{
+    if (!pl || !x || !y) return IGA_ERR_ARG;
+    SolverState *S;
+    int st;
+    if ((st = ensure_state(pl, &S))) return st;
+    if (prec == IGA_FP64) {
+        if ((st = alloc_prec(S->d, pl, *S))) return st;
+        fem_apply_kernel<double><<<kRedBlocks, kThreads, 0, (cudaStream_t)stream>>>(
+            (const double *)x, (double *)y, coef_of(S->d, pl));
+    } else if (prec == IGA_FP32) {
+        if ((st = alloc_prec(S->f, pl, *S))) return st;
+        fem_apply_kernel<float><<<kRedBlocks, kThreads, 0, (cudaStream_t)stream>>>((const float *)x, (float *)y,
+                                                                                 coef_of(S->f, pl));
+    } else {
+        return IGA_ERR_ARG;
+    }
+    SOLVE_TRY(cudaGetLastError());
+    return IGA_OK;
+}
+
+int iga_fem_assemble_csr(iga_plan *pl, int sign, int32_t *rowptr, int32_t *col, double *val, int64_t *nnz,
+                         void *stream)
+{
+    if (!pl || (sign != 1 && sign != -1)) return IGA_ERR_ARG;
+    const int m = pl->m, n = pl->n;
+    // Row lengths: 1 on the boundary, (free neighbours in x) * (free neighbours in y) inside.
+    auto cnt = [](int i, int mm) { return 1 + (i - 1 >= 1) + (i + 1 <= mm - 2); };
+    std::vector<int32_t> rp((size_t)m * n + 1);
+    long long acc = 0;
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) {
+            rp[(size_t)j * m + i] = (int32_t)acc;
+            const bool b = i == 0 || j == 0 || i == m - 1 || j == n - 1;
+            acc += b ? 1 : cnt(i, m) * cnt(j, n);
+        }
+    rp[(size_t)m * n] = (int32_t)acc;
+    if (acc > INT32_MAX) return IGA_ERR_UNSUPPORTED;
+    if (nnz) *nnz = acc;
+    if (!rowptr && !col && !val) return IGA_OK;
+    if (!rowptr || !col || !val) return IGA_ERR_ARG;
+    SolverState *S;
+    int st;
+    if ((st = ensure_state(pl, &S))) return st;
+    if ((st = alloc_prec(S->d, pl, *S))) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    SOLVE_TRY(cudaMemcpyAsync(rowptr, rp.data(), rp.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    fem_csr_kernel<<<kRedBlocks, kThreads, 0, s>>>(rowptr, col, val, coef_of(S->d, pl), (double)sign);
+    SOLVE_TRY(cudaStreamSynchronize(s));
+    return IGA_OK;
+}
+
+int iga_solve(iga_plan *pl, const double *b, double *x, const iga_solve_opts *o_in, iga_solve_stats *stats,
+              void *stream)
+{
+    if (!pl || !b || !x) return IGA_ERR_ARG;
+    iga_solve_opts o;
+    iga_solve_opts_default(&o);
+    if (o_in) o = *o_in;
+    if (o.pc != IGA_PC_NONE && o.pc != IGA_PC_FEM_CG && o.pc != IGA_PC_FEM_EXACT) {
+        set_error("unknown preconditioner");
+        return IGA_ERR_ARG;
+    }
+    if (!pl->op64.ready) {
+        set_error("iga_solve needs the FP64 operator (plan precision IGA_FP64 or IGA_MIXED)");
+        return IGA_ERR_ARG;
+    }
+    if (o.precision == IGA_MIXED && !pl->op32.ready) {
+        set_error("IGA_MIXED solves need a plan created with precision IGA_MIXED");
+        return IGA_ERR_ARG;
+    }
+    SolverState *S;
+    int st;
+    if ((st = ensure_state(pl, &S))) return st;
+    SOLVE_TRY(cudaSetDevice(pl->device));
+    const auto t0 = std::chrono::steady_clock::now();
+    // Order the solve after the caller's stream and the caller's stream after the solve.
+    cudaEvent_t ev;
+    SOLVE_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    SOLVE_TRY(cudaEventRecord(ev, (cudaStream_t)stream));
+    SOLVE_TRY(cudaStreamWaitEvent(S->stream, ev, 0));
+    const long long N = pl->nfunc;
+    iga_solve_stats stt{};
+    if (!o.x0_nonzero) zero_kernel<double><<<kRedBlocks, kThreads, 0, S->stream>>>(x, N);
+    if ((st = true_residual(pl, S, b, x))) return st;
+    if (!std::isfinite(S->h->bb) || !std::isfinite(S->h->rr)) {
+        cudaEventDestroy(ev);
+        if (stats) {
+            *stats = iga_solve_stats{};
+            stats->status = IGA_ERR_NONFINITE;
+            stats->relres = NAN;
+        }
+        set_error("non-finite value in b or in the initial residual");
+        return IGA_ERR_NONFINITE;
+    }
+    const double bnorm = std::sqrt(S->h->bb);
+    double rel = bnorm > 0 ? std::sqrt(S->h->rr) / bnorm : 0.0;
+    int result = IGA_OK;
+    if (o.precision == IGA_FP64) {
+        if ((st = alloc_prec(S->d, pl, *S))) return st;
+        // Restart from the true residual until it meets rtol (recurrence drift).
+        for (int restart = 0; restart < 4 && rel > o.rtol; ++restart) {
+            st = pcg<double>(pl, S, S->d, o, b, x, o.rtol, bnorm, o.pc_rtol, IGA_FP64, stt.iterations,
+                             stt.pc_iterations);
+            if (st && st != IGA_ERR_NOT_CONVERGED) {
+                result = st;
+                break;
+            }
+            if ((st = true_residual(pl, S, b, x))) return st;
+            rel = std::sqrt(S->h->rr) / bnorm;
+            if (!std::isfinite(rel)) {
+                result = IGA_ERR_NONFINITE;
+                break;
+            }
+        }
+    } else {
+        if ((st = alloc_prec(S->f, pl, *S))) return st;
+        for (int sw = 0; sw < o.max_sweeps && rel > o.rtol; ++sw) {
+            // rhs of the sweep: r64 / ||r64|| in FP32; correction d solves K d = r / ||r||.
+            const double scale = std::sqrt(S->h->rr);
+            scale_down_kernel<<<kRedBlocks, kThreads, 0, S->stream>>>(S->r64, S->f.b, N, S->s);
+            zero_kernel<float><<<kRedBlocks, kThreads, 0, S->stream>>>(S->f.x, N);
+            st = pcg<float>(pl, S, S->f, o, S->f.b, S->f.x, o.sweep_rtol, 1.0, o.pc_rtol, IGA_FP32, stt.iterations,
+                            stt.pc_iterations);
+            if (st && st != IGA_ERR_NOT_CONVERGED) {
+                result = st;
+                break;
+            }
+            refine_update_kernel<<<kRedBlocks, kThreads, 0, S->stream>>>(x, S->f.x, N, scale);
+            ++stt.sweeps;
+            if ((st = true_residual(pl, S, b, x))) return st;
+            rel = std::sqrt(S->h->rr) / bnorm;
+            if (!std::isfinite(rel)) {
+                result = IGA_ERR_NONFINITE;
+                break;
+            }
+        }
+    }
+    SOLVE_TRY(cudaEventRecord(ev, S->stream));
+    SOLVE_TRY(cudaStreamWaitEvent((cudaStream_t)stream, ev, 0));
+    SOLVE_TRY(cudaStreamSynchronize(S->stream));
+    cudaEventDestroy(ev);
+    stt.relres = rel;
+    if (result == IGA_OK && !(rel <= o.rtol)) result = IGA_ERR_NOT_CONVERGED;
+    stt.status = result;
+    stt.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (stats) *stats = stt;
+    return result;
+}
+
+}  // extern "C"

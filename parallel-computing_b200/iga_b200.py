@@ -49,6 +49,19 @@ class PlanInfo(ctypes.Structure):
                 ("rows_per_strip", ctypes.c_int), ("warps_per_cta", ctypes.c_int)]
 
 
+class SolveOpts(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("pc", ctypes.c_int), ("rtol", ctypes.c_double),
+                ("max_it", ctypes.c_int), ("pc_rtol", ctypes.c_double), ("pc_max_it", ctypes.c_int),
+                ("sweep_rtol", ctypes.c_double), ("max_sweeps", ctypes.c_int), ("x0_nonzero", ctypes.c_int)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("iterations", ctypes.c_int), ("pc_iterations", ctypes.c_int64),
+                ("sweeps", ctypes.c_int), ("relres", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
+PC_NONE, PC_FEM_CG, PC_FEM_EXACT = 0, 1, 2
+
 _LIB = None
 
 # (name, restype, argtypes) of every exported C entry point.
@@ -68,6 +81,12 @@ SIGNATURES = [
     ("iga_MatrixFreeMatMultCUDA", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 15),
     ("iga_MatrixFreeMatMultCUDA_release", ctypes.c_int, []),
     ("iga_MatrixFreeMatMultCUDA_noalloc", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 16),
+    ("iga_solve_opts_default", None, [ctypes.POINTER(SolveOpts)]),
+    ("iga_solve", ctypes.c_int, [VP, VP, VP, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveStats), VP]),
+    ("iga_fem_apply", ctypes.c_int, [VP, ctypes.c_int, VP, VP, VP]),
+    ("iga_fem_assemble_csr", ctypes.c_int, [VP, ctypes.c_int, VP, VP, VP, ctypes.POINTER(ctypes.c_int64), VP]),
+    ("iga_fem_nodes", ctypes.c_int, [VP, VP, VP]),
+    ("iga_pc_apply", ctypes.c_int, [VP, ctypes.c_int, ctypes.c_int, VP, VP, ctypes.c_double, ctypes.c_int, VP]),
 ]
 
 
@@ -198,3 +217,41 @@ class Plan:
     def rhs(self, F, fkind=F_REFERENCE, stream=None):
         _check(_lib().iga_rhs(self.h, fkind, _ptr(F), _stream(stream)), "iga_rhs")
         return F
+
+    def solve(self, b, x, stream=None, check=True, **kw):
+        """Solve K x = b (SPD form) on the device; keyword arguments set iga_solve_opts fields."""
+        o = SolveOpts()
+        _lib().iga_solve_opts_default(ctypes.byref(o))
+        for k, v in kw.items():
+            setattr(o, k, v)
+        st = SolveStats()
+        status = _lib().iga_solve(self.h, _ptr(b), _ptr(x), ctypes.byref(o), ctypes.byref(st), _stream(stream))
+        if check:
+            _check(status, "iga_solve")
+        return st
+
+    def fem_apply(self, x, y, precision=FP64, stream=None):
+        _check(_lib().iga_fem_apply(self.h, precision, _ptr(x), _ptr(y), _stream(stream)), "iga_fem_apply")
+
+    def pc_apply(self, r, z, pc=PC_FEM_EXACT, precision=FP64, pc_rtol=1e-10, pc_max_it=10000, stream=None):
+        _check(_lib().iga_pc_apply(self.h, pc, precision, _ptr(r), _ptr(z), pc_rtol, pc_max_it, _stream(stream)),
+               "iga_pc_apply")
+
+    def fem_nodes(self):
+        gx = np.empty(self.mesh["nex"] + self.mesh["p"])
+        gy = np.empty(self.mesh["ney"] + self.mesh.get("q", self.mesh["p"]))
+        _check(_lib().iga_fem_nodes(self.h, _ptr(gx), _ptr(gy)), "iga_fem_nodes")
+        return gx, gy
+
+    def fem_csr(self, sign=-1):
+        """Device CSR of the FEM preconditioner matrix, returned as host numpy (rowptr, col, val)."""
+        import torch
+        nnz = ctypes.c_int64()
+        _check(_lib().iga_fem_assemble_csr(self.h, sign, None, None, None, ctypes.byref(nnz), None), "csr nnz")
+        rp = torch.empty(self.nfunc + 1, dtype=torch.int32, device="cuda")
+        col = torch.empty(nnz.value, dtype=torch.int32, device="cuda")
+        val = torch.empty(nnz.value, dtype=torch.float64, device="cuda")
+        _check(_lib().iga_fem_assemble_csr(self.h, sign, _ptr(rp), _ptr(col), _ptr(val), ctypes.byref(nnz), None),
+               "iga_fem_assemble_csr")
+        torch.cuda.synchronize()
+        return rp.cpu().numpy(), col.cpu().numpy(), val.cpu().numpy()
