@@ -207,6 +207,52 @@ def reference_arm(args):
     print(json.dumps(out), flush=True)
 
 
+def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
+    """Time-to-solution of K u = F (f = 2 pi^2 sin(pi x) sin(pi y)) to a relative
+    true residual of 1e-10: plain FP64 PCG vs FP32 PCG sweeps + FP64 refinement,
+    both with the FEM preconditioner inverted exactly; plus the reference's
+    preconditioner (inner Jacobi-CG to 1e-10) on the p=2 64x64 configuration."""
+    out = {"problem": f"p=3 {ne}x{ne}, f=2pi^2 sin(pi x) sin(pi y), K u = F, rtol 1e-10 (true residual)",
+           "pc": "bilinear-FEM matrix, exact inverse (tensor-product fast diagonalisation; FP64 DGEMM / FP32 TF32)"}
+    plan = ib.Plan(mesh, precision=ib.MIXED)
+    b = torch.empty(plan.nfunc, dtype=torch.float64, device="cuda")
+    plan.rhs(b, ib.F_SINSIN)
+    stream = torch.cuda.current_stream()
+    for name, kw in (("fp64", dict(pc=ib.PC_FEM_EXACT)),
+                     ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED))):
+        x = torch.zeros_like(b)
+        plan.solve(b, x, **kw)   # warm-up: eigen-decomposition, cuBLAS, allocations
+        times, st = [], None
+        for _ in range(3):
+            x.zero_()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = plan.solve(b, x, stream=stream, **kw)
+            e1.record(stream)
+            barrier()
+            times.append(max_over_ranks(e0.elapsed_time(e1) / 1e3))
+        out[name] = {"seconds": statistics.median(times), "iterations": st.iterations, "sweeps": st.sweeps,
+                     "relres": st.relres}
+    out["speedup_fp32_refine_vs_fp64"] = out["fp64"]["seconds"] / out["fp32_refine"]["seconds"]
+    plan.close()
+    # reference preconditioner, p=2 64x64 (the CPU-runnable configuration)
+    m2 = ib.unit_square(2, 64)
+    p2 = ib.Plan(m2)
+    b2 = torch.empty(p2.nfunc, dtype=torch.float64, device="cuda")
+    p2.rhs(b2, ib.F_SINSIN)
+    x2 = torch.zeros_like(b2)
+    p2.solve(b2, x2, pc=ib.PC_FEM_CG)
+    x2.zero_()
+    st = p2.solve(b2, x2, pc=ib.PC_FEM_CG)
+    out["p2_64x64_reference_pc"] = {"seconds": st.seconds, "iterations": st.iterations,
+                                    "inner_iterations": st.pc_iterations, "relres": st.relres,
+                                    "pc": "inner Jacobi-CG on the FEM matrix to 1e-10 (the reference's PCSHELL)"}
+    p2.close()
+    torch.cuda.empty_cache()
+    return out
+
+
 # --------------------------------------------------------------- our arm
 def our_arm(args):
     import torch
@@ -308,6 +354,13 @@ def our_arm(args):
         e2e = {"value": ws * N * k_e2e / t_e2e / 1e9, "unit": "GDOF/s", "h2d_bytes_per_step": 8 * N,
                "d2h_bytes_per_step": 8 * N, "call": "iga_apply_host (MATSHELL MatMult on host vectors)"}
 
+    solve = None
+    if not args.skip_solve:
+        plan.close()
+        torch.cuda.empty_cache()
+        solve = time_solves(ib, torch, mesh, ne, barrier, max_over_ranks)
+        plan = ib.Plan(mesh, geometry=ib.GEOM_PRECOMPUTED)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         rate, kind, threads, t = cpu_reference_apply_rate(256, 3, os.cpu_count() or 1)
@@ -330,7 +383,7 @@ def our_arm(args):
                             "kernel": "apply_kernel + seam_fixup_kernel (one MatMult)",
                             "algo_bytes_per_launch": algo},
                "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": 2 * args.steps,
-               "variants": variants}
+               "variants": variants, "solve": solve}
         print(json.dumps(out), flush=True)
     plan.close()
     if dist is not None:
@@ -348,6 +401,7 @@ def main():
     ap.add_argument("--ne", type=int, default=NE, help="elements per direction (profiling runs use smaller cases)")
     ap.add_argument("--skip-variants", action="store_true", help="skip the on-the-fly-geometry timing")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer timing")
+    ap.add_argument("--skip-solve", action="store_true", help="skip the time-to-1e-10 solves")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
