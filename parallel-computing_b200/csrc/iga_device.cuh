@@ -70,7 +70,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
     return false;
 }
 
-// cp.async (LDGSTS) of 4 or 8 bytes with zero fill when `valid` is false.
+// cp.async (LDGSTS) of 4, 8 or 16 bytes with zero fill when `valid` is false.
 template <int BYTES>
 __device__ __forceinline__ void cp_async_zfill(void *dst, const void *src, bool valid)
 {
@@ -86,7 +86,10 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // ---------------------------------------------------------------- strips
-// The element grid is cut into warp strips of 32 element columns by TY
+// Element columns per warp strip (two lanes per element column).
+constexpr int kSW = 16;
+
+// The element grid is cut into warp strips of kSW element columns by TY
 // element rows (nominal sizes; strips that overhang the mesh are padded with
 // empty elements). A control-point row R (or column C) is covered by the
 // strips whose element range, widened by p to the right/top, contains it:
@@ -100,7 +103,7 @@ struct StripGrid {
     int FS;         // frame slots per strip
 };
 
-__host__ __device__ __forceinline__ int frame_size(int P, int TY) { return 2 * P * (TY + P) + 2 * P * (32 - P); }
+__host__ __device__ __forceinline__ int frame_size(int P, int TY) { return 2 * P * (TY + P) + 2 * P * (kSW - P); }
 
 // Number of strips covering coordinate c along a direction of strip width w
 // with NS strips, and the first (lowest) of them.
@@ -114,13 +117,13 @@ __host__ __device__ __forceinline__ int cover(int c, int w, int NS, int P, int &
 }
 
 // Slot of footprint position (lr, lc) in a strip's frame (only positions that
-// can be covered by another strip: lc < P, lc >= 32, lr < P or lr >= TY).
+// can be covered by another strip: lc < P, lc >= kSW, lr < P or lr >= TY).
 __host__ __device__ __forceinline__ int frame_index(int lr, int lc, int P, int TY)
 {
     if (lc < P) return lr * P + lc;
-    if (lc >= 32) return P * (TY + P) + lr * P + (lc - 32);
-    if (lr < P) return 2 * P * (TY + P) + lr * (32 - P) + (lc - P);
-    return 2 * P * (TY + P) + P * (32 - P) + (lr - TY) * (32 - P) + (lc - P);
+    if (lc >= kSW) return P * (TY + P) + lr * P + (lc - kSW);
+    if (lr < P) return 2 * P * (TY + P) + lr * (kSW - P) + (lc - P);
+    return 2 * P * (TY + P) + P * (kSW - P) + (lr - TY) * (kSW - P) + (lc - P);
 }
 
 }  // namespace iga

@@ -60,24 +60,24 @@ __global__ void noalloc_tables_kernel(double *__restrict__ tabX, double *__restr
                                       const double *__restrict__ qw1, const double *__restrict__ qw2, int P,
                                       int nex, int ney, int NSX)
 {
-    const int NB = P + 1, NQ = P + 1;
-    const long long nX = (long long)NSX * 2 * NQ * NB * 32;
+    const int NB = P + 1, NQ = P + 1, QH = (NQ + 1) / 2;
+    const long long nX = (long long)NSX * 2 * QH * NB * 32;
     const long long nY = (long long)ney * 2 * NQ * NB;
     const long long tid0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (tid0 == 0) *err = 0;
     for (long long t = tid0; t < nX + nY + NQ * NQ; t += (long long)gridDim.x * blockDim.x) {
-        if (t < nX) {   // [gx][kind][qx][il][lane]
+        if (t < nX) {   // [gx][kind][j][il][lane]: lane 2c+h = column 16 gx + c, qx = h QH + j
             const int lane = (int)(t % 32);
             long long r = t / 32;
             const int il = (int)(r % NB);
             r /= NB;
-            const int qx = (int)(r % NQ);
-            r /= NQ;
+            const int j = (int)(r % QH);
+            r /= QH;
             const int kind = (int)(r % 2);
             const int gx = (int)(r / 2);
-            const int ex = 32 * gx + lane;
+            const int ex = iga::kSW * gx + lane / 2, qx = (lane % 2) * QH + j;
             double v = 0.0;
-            if (ex < nex) {
+            if (ex < nex && qx < NQ) {
                 const double *Ce = C1 + (size_t)ex * NB * NB + il * NB;
                 const double *Bq = (kind ? dB1 : B1) + qx * NB;
                 for (int k = 0; k < NB; ++k) v += Ce[k] * Bq[k];
@@ -111,13 +111,13 @@ size_t up256(size_t v) { return (v + 255) & ~size_t(255); }
 
 Layout layout_for(int P, int nex, int ney, int TY)
 {
-    const int NB = P + 1, NQ = P + 1;
-    const long long NSX = (nex + 31) / 32, NSY = (ney + TY - 1) / TY;
+    const int NB = P + 1, NQ = P + 1, QH = (NQ + 1) / 2;
+    const long long NSX = (nex + iga::kSW - 1) / iga::kSW, NSY = (ney + TY - 1) / TY;
     Layout L;
     L.off_err = 0;
     L.off_wq = 256;
     L.off_tabX = L.off_wq + up256(sizeof(double) * NQ * NQ);
-    L.off_tabY = L.off_tabX + up256(sizeof(double) * NSX * 2 * NQ * NB * 32);
+    L.off_tabY = L.off_tabX + up256(sizeof(double) * NSX * 2 * QH * NB * 32);
     L.off_frame = L.off_tabY + up256(sizeof(double) * (size_t)ney * 2 * NQ * NB);
     L.total = L.off_frame + up256(sizeof(double) * NSX * NSY * iga::frame_size(P, TY));
     return L;
@@ -128,9 +128,9 @@ int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int 
            const double *d_in, double *d_out, cudaStream_t s)
 {
     using namespace iga;
-    int W = 8;
-    while (W > 1 && apply_smem_bytes<P, double, 2>(W) > 220 * 1024) --W;
-    const size_t smem = apply_smem_bytes<P, double, 2>(W);
+    int W = apply_max_threads<P, double, 1>() / 32;
+    while (W > 1 && apply_smem_bytes<P, double, 1, 2>(W) > 220 * 1024) --W;
+    const size_t smem = apply_smem_bytes<P, double, 1, 2>(W);
     auto kern = apply_kernel<P, double, 1, 2>;
     {
         std::lock_guard<std::mutex> lk(g_mu);
@@ -146,7 +146,7 @@ int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int 
     g.nex = nex;
     g.ney = ney;
     g.TY = TY;
-    g.NSX = (nex + 31) / 32;
+    g.NSX = (nex + kSW - 1) / kSW;
     g.NSY = (ney + TY - 1) / TY;
     g.P = P;
     g.FS = frame_size(P, TY);
@@ -207,7 +207,7 @@ extern "C" int iga_MatrixFreeMatMultCUDA_noalloc(int p, int q, int nex, int ney,
         return IGA_ERR_CUDA;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    const int NSX = (nex + 31) / 32;
+    const int NSX = (nex + iga::kSW - 1) / iga::kSW;
     noalloc_tables_kernel<<<148, 256, 0, s>>>(
         reinterpret_cast<double *>(base + Ly.off_tabX), reinterpret_cast<double *>(base + Ly.off_tabY),
         reinterpret_cast<double *>(base + Ly.off_wq), reinterpret_cast<int *>(base + Ly.off_err), d_B1, d_dB1, d_B2,

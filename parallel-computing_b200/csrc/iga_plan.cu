@@ -19,7 +19,7 @@ namespace iga {
 // ---------------------------------------------------------------- setup kernels
 // Precomputed geometry (the mult_sf path): G = w kappa det(J) J^-1 J^-T at
 // every quadrature point, in the order apply_kernel streams it:
-// [gx][gy][s][qp][3][lane]. Padding elements get G = 0.
+// [strip][row][qy][qx][3][column of the strip]. Padding elements get G = 0.
 template <typename T>
 __global__ void geom_setup_kernel(T *__restrict__ G, const double *__restrict__ tabX64,
                                   const double *__restrict__ tabY64, const double *__restrict__ CP,
@@ -27,18 +27,18 @@ __global__ void geom_setup_kernel(T *__restrict__ G, const double *__restrict__ 
                                   int *err)
 {
     const int P = g.P, NB = P + 1, NQ = P + 1, NQ2 = NQ * NQ;
-    const long long total = (long long)g.NSX * g.NSY * g.TY * NQ2 * 32;
+    const long long total = (long long)g.NSX * g.NSY * g.TY * NQ2 * kSW;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int lane = (int)(t % 32);
-        long long r = t / 32;
+        const int c = (int)(t % kSW);
+        long long r = t / kSW;
         const int qp = (int)(r % NQ2);
         r /= NQ2;
         const int s = (int)(r % g.TY);
         r /= g.TY;
         const int gy = (int)(r % g.NSY);
         const int gx = (int)(r / g.NSY);
-        const int ex = 32 * gx + lane, ey = g.TY * gy + s;
+        const int ex = kSW * gx + c, ey = g.TY * gy + s;
         const int qx = qp % NQ, qy = qp / NQ;
         double g00 = 0, g01 = 0, g11 = 0;
         if (ex < g.nex && ey < g.ney) {
@@ -66,10 +66,10 @@ __global__ void geom_setup_kernel(T *__restrict__ G, const double *__restrict__ 
             g01 = -f * (x_xi * x_eta + y_xi * y_eta);
             g11 = f * (x_xi * x_xi + y_xi * y_xi);
         }
-        const size_t base = ((((size_t)gx * g.NSY + gy) * g.TY + s) * NQ2 + qp) * 3 * 32 + lane;
+        const size_t base = ((((size_t)gx * g.NSY + gy) * g.TY + s) * NQ2 + qp) * 3 * kSW + c;
         G[base] = (T)g00;
-        G[base + 32] = (T)g01;
-        G[base + 64] = (T)g11;
+        G[base + kSW] = (T)g01;
+        G[base + 2 * kSW] = (T)g11;
     }
 }
 
@@ -152,44 +152,41 @@ static int upload(T **dst, const void *src, size_t bytes)
     return IGA_OK;
 }
 
-static int nst_for(int prec) { return prec == IGA_FP64 ? 2 : 3; }
-
-template <int P, typename T>
-static size_t smem_for(int W, int NST)
-{
-    return NST == 2 ? apply_smem_bytes<P, T, 2>(W) : apply_smem_bytes<P, T, 3>(W);
-}
-
-template <typename T>
-static size_t smem_dispatch(int P, int W, int NST)
-{
-    switch (P) {
-    case 1: return smem_for<1, T>(W, NST);
-    case 2: return smem_for<2, T>(W, NST);
-    case 3: return smem_for<3, T>(W, NST);
-    case 4: return smem_for<4, T>(W, NST);
-    default: return smem_for<5, T>(W, NST);
-    }
-}
-
 static constexpr size_t kSmemBudget = 220 * 1024;
 
-// Warps per CTA: as many as fit in shared memory, at most 8.
-static int warps_for(int P, int prec)
+// Warps per CTA: as many as the shared memory and the kernel's register budget allow.
+template <int P, typename T, int GEOM>
+static int warps_for_t()
 {
-    const int NST = nst_for(prec);
-    for (int W = 8; W >= 1; --W) {
-        const size_t b = prec == IGA_FP64 ? smem_dispatch<double>(P, W, NST) : smem_dispatch<float>(P, W, NST);
-        if (b <= kSmemBudget) return W;
-    }
+    constexpr int NST = apply_stages<P, T>();
+    for (int W = apply_max_threads<P, T, GEOM>() / 32; W >= 1; --W)
+        if (apply_smem_bytes<P, T, GEOM, NST>(W) <= kSmemBudget) return W;
     return 1;
+}
+
+template <typename T, int GEOM>
+static int warps_for_g(int P)
+{
+    switch (P) {
+    case 1: return warps_for_t<1, T, GEOM>();
+    case 2: return warps_for_t<2, T, GEOM>();
+    case 3: return warps_for_t<3, T, GEOM>();
+    case 4: return warps_for_t<4, T, GEOM>();
+    default: return warps_for_t<5, T, GEOM>();
+    }
+}
+
+static int warps_for(int P, int prec, int geom)
+{
+    if (prec == IGA_FP64) return geom ? warps_for_g<double, 1>(P) : warps_for_g<double, 0>(P);
+    return geom ? warps_for_g<float, 1>(P) : warps_for_g<float, 0>(P);
 }
 
 // Rows per strip: the candidate whose CTA count fills the SMs best, with a
 // small penalty on short strips (more seam traffic).
 static int rows_for(int nex, int ney, int W, int nsm)
 {
-    const int NSX = (nex + 31) / 32;
+    const int NSX = (nex + kSW - 1) / kSW;
     int best = 64;
     double best_cost = 1e300;
     for (int TY : {64, 48, 32, 24, 16}) {
@@ -216,17 +213,19 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
 {
     const int p = P.p, NB = p + 1, NQ = p + 1, NQ2 = NQ * NQ;
     const StripGrid &g = pl->grid;
-    // x tables regrouped per column strip: [gx][kind][qx][il][lane]
-    std::vector<T> hx((size_t)g.NSX * 2 * NQ * NB * 32, T(0));
+    // x tables regrouped per column strip: [gx][kind][j][il][lane], lane = 2c + h
+    // holding element column 16 gx + c at quadrature column qx = h QH + j.
+    const int QH = (NQ + 1) / 2;
+    std::vector<T> hx((size_t)g.NSX * 2 * QH * NB * 32, T(0));
     for (int gx = 0; gx < g.NSX; ++gx)
         for (int kind = 0; kind < 2; ++kind)
-            for (int qx = 0; qx < NQ; ++qx)
+            for (int j = 0; j < QH; ++j)
                 for (int il = 0; il < NB; ++il)
                     for (int lane = 0; lane < 32; ++lane) {
-                        const int ex = 32 * gx + lane;
+                        const int ex = kSW * gx + lane / 2, qx = (lane % 2) * QH + j;
                         double v = 0.0;
-                        if (ex < P.nex) v = (kind ? tx.der : tx.val)[((size_t)ex * NQ + qx) * NB + il];
-                        hx[((((size_t)gx * 2 + kind) * NQ + qx) * NB + il) * 32 + lane] = (T)v;
+                        if (ex < P.nex && qx < NQ) v = (kind ? tx.der : tx.val)[((size_t)ex * NQ + qx) * NB + il];
+                        hx[((((size_t)gx * 2 + kind) * QH + j) * NB + il) * 32 + lane] = (T)v;
                     }
     std::vector<T> hy((size_t)P.ney * 2 * NQ * NB);
     for (int ey = 0; ey < P.ney; ++ey)
@@ -242,14 +241,18 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
     for (int a = 0; a < NQ; ++a)
         for (int b = 0; b < NQ; ++b) hw[a * NQ + b] = (T)(qw[a] * qw[b]);
     if ((st = upload((T **)&op.wq, hw.data(), hw.size() * sizeof(T)))) return st;
-    if (!P.kappa.empty() && pl->geometry == IGA_GEOM_ON_THE_FLY) {
-        std::vector<T> hk(P.kappa.begin(), P.kappa.end());
-        if ((st = upload((T **)&op.kappa, hk.data(), hk.size() * sizeof(T)))) return st;
+    if (pl->geometry == IGA_GEOM_ON_THE_FLY) {
+        if (!P.kappa.empty()) {
+            std::vector<T> hk(P.kappa.begin(), P.kappa.end());
+            if ((st = upload((T **)&op.kappa, hk.data(), hk.size() * sizeof(T)))) return st;
+        }
+        std::vector<T> hc(P.CP.begin(), P.CP.end());
+        if ((st = upload((T **)&op.CP, hc.data(), hc.size() * sizeof(T)))) return st;
     }
     size_t fbytes = (size_t)g.NSX * g.NSY * g.FS * sizeof(T);
     if ((st = upload((T **)&op.frame, nullptr, fbytes))) return st;
     if (pl->geometry == IGA_GEOM_PRECOMPUTED) {
-        const size_t gelems = (size_t)g.NSX * g.NSY * g.TY * NQ2 * 3 * 32;
+        const size_t gelems = (size_t)g.NSX * g.NSY * g.TY * NQ2 * 3 * kSW;
         op.geom_bytes = gelems * sizeof(T);
         if ((st = upload((T **)&op.G, nullptr, op.geom_bytes))) return st;
         double *kap = nullptr;
@@ -276,7 +279,7 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
     a.G = (const T *)op.G;
     a.tabX = (const T *)op.tabX;
     a.tabY = (const T *)op.tabY;
-    a.CP = pl->CP;
+    a.CP = (const T *)op.CP;
     a.wq = (const T *)op.wq;
     a.kappa = (const T *)op.kappa;
     a.frame = (T *)op.frame;
@@ -285,7 +288,7 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
     a.bc = bc;
     a.err = pl->d_err;
     const int W = op.warps;
-    const size_t smem = apply_smem_bytes<P, T, NST>(W);
+    const size_t smem = apply_smem_bytes<P, T, GEOM, NST>(W);
     auto kern = apply_kernel<P, T, GEOM, NST>;
     static bool attr_set = false;   // per template instance
     if (!attr_set) {
@@ -307,7 +310,7 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
 template <int P, typename T>
 static int launch_apply_p(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s, int sign, int bc)
 {
-    constexpr int NST = sizeof(T) == 8 ? 2 : 3;
+    constexpr int NST = apply_stages<P, T>();
     if (pl->geometry == IGA_GEOM_PRECOMPUTED) return launch_apply_t<P, T, 0, NST>(pl, op, x, y, s, sign, bc);
     return launch_apply_t<P, T, 1, NST>(pl, op, x, y, s, sign, bc);
 }
@@ -353,7 +356,7 @@ int iga_check_error_flag(iga_plan *pl)
 
 static void free_op(OperatorData &op)
 {
-    for (void *p : {op.tabX, op.tabY, op.G, op.frame, op.wq, op.kappa})
+    for (void *p : {op.tabX, op.tabY, op.G, op.frame, op.wq, op.kappa, op.CP})
         if (p) cudaFree(p);
     op = OperatorData{};
 }
@@ -444,7 +447,8 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     pl->bc = opts.bc;
     pl->device = opts.device;
     pl->patch = P;
-    const int Wmin = std::min(opts.precision == IGA_FP32 ? 8 : warps_for(P.p, IGA_FP64), warps_for(P.p, IGA_FP32));
+    const int Wmin = std::min(opts.precision == IGA_FP32 ? 16 : warps_for(P.p, IGA_FP64, opts.geometry),
+                              opts.precision == IGA_FP64 ? 16 : warps_for(P.p, IGA_FP32, opts.geometry));
     const int TY = opts.rows_per_strip > 0 ? opts.rows_per_strip : rows_for(P.nex, P.ney, Wmin, nsm);
     if (TY < P.p || TY > 1024) {
         delete pl;
@@ -457,7 +461,7 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     g.nex = P.nex;
     g.ney = P.ney;
     g.TY = TY;
-    g.NSX = (P.nex + 31) / 32;
+    g.NSX = (P.nex + kSW - 1) / kSW;
     g.NSY = (P.ney + TY - 1) / TY;
     g.P = P.p;
     g.FS = frame_size(P.p, TY);
@@ -492,11 +496,11 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
         cudaMemset(pl->d_err, 0, sizeof(int));
     }
     if (opts.precision != IGA_FP32) {
-        pl->op64.warps = warps_for(P.p, IGA_FP64);
+        pl->op64.warps = warps_for(P.p, IGA_FP64, opts.geometry);
         if ((st = build_operator<double>(pl, pl->op64, P, tx, ty))) return fail(st);
     }
     if (opts.precision != IGA_FP64) {
-        pl->op32.warps = warps_for(P.p, IGA_FP32);
+        pl->op32.warps = warps_for(P.p, IGA_FP32, opts.geometry);
         if ((st = build_operator<float>(pl, pl->op32, P, tx, ty))) return fail(st);
     }
     int herr = 0;

@@ -20,6 +20,7 @@ struct OperatorData {
     void *frame = nullptr;  // seam frames
     void *wq = nullptr;     // [NQ*NQ] quadrature weight products
     void *kappa = nullptr;  // on-the-fly coefficient
+    void *CP = nullptr;     // on-the-fly control points in the operator precision
     size_t geom_bytes = 0;
 };
 
