@@ -174,8 +174,23 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kern
     constexpr int D = S::XR - 1;
     for (int k = 0; k < D; ++k) fetch_row(k);
 
-    // This lane's x-direction tables: tabXs[kind][j][il][lane].
-    auto tx = [&](int kind, int j, int il) -> T { return tabXs[((kind * QH + j) * NB + il) * 32 + lane]; };
+    // This lane's x-direction tables: tabXs[kind][j][il][lane]; held in
+    // registers in FP32 (16 values at p = 3), read from shared memory in FP64
+    // where registers are the scarcer resource.
+    constexpr bool TXREG = sizeof(T) == 4;
+    T txr[TXREG ? 2 : 1][TXREG ? QH : 1][TXREG ? NB : 1];
+    if constexpr (TXREG) {
+#pragma unroll
+        for (int kind = 0; kind < 2; ++kind)
+#pragma unroll
+            for (int j = 0; j < QH; ++j)
+#pragma unroll
+                for (int il = 0; il < NB; ++il) txr[kind][j][il] = tabXs[((kind * QH + j) * NB + il) * 32 + lane];
+    }
+    auto tx = [&](int kind, int j, int il) -> T {
+        if constexpr (TXREG) return txr[kind][j][il];
+        else return tabXs[((kind * QH + j) * NB + il) * 32 + lane];
+    };
     unsigned colmask = 0;   // IGA_BC_IDENTITY: bit il set if column ex+il is a boundary column
     if (a.bc == 1)
         for (int il = 0; il <= P; ++il) {
@@ -266,15 +281,16 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kern
         }
         const int R = ey0 + lr;
         if (R >= g.n) return;
-        int fb;
-        const int rc = cover(R, g.TY, g.NSY, P, fb);
+        // Strips covering row R / column C (closed form of cover()): the
+        // first P rows/columns of a strip are shared with the strip before
+        // it (if any), the P rows/columns past its end with the one after it.
+        const bool row_single = lr < g.TY ? (lr >= P || gy == 0) : (gy + 1 >= g.NSY);
         const int lc = h ? kSW + c : c;
         const int C = ex0 + lc;
         if ((h == 0 || c < P) && C < g.m) {
             const T v = h ? spill : tot;
-            int fa;
-            const int cc = cover(C, kSW, g.NSX, P, fa);
-            if (rc == 1 && cc == 1) store(R, C, v);
+            const bool col_single = h ? (gx + 1 >= g.NSX) : (c >= P || gx == 0);
+            if (row_single && col_single) store(R, C, v);
             else frame[frame_index(lr, lc, P, g.TY)] = v;
         }
     };
