@@ -103,6 +103,16 @@ typedef struct {
  * C1 nElemX*(p+1)^2, C2 nElemY*(p+1)^2 (host arrays). */
 int iga_mesh_unit_square(int p, int nElemX, int nElemY, double Lx, double Ly, double *CP, double *C1, double *C2);
 
+/* Exact quarter annulus r in [r_in, r_out], theta in [0, pi/2] as a NURBS
+ * patch (no counterpart in the reference, which has no rational geometry):
+ * radial direction (index i, x-fastest) linear, angular direction the rational
+ * quadratic arc with middle weight sqrt(2)/2, both degree-elevated to p >= 2
+ * and refined by uniform knot insertion to nElemX x nElemY elements. Outputs:
+ * CP 2*(nElemX+p)*(nElemY+p), W (nElemX+p)*(nElemY+p) weights, C1/C2
+ * extraction operators as for iga_mesh_unit_square. */
+int iga_mesh_quarter_annulus(int p, int nElemX, int nElemY, double r_in, double r_out, double *CP, double *W,
+                             double *C1, double *C2);
+
 /* ---------------------------------------------------------------- plans */
 /* Build a plan: validate the mesh, upload the tables, precompute geometry. */
 int iga_plan_create(const iga_mesh_desc *mesh, const iga_opts *opts, iga_plan **out);

@@ -472,6 +472,43 @@ void orc_rhs(const orc_patch *P, int fkind, double *F)
         }
 }
 
+void orc_qp_points(const orc_patch *P, double *xy, double *jw)
+{
+    const int p = P->p, q = P->q;
+    tables t;
+    make_tables(p, q, &t);
+    double R[ORC_MAXN], Rx[ORC_MAXN], Ry[ORC_MAXN];
+    for (int ey = 0; ey < P->ney; ++ey)
+        for (int ex = 0; ex < P->nex; ++ex)
+            for (int jj = 0; jj < t.nq2; ++jj)
+                for (int ii = 0; ii < t.nq1; ++ii) {
+                    const size_t k = ((size_t)ey * P->nex + ex) * t.nq1 * t.nq2 + jj * t.nq1 + ii;
+                    double jxw, xq, yq;
+                    element_qp(P, &t, ex, ey, ii, jj, R, Rx, Ry, &jxw, &xq, &yq);
+                    xy[2 * k] = xq;
+                    xy[2 * k + 1] = yq;
+                    if (jw) jw[k] = jxw;
+                }
+}
+
+void orc_eval_qp(const orc_patch *P, const double *u, double *vals)
+{
+    const int p = P->p, q = P->q, m = P->nex + p, n = (p + 1) * (q + 1);
+    tables t;
+    make_tables(p, q, &t);
+    double R[ORC_MAXN], Rx[ORC_MAXN], Ry[ORC_MAXN];
+    for (int ey = 0; ey < P->ney; ++ey)
+        for (int ex = 0; ex < P->nex; ++ex)
+            for (int jj = 0; jj < t.nq2; ++jj)
+                for (int ii = 0; ii < t.nq1; ++ii) {
+                    double jxw;
+                    element_qp(P, &t, ex, ey, ii, jj, R, Rx, Ry, &jxw, NULL, NULL);
+                    double s = 0.0;
+                    for (int a = 0; a < n; ++a) s += R[a] * u[(size_t)(ey + a / (p + 1)) * m + (ex + a % (p + 1))];
+                    vals[((size_t)ey * P->nex + ex) * t.nq1 * t.nq2 + jj * t.nq1 + ii] = s;
+                }
+}
+
 void orc_adjoint_grad(const orc_patch *P, const double *u, const double *lam, double *g)
 {
     const int p = P->p, q = P->q, m = P->nex + p, n = (p + 1) * (q + 1);

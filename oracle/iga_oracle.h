@@ -54,6 +54,11 @@ void orc_apply_sf(const orc_patch *P, const double *x, double *y, double sign);
 /* F = int R f, F[Dir] = 0. fkind 0: x(1-x)y(1-y) (reference), 1: 2 pi^2 sin(pi x) sin(pi y),
  * 2: annulus manufactured f for u = sin(pi r) sin(2 theta). */
 void orc_rhs(const orc_patch *P, int fkind, double *F);
+/* Physical coordinates (x, y interleaved) and JxW at every quadrature point,
+ * element-major with qx fastest. */
+void orc_qp_points(const orc_patch *P, double *xy, double *jxw);
+/* u_h = sum_a R_a u_a at every quadrature point (same order). */
+void orc_eval_qp(const orc_patch *P, const double *u, double *vals);
 /* dJ/dkappa_q = -grad(lam).grad(u) * JxW_q at every quadrature point. */
 void orc_adjoint_grad(const orc_patch *P, const double *u, const double *lam, double *g);
 

@@ -163,6 +163,72 @@ Tables1D tables_1d(int p, int ne, const double *C, const double *wt)
     return t;
 }
 
+// ------------------------------------------------------------ NURBS annulus
+namespace {
+using Hpt = std::vector<double>;   // homogeneous point (w x, w y, w)
+
+// Degree elevation of one Bezier segment: Q_i = i/(p+1) P_{i-1} + (1 - i/(p+1)) P_i.
+std::vector<Hpt> bezier_elevate(const std::vector<Hpt> &P)
+{
+    const int p = (int)P.size() - 1;
+    std::vector<Hpt> Q(p + 2, Hpt(P[0].size(), 0.0));
+    for (int i = 0; i <= p + 1; ++i) {
+        const double a = (double)i / (p + 1);
+        for (size_t d = 0; d < P[0].size(); ++d)
+            Q[i][d] = (i > 0 ? a * P[i - 1][d] : 0.0) + (i <= p ? (1.0 - a) * P[i][d] : 0.0);
+    }
+    return Q;
+}
+
+// Boehm's single knot insertion of u into a degree-p curve (homogeneous).
+void insert_knot(std::vector<Hpt> &P, std::vector<double> &U, int p, double u)
+{
+    int k = p;
+    while (k + 1 < (int)U.size() - p - 1 && U[k + 1] <= u) ++k;   // U[k] <= u < U[k+1]
+    std::vector<Hpt> Q(P.size() + 1, Hpt(P[0].size(), 0.0));
+    for (int i = 0; i <= k - p; ++i) Q[i] = P[i];
+    for (int i = k - p + 1; i <= k; ++i) {
+        const double a = (u - U[i]) / (U[i + p] - U[i]);
+        for (size_t d = 0; d < P[0].size(); ++d) Q[i][d] = a * P[i][d] + (1.0 - a) * P[i - 1][d];
+    }
+    for (int i = k + 1; i < (int)Q.size(); ++i) Q[i] = P[i - 1];
+    U.insert(U.begin() + k + 1, u);
+    P.swap(Q);
+}
+
+// Coarse single-segment curve elevated to degree p and refined to ne elements on [0,1].
+std::vector<Hpt> elevate_refine(std::vector<Hpt> P, int p, int ne)
+{
+    while ((int)P.size() - 1 < p) P = bezier_elevate(P);
+    std::vector<double> U(p + 1, 0.0);
+    U.insert(U.end(), p + 1, 1.0);
+    for (int k = 1; k < ne; ++k) insert_knot(P, U, p, (double)k / ne);
+    return P;
+}
+}  // namespace
+
+void quarter_annulus(int p, int ner, int net, double r_in, double r_out, std::vector<double> &CP,
+                     std::vector<double> &W, std::vector<double> &C1, std::vector<double> &C2)
+{
+    // radial: r(xi) = r_in + (r_out - r_in) xi as a linear Bezier segment (weights 1)
+    const std::vector<Hpt> rad = elevate_refine({{r_in, 1.0}, {r_out, 1.0}}, p, ner);
+    // angular: unit quarter circle, rational quadratic, homogeneous (w x, w y, w)
+    const double s2 = std::sqrt(0.5);
+    const std::vector<Hpt> ang = elevate_refine({{1.0, 0.0, 1.0}, {s2, s2, s2}, {0.0, 1.0, 1.0}}, p, net);
+    const int m = (int)rad.size(), n = (int)ang.size();
+    CP.assign(2 * (size_t)m * n, 0.0);
+    W.assign((size_t)m * n, 0.0);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) {
+            const double r = rad[i][0] / rad[i][1], w = ang[j][2];
+            CP[2 * ((size_t)j * m + i)] = r * ang[j][0] / w;
+            CP[2 * ((size_t)j * m + i) + 1] = r * ang[j][1] / w;
+            W[(size_t)j * m + i] = w;
+        }
+    C1 = extraction(p, open_knots(p, ner, 1.0));
+    C2 = extraction(p, open_knots(p, net, 1.0));
+}
+
 static bool factor_weights(const double *w, int m, int n, std::vector<double> &a, std::vector<double> &b)
 {
     // w(i,j) = a(i) b(j) with a(0) = 1 (scale-free factorisation).

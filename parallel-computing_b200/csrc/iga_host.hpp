@@ -37,6 +37,15 @@ struct Tables1D {
 };
 Tables1D tables_1d(int p, int ne, const double *C /* ne*(p+1)^2 */, const double *wt /* ne+p or null */);
 
+// Exact quarter annulus r in [r_in, r_out], theta in [0, pi/2] as a NURBS
+// patch: radial direction (x-fastest index) linear, angular direction the
+// rational quadratic arc (weights 1, sqrt(2)/2, 1), both degree-elevated to p
+// and refined by uniform knot insertion to ner x net elements. Outputs the
+// control points (x, y interleaved), one weight per control point, and the
+// (open uniform) knot vectors' extraction operators.
+void quarter_annulus(int p, int ner, int net, double r_in, double r_out, std::vector<double> &CP,
+                     std::vector<double> &W, std::vector<double> &C1, std::vector<double> &C2);
+
 // Host description of a validated patch.
 struct Patch {
     int p = 0, q = 0, nex = 0, ney = 0, m = 0, n = 0;

@@ -409,6 +409,20 @@ int iga_mesh_unit_square(int p, int nex, int ney, double Lx, double Ly, double *
     return IGA_OK;
 }
 
+int iga_mesh_quarter_annulus(int p, int nex, int ney, double r_in, double r_out, double *CP, double *W, double *C1,
+                             double *C2)
+{
+    if (p < 2 || p > 8 || nex < 1 || ney < 1 || !CP || !W || !C1 || !C2 || !(r_in > 0) || !(r_out > r_in))
+        return IGA_ERR_ARG;
+    std::vector<double> cp, w, c1, c2;
+    quarter_annulus(p, nex, ney, r_in, r_out, cp, w, c1, c2);
+    std::memcpy(CP, cp.data(), cp.size() * sizeof(double));
+    std::memcpy(W, w.data(), w.size() * sizeof(double));
+    std::memcpy(C1, c1.data(), c1.size() * sizeof(double));
+    std::memcpy(C2, c2.data(), c2.size() * sizeof(double));
+    return IGA_OK;
+}
+
 int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **out)
 {
     if (!d || !out) return IGA_ERR_ARG;

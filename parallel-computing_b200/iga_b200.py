@@ -71,6 +71,8 @@ SIGNATURES = [
     ("iga_opts_default", None, [ctypes.POINTER(Opts)]),
     ("iga_mesh_unit_square", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                             ctypes.c_double, VP, VP, VP]),
+    ("iga_mesh_quarter_annulus", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                ctypes.c_double, VP, VP, VP, VP]),
     ("iga_plan_create", ctypes.c_int, [ctypes.POINTER(MeshDesc), ctypes.POINTER(Opts), ctypes.POINTER(VP)]),
     ("iga_plan_destroy", ctypes.c_int, [VP]),
     ("iga_plan_get_info", ctypes.c_int, [VP, ctypes.POINTER(PlanInfo)]),
@@ -145,6 +147,20 @@ def unit_square(p, nex, ney=None, Lx=1.0, Ly=1.0):
            "iga_mesh_unit_square")
     return dict(p=p, q=p, nex=nex, ney=ney, CP=CP, C1=C1, C2=C2, W=None, kappa=None,
                 h1=np.full(nex, Lx / nex), h2=np.full(ney, Ly / ney))
+
+
+def quarter_annulus(p, nex, ney=None, r_in=1.0, r_out=2.0):
+    """Exact NURBS quarter annulus (radial direction first): dict(p, q, nex, ney, CP, W, C1, C2)."""
+    ney = nex if ney is None else ney
+    m, n = nex + p, ney + p
+    CP = np.empty(2 * m * n)
+    W = np.empty(m * n)
+    C1 = np.empty(nex * (p + 1) ** 2)
+    C2 = np.empty(ney * (p + 1) ** 2)
+    _check(_lib().iga_mesh_quarter_annulus(p, nex, ney, r_in, r_out, _ptr(CP), _ptr(W), _ptr(C1), _ptr(C2)),
+           "iga_mesh_quarter_annulus")
+    return dict(p=p, q=p, nex=nex, ney=ney, CP=CP, W=W, C1=C1, C2=C2, kappa=None,
+                h1=np.full(nex, 1.0 / nex), h2=np.full(ney, 1.0 / ney))
 
 
 class Plan:

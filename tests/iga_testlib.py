@@ -74,6 +74,8 @@ class Oracle:
         self.L.orc_apply_sf.argtypes = [ctypes.POINTER(OrcPatch), VP, VP, ctypes.c_double]
         self.L.orc_rhs.argtypes = [ctypes.POINTER(OrcPatch), ctypes.c_int, VP]
         self.L.orc_adjoint_grad.argtypes = [ctypes.POINTER(OrcPatch), VP, VP, VP]
+        self.L.orc_qp_points.argtypes = [ctypes.POINTER(OrcPatch), VP, VP]
+        self.L.orc_eval_qp.argtypes = [ctypes.POINTER(OrcPatch), VP, VP]
         self.L.orc_fem_nodes.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, VP]
         self.L.orc_fem_matvec.argtypes = [ctypes.c_int, ctypes.c_int, VP, VP, VP, VP, ctypes.c_double]
         self.L.orc_pcg.argtypes = [ctypes.POINTER(OrcPatch), VP, VP, VP, VP, ctypes.c_double, ctypes.c_int,
@@ -146,6 +148,20 @@ class Oracle:
         F = np.empty((mesh["nex"] + mesh["p"]) * (mesh["ney"] + mesh["q"]))
         self.L.orc_rhs(ctypes.byref(P), fkind, _p(F))
         return F
+
+    def qp_points(self, mesh):
+        P = self.patch(mesh)
+        nq = mesh["nex"] * mesh["ney"] * (mesh["p"] + 1) * (mesh["q"] + 1)
+        xy, jw = np.empty(2 * nq), np.empty(nq)
+        self.L.orc_qp_points(ctypes.byref(P), _p(xy), _p(jw))
+        return xy.reshape(-1, 2), jw
+
+    def eval_qp(self, mesh, u):
+        P = self.patch(mesh)
+        vals = np.empty(mesh["nex"] * mesh["ney"] * (mesh["p"] + 1) * (mesh["q"] + 1))
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        self.L.orc_eval_qp(ctypes.byref(P), _p(u), _p(vals))
+        return vals
 
     def adjoint_grad(self, mesh, u, lam):
         P = self.patch(mesh)
