@@ -236,6 +236,36 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
                      "relres": st.relres}
     out["speedup_fp32_refine_vs_fp64"] = out["fp64"]["seconds"] / out["fp32_refine"]["seconds"]
     plan.close()
+    # mixed-precision configuration: NURBS quarter annulus, p=4, 1024x1024,
+    # u = sin(pi r) sin(2 theta); error of the FP32+refine solution vs the FP64 one
+    ma = ib.quarter_annulus(4, 1024)
+    pa = ib.Plan(ma, precision=ib.MIXED)
+    ba = torch.empty(pa.nfunc, dtype=torch.float64, device="cuda")
+    pa.rhs(ba, ib.F_ANNULUS)
+    xs = {}
+    ann = {"problem": "quarter annulus r in [1,2] (NURBS, p=4), 1024x1024, u = sin(pi r) sin(2 theta), rtol 1e-10"}
+    for name, kw in (("fp64", dict(pc=ib.PC_FEM_EXACT)), ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED))):
+        x = torch.zeros_like(ba)
+        pa.solve(ba, x, **kw)
+        times = []
+        for _ in range(3):
+            x.zero_()
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = pa.solve(ba, x, stream=stream, **kw)
+            e1.record(stream)
+            barrier()
+            times.append(max_over_ranks(e0.elapsed_time(e1) / 1e3))
+        xs[name] = x
+        ann[name] = {"seconds": statistics.median(times), "iterations": st.iterations, "sweeps": st.sweeps,
+                     "relres": st.relres}
+    ann["speedup_fp32_refine_vs_fp64"] = ann["fp64"]["seconds"] / ann["fp32_refine"]["seconds"]
+    ann["rel_error_fp32_refine_vs_fp64"] = float((xs["fp32_refine"] - xs["fp64"]).norm() / xs["fp64"].norm())
+    out["annulus_p4_1024"] = ann
+    pa.close()
+    del xs
+    torch.cuda.empty_cache()
     # reference preconditioner, p=2 64x64 (the CPU-runnable configuration)
     m2 = ib.unit_square(2, 64)
     p2 = ib.Plan(m2)

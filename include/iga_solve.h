@@ -83,6 +83,20 @@ int iga_fem_apply(iga_plan *plan, int precision, const void *x_dev, void *y_dev,
 int iga_fem_assemble_csr(iga_plan *plan, int sign, int32_t *rowptr_dev, int32_t *colidx_dev, double *vals_dev,
                          int64_t *nnz, void *stream);
 
+/* Coefficient of -div(kappa grad u) = f at the quadrature points (device array,
+ * element-major, qx fastest; nElemX*nElemY*(p+1)^2 doubles), replacing the
+ * plan's current kappa (kappa = 1 in the reference). Recomputes the
+ * precomputed geometry on the device; on-the-fly plans store kappa. The
+ * solver's preconditioners are rescaled by the local mean of kappa. No
+ * counterpart in the reference. */
+int iga_plan_set_kappa(iga_plan *plan, const double *kappa_dev, void *stream);
+
+/* Adjoint gradient (no counterpart in the reference): g_q = -(grad lambda .
+ * grad u)(x_q) * JxW_q at every quadrature point (same layout as kappa), i.e.
+ * dJ/dkappa_q when K(kappa) u = F and K lambda = dJ/du with lambda = 0 on the
+ * boundary. u, lambda: nfunc doubles on the device. */
+int iga_adjoint_grad(iga_plan *plan, const double *u_dev, const double *lambda_dev, double *g_dev, void *stream);
+
 /* 1-D node coordinates of the FEM preconditioner grid (host arrays of
  * nElemX+p and nElemY+q entries): degree p-2 Greville abscissae of the
  * shortened knot vector (matrix_free/preprocess_fem.cpp:38-60) for p >= 3; the

@@ -255,12 +255,9 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
         const size_t gelems = (size_t)g.NSX * g.NSY * g.TY * NQ2 * 3 * kSW;
         op.geom_bytes = gelems * sizeof(T);
         if ((st = upload((T **)&op.G, nullptr, op.geom_bytes))) return st;
-        double *kap = nullptr;
-        if (!P.kappa.empty())
-            if ((st = upload(&kap, P.kappa.data(), P.kappa.size() * sizeof(double)))) return st;
-        geom_setup_kernel<T><<<1184, 256>>>((T *)op.G, pl->tabX64, pl->tabY64, pl->CP, pl->qw, kap, g, pl->d_err);
+        geom_setup_kernel<T><<<1184, 256>>>((T *)op.G, pl->tabX64, pl->tabY64, pl->CP, pl->qw, pl->kappa_dev, g,
+                                            pl->d_err);
         cudaError_t e = cudaDeviceSynchronize();
-        if (kap) cudaFree(kap);
         if (e != cudaSuccess) {
             set_error(std::string("geometry setup: ") + cudaGetErrorString(e));
             return IGA_ERR_CUDA;
@@ -352,6 +349,13 @@ int iga_check_error_flag(iga_plan *pl)
         return h;
     }
     return IGA_OK;
+}
+
+template <typename T>
+__global__ void kappa_convert_kernel(T *__restrict__ dst, const double *__restrict__ src, long long n)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        dst[t] = (T)src[t];
 }
 
 static void free_op(OperatorData &op)
@@ -508,6 +512,10 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
         if ((st = upload(&pl->qw, qw.data(), qw.size() * 8))) return fail(st);
         if ((st = upload(&pl->d_err, nullptr, sizeof(int)))) return fail(st);
         cudaMemset(pl->d_err, 0, sizeof(int));
+        if (!P.kappa.empty()) {
+            if ((st = upload(&pl->kappa_dev, P.kappa.data(), P.kappa.size() * 8))) return fail(st);
+            pl->kappa_version = 1;
+        }
     }
     if (opts.precision != IGA_FP32) {
         pl->op64.warps = warps_for(P.p, IGA_FP64, opts.geometry);
@@ -535,6 +543,7 @@ int iga_plan_destroy(iga_plan *pl)
     free_op(pl->op64);
     free_op(pl->op32);
     for (void *p : {(void *)pl->tabX64, (void *)pl->tabY64, (void *)pl->CP, (void *)pl->qw, (void *)pl->d_err,
+                    (void *)pl->kappa_dev,
                     (void *)pl->h_stage_x, (void *)pl->d_stage_x, (void *)pl->d_stage_y})
         if (p) cudaFree(p);
     if (pl->h_pinned) cudaFreeHost(pl->h_pinned);
@@ -561,6 +570,36 @@ int iga_plan_get_info(const iga_plan *pl, iga_plan_info *info)
     }
     info->rows_per_strip = pl->grid.TY;
     info->warps_per_cta = pl->op64.ready ? pl->op64.warps : pl->op32.warps;
+    return IGA_OK;
+}
+
+int iga_plan_set_kappa(iga_plan *pl, const double *kappa, void *stream)
+{
+    if (!pl || !kappa) return IGA_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long nq = (long long)pl->nex * pl->ney * (pl->p + 1) * (pl->p + 1);
+    if (!pl->kappa_dev) IGA_CUDA_TRY(cudaMalloc((void **)&pl->kappa_dev, nq * sizeof(double)));
+    IGA_CUDA_TRY(cudaMemcpyAsync(pl->kappa_dev, kappa, nq * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    ++pl->kappa_version;
+    OperatorData *ops[2] = {&pl->op64, &pl->op32};
+    for (int k = 0; k < 2; ++k) {
+        OperatorData &op = *ops[k];
+        if (!op.ready) continue;
+        if (pl->geometry == IGA_GEOM_PRECOMPUTED) {
+            if (k == 0)
+                geom_setup_kernel<double><<<1184, 256, 0, s>>>((double *)op.G, pl->tabX64, pl->tabY64, pl->CP, pl->qw,
+                                                              pl->kappa_dev, pl->grid, pl->d_err);
+            else
+                geom_setup_kernel<float><<<1184, 256, 0, s>>>((float *)op.G, pl->tabX64, pl->tabY64, pl->CP, pl->qw,
+                                                             pl->kappa_dev, pl->grid, pl->d_err);
+        } else {
+            const size_t es = k == 0 ? sizeof(double) : sizeof(float);
+            if (!op.kappa) IGA_CUDA_TRY(cudaMalloc(&op.kappa, nq * es));
+            if (k == 0) kappa_convert_kernel<double><<<296, 256, 0, s>>>((double *)op.kappa, pl->kappa_dev, nq);
+            else kappa_convert_kernel<float><<<296, 256, 0, s>>>((float *)op.kappa, pl->kappa_dev, nq);
+        }
+    }
+    IGA_CUDA_TRY(cudaGetLastError());
     return IGA_OK;
 }
 

@@ -41,6 +41,8 @@ struct iga_plan {
     iga::OperatorData op64, op32;
     double *tabX64 = nullptr, *tabY64 = nullptr, *CP = nullptr, *qw = nullptr;
     int *d_err = nullptr;
+    double *kappa_dev = nullptr;   // coefficient at the quadrature points (null: 1)
+    int kappa_version = 0;         // bumped by every change of kappa
     double *h_stage_x = nullptr, *d_stage_x = nullptr, *d_stage_y = nullptr;
     void *h_pinned = nullptr;
     iga::SolverState *solver = nullptr;
@@ -50,4 +52,6 @@ int iga_apply_internal(iga_plan *pl, int prec, const void *x, void *y, cudaStrea
 // Operator with explicit sign / boundary rule (the solver applies +K with identity rows).
 int iga_apply_internal_sb(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s, int sign, int bc);
 int iga_check_error_flag(iga_plan *pl);
+// Computes G of one operator precision from the plan's tables and kappa (device).
+int iga_rebuild_geometry(iga_plan *pl, cudaStream_t s);
 void iga_solver_release(iga_plan *pl);

@@ -453,6 +453,38 @@ __global__ void boundary_copy_kernel(T *__restrict__ z, const T *__restrict__ r,
     }
 }
 
+// ------------------------------------------------------------ kappa scaling of the preconditioner
+// s_i = 1 / sqrt(mean of kappa over the quadrature points of the elements
+// supporting control point i); the preconditioner becomes S M^-1 S, which
+// keeps the FEM matrix's shape and adds the coefficient's local magnitude.
+__global__ void kappa_scale_kernel(const double *__restrict__ kappa, double *__restrict__ s64, float *__restrict__ s32,
+                                   StripGrid g)
+{
+    const int P = g.P, NQ2 = (P + 1) * (P + 1);
+    const long long N = (long long)g.m * g.n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        const int C = (int)(t % g.m), R = (int)(t / g.m);
+        double sum = 0.0;
+        int cnt = 0;
+        for (int ey = max(0, R - P); ey <= min(R, g.ney - 1); ++ey)
+            for (int ex = max(0, C - P); ex <= min(C, g.nex - 1); ++ex) {
+                const double *k = kappa + ((size_t)ey * g.nex + ex) * NQ2;
+                for (int q = 0; q < NQ2; ++q) sum += k[q];
+                cnt += NQ2;
+            }
+        const double v = (cnt > 0 && sum > 0.0) ? 1.0 / sqrt(sum / cnt) : 1.0;
+        s64[t] = v;
+        s32[t] = (float)v;
+    }
+}
+
+template <typename T>
+__global__ void mul_kernel(T *__restrict__ out, const T *__restrict__ a, const T *__restrict__ b, long long N)
+{
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        out[t] = a[t] * b[t];
+}
+
 // ------------------------------------------------------------ host state
 template <typename T>
 struct PrecState {
@@ -460,6 +492,7 @@ struct PrecState {
     T *kd = nullptr, *ko = nullptr, *md = nullptr, *mo = nullptr;
     T *ld = nullptr, *lo = nullptr, *nd = nullptr, *no = nullptr;
     T *x = nullptr, *r = nullptr, *z = nullptr, *zo = nullptr, *p = nullptr, *q = nullptr, *b = nullptr;
+    T *sc = nullptr;   // kappa-scaled preconditioner input
     T *iz = nullptr, *ir = nullptr, *ip = nullptr, *iq = nullptr;
     cudaGraphExec_t chunk = nullptr;
     // exact FEM inverse: eigenvectors (column-major), eigenvalues, two work matrices
@@ -480,6 +513,9 @@ struct SolverState {
     cublasHandle_t blas = nullptr;
     bool fd_host = false;
     std::vector<double> lamx, lamy, Vx, Vy;   // host eigenpairs (built once)
+    double *ks64 = nullptr;                   // kappa scaling of the preconditioner
+    float *ks32 = nullptr;
+    int kappa_version = 0;
     DevScalars *s = nullptr;
     DevScalars *h = nullptr;   // pinned mirror
     double *partials = nullptr;
@@ -572,7 +608,7 @@ static int alloc_prec(PrecState<T> &ps, const iga_plan *pl, const SolverState &S
     if ((st = up(&ps.kd, kd)) || (st = up(&ps.ko, ko)) || (st = up(&ps.md, md)) || (st = up(&ps.mo, mo)) ||
         (st = up(&ps.ld, ld)) || (st = up(&ps.lo, lo)) || (st = up(&ps.nd, nd)) || (st = up(&ps.no, no)))
         return st;
-    for (T **v : {&ps.x, &ps.r, &ps.z, &ps.zo, &ps.p, &ps.q, &ps.b, &ps.iz, &ps.ir, &ps.ip, &ps.iq})
+    for (T **v : {&ps.x, &ps.r, &ps.z, &ps.zo, &ps.p, &ps.q, &ps.b, &ps.sc, &ps.iz, &ps.ir, &ps.ip, &ps.iq})
         SOLVE_TRY(cudaMalloc((void **)v, sizeof(T) * N));
     ps.ready = true;
     return IGA_OK;
@@ -609,7 +645,7 @@ template <typename T>
 static void free_prec(PrecState<T> &ps)
 {
     T *bufs[] = {ps.kd, ps.ko, ps.md, ps.mo, ps.ld, ps.lo, ps.nd, ps.no, ps.x, ps.r, ps.z, ps.zo, ps.p,
-                 ps.q, ps.b, ps.iz, ps.ir, ps.ip, ps.iq, ps.Vx, ps.Vy, ps.lx, ps.ly, ps.W1, ps.W2};
+                 ps.q, ps.b, ps.sc, ps.iz, ps.ir, ps.ip, ps.iq, ps.Vx, ps.Vy, ps.lx, ps.ly, ps.W1, ps.W2};
     for (T *v : bufs)
         if (v) cudaFree(v);
     if (ps.chunk) cudaGraphExecDestroy(ps.chunk);
@@ -623,7 +659,8 @@ void iga_solver_release(iga_plan *pl)
     cudaSetDevice(S->device);
     free_prec(S->d);
     free_prec(S->f);
-    for (void *v : {(void *)S->s, (void *)S->partials, (void *)S->counter, (void *)S->r64, (void *)S->q64})
+    for (void *v : {(void *)S->s, (void *)S->partials, (void *)S->counter, (void *)S->r64, (void *)S->q64,
+                    (void *)S->ks64, (void *)S->ks32})
         if (v) cudaFree(v);
     if (S->h) cudaFreeHost(S->h);
     if (S->blas) cublasDestroy(S->blas);
@@ -795,10 +832,47 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
     return IGA_OK;
 }
 
-// z = M^-1 r for the configured preconditioner.
+template <typename T>
+static int pc_apply_core(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const iga_solve_opts &o, const T *r,
+                         T *z, double pc_rtol, int64_t &pc_iters);
+
+static const double *kscale(SolverState *S, double *) { return S->ks64; }
+static const float *kscale(SolverState *S, float *) { return S->ks32; }
+
+// Scaling vector of the current kappa (null when the plan has none).
+static int update_kscale(const iga_plan *pl, SolverState *S)
+{
+    if (!pl->kappa_dev || S->kappa_version == pl->kappa_version) return IGA_OK;
+    if (!S->ks64) {
+        SOLVE_TRY(cudaMalloc((void **)&S->ks64, sizeof(double) * pl->nfunc));
+        SOLVE_TRY(cudaMalloc((void **)&S->ks32, sizeof(float) * pl->nfunc));
+    }
+    kappa_scale_kernel<<<kRedBlocks, kThreads, 0, S->stream>>>(pl->kappa_dev, S->ks64, S->ks32, pl->grid);
+    S->kappa_version = pl->kappa_version;
+    SOLVE_TRY(cudaGetLastError());
+    return IGA_OK;
+}
+
+// z = M^-1 r for the configured preconditioner; with a coefficient kappa,
+// z = S M^-1 (S r) with the local scaling S.
 template <typename T>
 static int pc_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const iga_solve_opts &o, const T *r, T *z,
                     double pc_rtol, int64_t &pc_iters)
+{
+    const long long N = pl->nfunc;
+    if (o.pc == IGA_PC_NONE || !pl->kappa_dev) return pc_apply_core(ps, pl, S, o, r, z, pc_rtol, pc_iters);
+    int st;
+    if ((st = update_kscale(pl, S))) return st;
+    const T *sv = kscale(S, (T *)nullptr);
+    mul_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(ps.sc, r, sv, N);
+    if ((st = pc_apply_core(ps, pl, S, o, ps.sc, z, pc_rtol, pc_iters))) return st;
+    mul_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(z, z, sv, N);
+    return IGA_OK;
+}
+
+template <typename T>
+static int pc_apply_core(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const iga_solve_opts &o, const T *r,
+                         T *z, double pc_rtol, int64_t &pc_iters)
 {
     const long long N = pl->nfunc;
     if (o.pc == IGA_PC_NONE) {

@@ -89,6 +89,8 @@ SIGNATURES = [
     ("iga_fem_assemble_csr", ctypes.c_int, [VP, ctypes.c_int, VP, VP, VP, ctypes.POINTER(ctypes.c_int64), VP]),
     ("iga_fem_nodes", ctypes.c_int, [VP, VP, VP]),
     ("iga_pc_apply", ctypes.c_int, [VP, ctypes.c_int, ctypes.c_int, VP, VP, ctypes.c_double, ctypes.c_int, VP]),
+    ("iga_plan_set_kappa", ctypes.c_int, [VP, VP, VP]),
+    ("iga_adjoint_grad", ctypes.c_int, [VP, VP, VP, VP, VP]),
 ]
 
 
@@ -161,6 +163,47 @@ def quarter_annulus(p, nex, ney=None, r_in=1.0, r_out=2.0):
            "iga_mesh_quarter_annulus")
     return dict(p=p, q=p, nex=nex, ney=ney, CP=CP, W=W, C1=C1, C2=C2, kappa=None,
                 h1=np.full(nex, 1.0 / nex), h2=np.full(ney, 1.0 / ney))
+
+
+def splitmix_normal(seed, n, offset=0):
+    """N(0,1) from the SplitMix64 counter stream (Box-Muller on consecutive pairs)."""
+    m = (n + 1) // 2
+    i = np.arange(2 * offset + 1, 2 * offset + 2 * m + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = np.uint64(seed) + i * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+    r = np.sqrt(-2.0 * np.log(1.0 - u[0::2]))
+    out = np.empty(2 * m)
+    out[0::2] = r * np.cos(2 * np.pi * u[1::2])
+    out[1::2] = r * np.sin(2 * np.pi * u[1::2])
+    return out[:n]
+
+
+def grf_qp(mesh, sigma=1.0, ell=0.1, seed=3):
+    """Gaussian random field with squared-exponential covariance sigma^2
+    exp(-|x-x'|^2 / (2 ell^2)) sampled at the quadrature points of a unit-square
+    patch (element-major, qx fastest). The covariance is separable on the tensor
+    grid of quadrature points, so g = sigma Lx Z Ly^T with Lx Lx^T = Kx from
+    1-D eigendecompositions and Z ~ N(0,1) from the SplitMix64 stream."""
+    p, nex, ney = mesh["p"], mesh["nex"], mesh["ney"]
+    nq = p + 1
+    t = np.polynomial.legendre.leggauss(nq)[0] * 0.5 + 0.5
+    xs = ((np.arange(nex)[:, None] + t[None, :]) / nex).ravel()
+    ys = ((np.arange(ney)[:, None] + t[None, :]) / ney).ravel()
+
+    def factor(z):
+        K = np.exp(-(z[:, None] - z[None, :]) ** 2 / (2 * ell * ell))
+        w, V = np.linalg.eigh(K)
+        return V * np.sqrt(np.clip(w, 0.0, None))
+
+    Lx, Ly = factor(xs), factor(ys)
+    Z = splitmix_normal(seed, len(ys) * len(xs)).reshape(len(ys), len(xs))
+    G = sigma * (Ly @ Z @ Lx.T)          # G[b, a]: y point b, x point a
+    G = G.reshape(ney, nq, nex, nq).transpose(0, 2, 1, 3)   # [ey][ex][qy][qx]
+    return np.ascontiguousarray(G).ravel()
 
 
 class Plan:
@@ -253,6 +296,14 @@ class Plan:
         _check(_lib().iga_pc_apply(self.h, pc, precision, _ptr(r), _ptr(z), pc_rtol, pc_max_it, _stream(stream)),
                "iga_pc_apply")
 
+    def set_kappa(self, kappa, stream=None):
+        """Coefficient at the quadrature points (device tensor, element-major, qx fastest)."""
+        _check(_lib().iga_plan_set_kappa(self.h, _ptr(kappa), _stream(stream)), "iga_plan_set_kappa")
+
+    def adjoint_grad(self, u, lam, g, stream=None):
+        _check(_lib().iga_adjoint_grad(self.h, _ptr(u), _ptr(lam), _ptr(g), _stream(stream)), "iga_adjoint_grad")
+        return g
+
     def fem_nodes(self):
         gx = np.empty(self.mesh["nex"] + self.mesh["p"])
         gy = np.empty(self.mesh["ney"] + self.mesh.get("q", self.mesh["p"]))
@@ -271,3 +322,36 @@ class Plan:
                "iga_fem_assemble_csr")
         torch.cuda.synchronize()
         return rp.cpu().numpy(), col.cpu().numpy(), val.cpu().numpy()
+
+
+def kappa_solve_function():
+    """torch.autograd.Function u = K(kappa)^-1 F (a thin test binding over
+    iga_plan_set_kappa, iga_solve and iga_adjoint_grad): backward runs the
+    adjoint solve K lambda = dL/du (lambda = 0 on the boundary) and returns
+    dL/dkappa_q = -(grad lambda . grad u) JxW_q."""
+    import torch
+
+    class KappaSolve(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, kappa, plan, F, bmask, solve_kw):
+            plan.set_kappa(kappa.detach().contiguous())
+            u = torch.zeros_like(F)
+            plan.solve(F, u, **solve_kw)
+            ctx.plan, ctx.bmask, ctx.solve_kw = plan, bmask, solve_kw
+            ctx.save_for_backward(kappa, u)
+            return u
+
+        @staticmethod
+        def backward(ctx, grad_u):
+            kappa, u = ctx.saved_tensors
+            plan = ctx.plan
+            plan.set_kappa(kappa.detach().contiguous())
+            rhs = grad_u.contiguous().clone()
+            rhs[ctx.bmask] = 0.0
+            lam = torch.zeros_like(rhs)
+            plan.solve(rhs, lam, **ctx.solve_kw)
+            g = torch.empty_like(kappa)
+            plan.adjoint_grad(u, lam, g)
+            return g, None, None, None, None
+
+    return KappaSolve
