@@ -266,6 +266,10 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
     pa.close()
     del xs
     torch.cuda.empty_cache()
+    # adjoint configuration: p=3 512x512, kappa = exp(g) (Gaussian random field,
+    # sigma 1, squared-exponential length 0.1, seed 3), u_obs = u(exp(0.8 g)) + 1%
+    # noise, J = |u - u_obs|^2 / 2; forward solve + adjoint solve + dJ/dkappa.
+    out["adjoint_p3_512"] = time_adjoint(ib, torch, stream, barrier, max_over_ranks)
     # reference preconditioner, p=2 64x64 (the CPU-runnable configuration)
     m2 = ib.unit_square(2, 64)
     p2 = ib.Plan(m2)
@@ -281,6 +285,58 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
     p2.close()
     torch.cuda.empty_cache()
     return out
+
+
+def time_adjoint(ib, torch, stream, barrier, max_over_ranks):
+    m = ib.unit_square(3, 512)
+    plan = ib.Plan(m)
+    n = plan.nfunc
+    g = ib.grf_qp(m, sigma=1.0, ell=0.1, seed=3)
+    F = torch.empty(n, dtype=torch.float64, device="cuda")
+    plan.rhs(F, ib.F_SINSIN)
+    mside = 515
+    bmask = torch.zeros(mside, mside, dtype=torch.bool, device="cuda")
+    bmask[0, :] = bmask[-1, :] = bmask[:, 0] = bmask[:, -1] = True
+    bmask = bmask.ravel()
+    kw = dict(pc=ib.PC_FEM_EXACT, rtol=1e-10)
+    KS = ib.kappa_solve_function()
+    with torch.no_grad():
+        u_true = KS.apply(torch.from_numpy(np.exp(0.8 * g)).cuda(), plan, F, bmask, kw)
+    noise = torch.from_numpy(ib.splitmix_normal(3, n, offset=10 ** 7)).cuda()
+    u_obs = u_true + 0.01 * float(u_true.abs().max()) * noise
+    u_obs[bmask] = 0.0
+    kappa = torch.from_numpy(np.exp(g)).cuda()
+
+    def J_and_grad():
+        k = kappa.clone().requires_grad_(True)
+        u = KS.apply(k, plan, F, bmask, kw)
+        J = 0.5 * ((u - u_obs) ** 2).sum()
+        J.backward()
+        return J, k.grad
+
+    J_and_grad()   # warm-up
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    J, grad = J_and_grad()
+    e1.record(stream)
+    barrier()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    # directional derivative vs central differences (2 random directions, step 1e-6)
+    errs = []
+    for k in range(2):
+        d = torch.from_numpy(ib.splitmix_normal(100 + k, kappa.numel())).cuda()
+        with torch.no_grad():
+            jp = 0.5 * ((KS.apply(kappa + 1e-6 * d, plan, F, bmask, kw) - u_obs) ** 2).sum()
+            jm = 0.5 * ((KS.apply(kappa - 1e-6 * d, plan, F, bmask, kw) - u_obs) ** 2).sum()
+        fd = float((jp - jm) / 2e-6)
+        ad = float((grad * d).sum())
+        errs.append(abs(fd - ad) / abs(ad))
+    plan.close()
+    torch.cuda.empty_cache()
+    return {"problem": "p=3 512x512, kappa = exp(GRF), J = |u - u_obs|^2 / 2",
+            "seconds_forward_adjoint_gradient": t, "J": float(J), "quadrature_points": int(kappa.numel()),
+            "fd_directional_rel_err": errs}
 
 
 # --------------------------------------------------------------- our arm

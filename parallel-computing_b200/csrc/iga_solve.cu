@@ -31,6 +31,7 @@ struct DevScalars {
     double alpha, beta, rz, rr, rr0, tol2, bb;      // outer PCG
     double ialpha, ibeta, irz, irr, itol2;          // inner FEM-CG
     int done, breakdown, idone, iiters, ibreak, imax;
+    int it, maxit;                                  // outer PCG in a device-side loop
 };
 
 // ------------------------------------------------------------ reductions
@@ -314,6 +315,38 @@ __global__ void pcg_xr_kernel(T *__restrict__ x, T *__restrict__ r, const T *__r
     if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) s->rr = tot[0];
 }
 
+// Same update inside the device-side loop: counts the iteration and sets the
+// loop's condition (continue while rr > tol2, it < maxit, no breakdown, finite).
+template <typename T>
+__global__ void pcg_xr_cond_kernel(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p,
+                                   const T *__restrict__ q, long long N, DevScalars *s, double *partials,
+                                   unsigned *counter, cudaGraphConditionalHandle h)
+{
+    const T al = (T)s->alpha;
+    double v[1] = {0.0};
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
+        x[t] += al * p[t];
+        const T rv = r[t] - al * q[t];
+        r[t] = rv;
+        v[0] += (double)rv * (double)rv;
+    }
+    double tot[1];
+    if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) {
+        s->rr = tot[0];
+        s->it += 1;
+        const bool go = tot[0] > s->tol2 && s->it < s->maxit && !s->breakdown && tot[0] == tot[0];
+        cudaGraphSetConditional(h, go ? 1u : 0u);
+    }
+}
+
+__global__ void loop_init_kernel(DevScalars *s, double tol2, int maxit)
+{
+    s->tol2 = tol2;
+    s->maxit = maxit;
+    s->it = 0;
+    s->breakdown = 0;
+}
+
 // Flexible (Polak-Ribiere) beta = r.(z - z_old) / rz_old; rz = r.z.
 template <typename T>
 __global__ void pcg_beta_kernel(const T *__restrict__ r, const T *__restrict__ z, const T *__restrict__ zo, long long N,
@@ -498,6 +531,11 @@ struct PrecState {
     // exact FEM inverse: eigenvectors (column-major), eigenvalues, two work matrices
     T *Vx = nullptr, *Vy = nullptr, *lx = nullptr, *ly = nullptr, *W1 = nullptr, *W2 = nullptr;
     int nxp = 0, nyp = 0;   // transform sizes padded to multiples of 64
+    // device-side PCG loop: a CUDA graph whose conditional WHILE node runs one
+    // iteration per pass (built for one preconditioner / kappa-scaling choice)
+    cudaGraphExec_t loop = nullptr;
+    int loop_pc = -1, loop_scaled = -1;
+    bool loop_failed = false;   // the loop graph could not be instantiated: host-driven loop
     FemCoef<T> coef() const
     {
         FemCoef<T> c;
@@ -511,6 +549,7 @@ struct SolverState {
     int device = 0;
     cudaStream_t stream = nullptr;
     cublasHandle_t blas = nullptr;
+    void *blas_ws = nullptr;   // fixed cuBLAS workspace (no allocation inside graph capture)
     bool fd_host = false;
     std::vector<double> lamx, lamy, Vx, Vy;   // host eigenpairs (built once)
     double *ks64 = nullptr;                   // kappa scaling of the preconditioner
@@ -649,6 +688,7 @@ static void free_prec(PrecState<T> &ps)
     for (T *v : bufs)
         if (v) cudaFree(v);
     if (ps.chunk) cudaGraphExecDestroy(ps.chunk);
+    if (ps.loop) cudaGraphExecDestroy(ps.loop);
     ps = PrecState<T>{};
 }
 
@@ -664,6 +704,7 @@ void iga_solver_release(iga_plan *pl)
         if (v) cudaFree(v);
     if (S->h) cudaFreeHost(S->h);
     if (S->blas) cublasDestroy(S->blas);
+    if (S->blas_ws) cudaFree(S->blas_ws);
     if (S->stream) cudaStreamDestroy(S->stream);
     delete S;
     pl->solver = nullptr;
@@ -780,6 +821,12 @@ static int fd_upload(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
     if (!S->blas) {
         if (cublasCreate(&S->blas) != CUBLAS_STATUS_SUCCESS) {
             set_error("cublasCreate failed");
+            return IGA_ERR_CUDA;
+        }
+        const size_t ws = size_t(256) << 20;
+        SOLVE_TRY(cudaMalloc(&S->blas_ws, ws));
+        if (cublasSetWorkspace(S->blas, S->blas_ws, ws) != CUBLAS_STATUS_SUCCESS) {
+            set_error("cublasSetWorkspace failed");
             return IGA_ERR_CUDA;
         }
     }
@@ -953,6 +1000,114 @@ static int pcg(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_solve_o
     return IGA_ERR_NOT_CONVERGED;
 }
 
+// Builds the device-side loop for the current preconditioner choice: body =
+// q = K p; alpha; x += alpha p, r -= alpha q (+ loop condition); z_old = z;
+// z = M^-1 r; beta; p = z + beta p, on the fixed buffers of ps.
+template <typename T>
+static int build_loop(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_solve_opts &o, int prec)
+{
+    const int scaled = pl->kappa_dev ? 1 : 0;
+    if (ps.loop_pc == o.pc && ps.loop_scaled == scaled && (ps.loop || ps.loop_failed))
+        return ps.loop ? IGA_OK : IGA_ERR_UNSUPPORTED;
+    if (ps.loop) {
+        cudaGraphExecDestroy(ps.loop);
+        ps.loop = nullptr;
+    }
+    const long long N = pl->nfunc;
+    const cudaStream_t s = S->stream;
+    cudaGraph_t g;
+    SOLVE_TRY(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h;
+    SOLVE_TRY(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    SOLVE_TRY(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    SOLVE_TRY(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    int64_t dummy = 0;
+    int st = iga_apply_internal_sb(pl, prec, ps.p, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY);
+    if (!st) {
+        pcg_pq_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.q, N, S->s, S->partials, S->counter);
+        pcg_xr_cond_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.x, ps.r, ps.p, ps.q, N, S->s, S->partials, S->counter,
+                                                             h);
+        copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.zo, ps.z, N);
+        st = pc_apply(ps, pl, S, o, ps.r, ps.z, o.pc_rtol, dummy);
+    }
+    if (!st) {
+        pcg_beta_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, ps.zo, N, S->s, S->partials, S->counter);
+        pcg_p_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.z, N, S->s, 0);
+    }
+    cudaGraph_t captured = body;
+    const cudaError_t ce = cudaStreamEndCapture(s, &captured);
+    if (st || ce != cudaSuccess) {
+        cudaGraphDestroy(g);
+        if (!st) set_error(std::string("PCG loop capture: ") + cudaGetErrorString(ce));
+        return st ? st : IGA_ERR_CUDA;
+    }
+    cudaGraphInstantiateParams ip = {};
+    const cudaError_t ie = cudaGraphInstantiateWithParams(&ps.loop, g, &ip);
+    if (ie != cudaSuccess) {
+        cudaGraphNodeType t = cudaGraphNodeTypeEmpty;
+        if (ip.errNode_out) cudaGraphNodeGetType(ip.errNode_out, &t);
+        set_error(std::string("PCG loop instantiation: ") + cudaGetErrorString(ie) + " (result " +
+                  std::to_string((int)ip.result_out) + ", node type " + std::to_string((int)t) + ")");
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        ps.loop = nullptr;
+        ps.loop_pc = o.pc;
+        ps.loop_scaled = scaled;
+        ps.loop_failed = true;
+        return IGA_ERR_UNSUPPORTED;
+    }
+    cudaGraphDestroy(g);
+    ps.loop_failed = false;
+    ps.loop_pc = o.pc;
+    ps.loop_scaled = scaled;
+    return IGA_OK;
+}
+
+// Flexible PCG whose iterations run on the device: one graph launch per solve.
+template <typename T>
+static int pcg_graph(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_solve_opts &o, const T *b, T *x,
+                     double rtol, double bnorm, int prec, int &its)
+{
+    const long long N = pl->nfunc;
+    const cudaStream_t s = S->stream;
+    int st;
+    if ((st = update_kscale(pl, S))) return st;
+    if (o.pc == IGA_PC_FEM_EXACT && (st = fd_upload(ps, pl, S))) return st;
+    if (b != ps.b) copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.b, b, N);
+    if (x != ps.x) copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.x, x, N);
+    if ((st = iga_apply_internal_sb(pl, prec, ps.x, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY))) return st;
+    sub_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.b, ps.q, ps.r, N, S->s, S->partials, S->counter);
+    if ((st = sync_scalars(S))) return st;
+    if (std::sqrt(S->h->rr) <= rtol * bnorm) return IGA_OK;
+    int64_t dummy = 0;
+    if ((st = pc_apply(ps, pl, S, o, ps.r, ps.z, o.pc_rtol, dummy))) return st;
+    dot_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, N, &S->s->rz, S->partials, S->counter);
+    pcg_p_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.z, N, S->s, 1);
+    st = build_loop(pl, S, ps, o, prec);
+    if (st == IGA_ERR_UNSUPPORTED) {   // e.g. a library kernel not allowed in a conditional body
+        int64_t pcits = 0;
+        st = pcg<T>(pl, S, ps, o, ps.b, ps.x, rtol, bnorm, o.pc_rtol, prec, its, pcits);
+        if (x != ps.x) copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(x, ps.x, N);
+        return st;
+    }
+    if (st) return st;
+    loop_init_kernel<<<1, 1, 0, s>>>(S->s, rtol * rtol * bnorm * bnorm, o.max_it);
+    SOLVE_TRY(cudaGraphLaunch(ps.loop, s));
+    if (x != ps.x) copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(x, ps.x, N);
+    if ((st = sync_scalars(S))) return st;
+    its += S->h->it;
+    if (S->h->breakdown) return IGA_ERR_BREAKDOWN;
+    if (!std::isfinite(S->h->rr)) return IGA_ERR_NONFINITE;
+    return std::sqrt(S->h->rr) <= rtol * bnorm ? IGA_OK : IGA_ERR_NOT_CONVERGED;
+}
+
 // ||b - K x|| (FP64 operator), into S->h->rr and S->h->bb.
 static int true_residual(iga_plan *pl, SolverState *S, const double *b, const double *x)
 {
@@ -1122,8 +1277,10 @@ int iga_solve(iga_plan *pl, const double *b, double *x, const iga_solve_opts *o_
         if ((st = alloc_prec(S->d, pl, *S))) return st;
         // Restart from the true residual until it meets rtol (recurrence drift).
         for (int restart = 0; restart < 4 && rel > o.rtol; ++restart) {
-            st = pcg<double>(pl, S, S->d, o, b, x, o.rtol, bnorm, o.pc_rtol, IGA_FP64, stt.iterations,
-                             stt.pc_iterations);
+            st = o.pc == IGA_PC_FEM_CG
+                     ? pcg<double>(pl, S, S->d, o, b, x, o.rtol, bnorm, o.pc_rtol, IGA_FP64, stt.iterations,
+                                   stt.pc_iterations)
+                     : pcg_graph<double>(pl, S, S->d, o, b, x, o.rtol, bnorm, IGA_FP64, stt.iterations);
             if (st && st != IGA_ERR_NOT_CONVERGED) {
                 result = st;
                 break;
@@ -1142,8 +1299,10 @@ int iga_solve(iga_plan *pl, const double *b, double *x, const iga_solve_opts *o_
             const double scale = std::sqrt(S->h->rr);
             scale_down_kernel<<<kRedBlocks, kThreads, 0, S->stream>>>(S->r64, S->f.b, N, S->s);
             zero_kernel<float><<<kRedBlocks, kThreads, 0, S->stream>>>(S->f.x, N);
-            st = pcg<float>(pl, S, S->f, o, S->f.b, S->f.x, o.sweep_rtol, 1.0, o.pc_rtol, IGA_FP32, stt.iterations,
-                            stt.pc_iterations);
+            st = o.pc == IGA_PC_FEM_CG
+                     ? pcg<float>(pl, S, S->f, o, S->f.b, S->f.x, o.sweep_rtol, 1.0, o.pc_rtol, IGA_FP32,
+                                  stt.iterations, stt.pc_iterations)
+                     : pcg_graph<float>(pl, S, S->f, o, S->f.b, S->f.x, o.sweep_rtol, 1.0, IGA_FP32, stt.iterations);
             if (st && st != IGA_ERR_NOT_CONVERGED) {
                 result = st;
                 break;
