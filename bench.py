@@ -270,6 +270,7 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
     # sigma 1, squared-exponential length 0.1, seed 3), u_obs = u(exp(0.8 g)) + 1%
     # noise, J = |u - u_obs|^2 / 2; forward solve + adjoint solve + dJ/dkappa.
     out["adjoint_p3_512"] = time_adjoint(ib, torch, stream, barrier, max_over_ranks)
+    out["batched_256"] = time_batch(ib, torch, stream, barrier, max_over_ranks)
     # reference preconditioner, p=2 64x64 (the CPU-runnable configuration)
     m2 = ib.unit_square(2, 64)
     p2 = ib.Plan(m2)
@@ -283,6 +284,43 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
                                     "inner_iterations": st.pc_iterations, "relres": st.relres,
                                     "pc": "inner Jacobi-CG on the FEM matrix to 1e-10 (the reference's PCSHELL)"}
     p2.close()
+    torch.cuda.empty_cache()
+    return out
+
+
+def time_batch(ib, torch, stream, barrier, max_over_ranks):
+    """256 independent unit-square solves (p uniform in {2, 3}, element counts per
+    direction uniform in {32, 48, ..., 256}, b ~ N(0,1) with zero boundary data,
+    seed 2) in one graph launch per batch solve, to a relative true residual of
+    1e-10 per problem; FP64 PCG and FP32 PCG sweeps + FP64 refinement, exact FEM
+    preconditioner, tile shapes from the committed tuning table."""
+    shapes = ib.batch_problems(256, seed=2)
+    meshes = [ib.unit_square(p, a, c) for p, a, c in shapes]
+    b = torch.from_numpy(ib.batch_rhs(shapes, seed=2)).cuda()
+    out = {"problems": "256 unit-square Poisson solves, p in {2,3}, nElemX, nElemY in {32,48,...,256} (seed 2), "
+                       "b ~ N(0,1), rtol 1e-10 per problem",
+           "dofs": int(b.numel()), "tune_file": os.path.basename(ib.TUNE_FILE)}
+    for name, prec in (("fp64", ib.FP64), ("fp32_refine", ib.MIXED)):
+        t0 = time.perf_counter()
+        batch = ib.Batch(meshes, precision=prec, tune_file=ib.TUNE_FILE)
+        setup = time.perf_counter() - t0
+        x = torch.zeros_like(b)
+        batch.solve(b, x)   # warm-up: graph capture and instantiation
+        times, st, its = [], None, None
+        for _ in range(3):
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st, its, rel = batch.solve(b, x, stream=stream)
+            e1.record(stream)
+            barrier()
+            times.append(max_over_ranks(e0.elapsed_time(e1) / 1e3))
+        sec = statistics.median(times)
+        out[name] = {"seconds": sec, "solves_per_s": 256 / sec, "setup_seconds": setup,
+                     "converged": st.converged, "max_iterations": st.max_iterations,
+                     "mean_iterations": float(its.mean()), "max_sweeps": st.max_sweeps, "max_relres": st.max_relres}
+        batch.close()
+    out["speedup_fp32_refine_vs_fp64"] = out["fp64"]["seconds"] / out["fp32_refine"]["seconds"]
     torch.cuda.empty_cache()
     return out
 

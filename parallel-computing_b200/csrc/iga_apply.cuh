@@ -102,15 +102,17 @@ __host__ __device__ constexpr int apply_max_threads()
                           : (P <= 2 ? (GEOM ? 384 : 512) : P == 3 ? (GEOM ? 320 : 448) : (GEOM ? 256 : 320));
 }
 
+// One CTA: column strip gx, strips gyb*W .. gyb*W+W-1 of that column (one per warp).
 template <int P, typename T, int GEOM, int NST>
-__global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kernel(ApplyParams<T> a)
+__device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__restrict__ x, T *__restrict__ y, const int gx,
+                                           const int gyb)
 {
     using S = ApplyShape<P, T>;
     constexpr int NB = S::NB, NQ = S::NQ, QH = S::QH;
     const StripGrid &g = a.g;
     const int lane = threadIdx.x, w = threadIdx.y, W = blockDim.y;
     const int c = lane >> 1, h = lane & 1;
-    const int gx = blockIdx.x, gy = blockIdx.y * W + w;
+    const int gy = gyb * W + w;
 
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
@@ -162,7 +164,7 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kern
             const int R = ey0 + k, C = ex0 + lane;
             const bool v = R < g.n && C < g.m;
             const size_t gi = v ? (size_t)R * g.m + C : 0;
-            cp_async_zfill<sizeof(T)>(xr + (k % S::XR) * S::XW + lane, a.x + gi, v);
+            cp_async_zfill<sizeof(T)>(xr + (k % S::XR) * S::XW + lane, x + gi, v);
             if (GEOM == 1) cp_async_zfill<2 * sizeof(T)>(cr + ((k % S::XR) * S::XW + lane) * 2, a.CP + 2 * gi, v);
         }
         if (k >= P && k < nrows)
@@ -255,7 +257,7 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kern
     auto store = [&](int R, int C, T v) {
         const size_t i = (size_t)R * g.m + C;
         const bool bnd = (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
-        a.y[i] = bnd ? (a.bc == 1 ? a.x[i] : T(0)) : a.sign * v;
+        y[i] = bnd ? (a.bc == 1 ? x[i] : T(0)) : a.sign * v;
     };
     T *frame = a.frame + (size_t)(gx * g.NSY + gy) * g.FS;
     auto write_row = [&](int lr, const T (&r0)[QH], const T (&r1)[QH]) {
@@ -421,48 +423,97 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kern
     cp_async_wait<0>();
 }
 
+template <int P, typename T, int GEOM, int NST>
+__global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kernel(ApplyParams<T> a)
+{
+    apply_tile<P, T, GEOM, NST>(a, a.x, a.y, blockIdx.x, blockIdx.y);
+}
+
+// Many independent patches in one launch: CTA b runs work item items[b] =
+// (problem, column strip, block of W strips) with that problem's parameters,
+// or nothing when the problem is marked inactive (converged).
+template <int P, typename T, int NST>
+__global__ void __launch_bounds__(apply_max_threads<P, T, 0>(), 1)
+    apply_batch_kernel(const ApplyParams<T> *__restrict__ params, const int4 *__restrict__ items,
+                       const int *__restrict__ active, const long long *__restrict__ offs, const T *__restrict__ xb,
+                       T *__restrict__ yb)
+{
+    const int4 it = items[blockIdx.x];
+    if (!active[it.x]) return;
+    const long long o = offs[it.x];
+    apply_tile<P, T, 0, NST>(params[it.x], xb + o, yb + o, it.y, it.z);
+}
+
 // Sums the frames of the strips covering each seam control point, strip
 // (row, then column) in ascending order, and stores sign * sum (boundary
-// rules as in apply_kernel).
+// rules as in apply_kernel). idx enumerates the seam points of grid g.
+template <typename T>
+__device__ __forceinline__ void seam_point(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
+                                           const StripGrid &g, T sign, int bc, long long idx)
+{
+    const int P = g.P;
+    const long long nvc = (long long)(g.NSX - 1) * P;   // vertical seam columns
+    const long long nV = nvc * g.n;
+    int R, C;
+    if (idx < nV) {
+        const int cid = (int)(idx % nvc);
+        R = (int)(idx / nvc);
+        C = kSW * (1 + cid / P) + cid % P;
+        if (C >= g.m) return;
+    } else {
+        const long long j = idx - nV;
+        C = (int)(j % g.m);
+        const int rid = (int)(j / g.m);
+        R = g.TY * (1 + rid / P) + rid % P;
+        if (R >= g.n) return;
+        const int s = C / kSW;
+        if (C % kSW < P && s >= 1 && s < g.NSX) return;   // handled as a vertical seam
+    }
+    int fa, fb;
+    const int ca = cover(C, kSW, g.NSX, P, fa);
+    const int cb = cover(R, g.TY, g.NSY, P, fb);
+    T v = 0;
+    for (int bi = 0; bi < cb; ++bi) {
+        const int b = fb + bi;
+        for (int ai = 0; ai < ca; ++ai) {
+            const int aa = fa + ai;
+            v += frame[(size_t)(aa * g.NSY + b) * g.FS + frame_index(R - g.TY * b, C - kSW * aa, P, g.TY)];
+        }
+    }
+    const size_t i = (size_t)R * g.m + C;
+    const bool bnd = (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
+    y[i] = bnd ? (bc == 1 ? x[i] : T(0)) : sign * v;
+}
+
+__host__ __device__ __forceinline__ long long seam_count(const StripGrid &g)
+{
+    return (long long)(g.NSX - 1) * g.P * g.n + (long long)(g.NSY - 1) * g.P * g.m;
+}
+
 template <int P, typename T>
 __global__ void seam_fixup_kernel(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
                                   StripGrid g, T sign, int bc)
 {
-    const long long nvc = (long long)(g.NSX - 1) * P;   // vertical seam columns
-    const long long nV = nvc * g.n;
-    const long long nH = (long long)(g.NSY - 1) * P * g.m;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < nV + nH;
-         idx += (long long)gridDim.x * blockDim.x) {
-        int R, C;
-        if (idx < nV) {
-            const int cid = (int)(idx % nvc);
-            R = (int)(idx / nvc);
-            C = kSW * (1 + cid / P) + cid % P;
-            if (C >= g.m) continue;
-        } else {
-            const long long j = idx - nV;
-            C = (int)(j % g.m);
-            const int rid = (int)(j / g.m);
-            R = g.TY * (1 + rid / P) + rid % P;
-            if (R >= g.n) continue;
-            const int s = C / kSW;
-            if (C % kSW < P && s >= 1 && s < g.NSX) continue;   // handled as a vertical seam
-        }
-        int fa, fb;
-        const int ca = cover(C, kSW, g.NSX, P, fa);
-        const int cb = cover(R, g.TY, g.NSY, P, fb);
-        T v = 0;
-        for (int bi = 0; bi < cb; ++bi) {
-            const int b = fb + bi;
-            for (int ai = 0; ai < ca; ++ai) {
-                const int aa = fa + ai;
-                v += frame[(size_t)(aa * g.NSY + b) * g.FS + frame_index(R - g.TY * b, C - kSW * aa, P, g.TY)];
-            }
-        }
-        const size_t i = (size_t)R * g.m + C;
-        const bool bnd = (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
-        y[i] = bnd ? (bc == 1 ? x[i] : T(0)) : sign * v;
-    }
+    const long long total = seam_count(g);
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x)
+        seam_point<T>(frame, x, y, g, sign, bc, idx);
+}
+
+// Seams of every active problem of a batch: blockIdx.y = problem.
+template <typename T>
+__global__ void seam_fixup_batch_kernel(const ApplyParams<T> *__restrict__ params, const int *__restrict__ active,
+                                        const long long *__restrict__ offs, const T *__restrict__ xb,
+                                        T *__restrict__ yb)
+{
+    const int pr = blockIdx.y;
+    if (!active[pr]) return;
+    const ApplyParams<T> &a = params[pr];
+    const long long total = seam_count(a.g);
+    const long long o = offs[pr];
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x)
+        seam_point<T>(a.frame, xb + o, yb + o, a.g, a.sign, a.bc, idx);
 }
 
 }  // namespace iga

@@ -176,7 +176,7 @@ static int warps_for_g(int P)
     }
 }
 
-static int warps_for(int P, int prec, int geom)
+int warps_for(int P, int prec, int geom)
 {
     if (prec == IGA_FP64) return geom ? warps_for_g<double, 1>(P) : warps_for_g<double, 0>(P);
     return geom ? warps_for_g<float, 1>(P) : warps_for_g<float, 0>(P);

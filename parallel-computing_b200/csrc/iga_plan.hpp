@@ -29,6 +29,10 @@ struct SolverState;   // defined by the solver translation unit
 void set_error(const std::string &s);
 const std::string &last_error();
 
+// Largest warps per CTA of the apply kernel for degree P, precision
+// (IGA_FP64 / IGA_FP32) and geometry mode that fits the shared-memory budget.
+int warps_for(int P, int prec, int geom);
+
 }  // namespace iga
 
 struct iga_plan {

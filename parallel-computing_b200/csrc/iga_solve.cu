@@ -19,6 +19,7 @@
 
 #include "../../include/iga_solve.h"
 #include "iga_fastdiag.hpp"
+#include "iga_fem.hpp"
 #include "iga_plan.hpp"
 
 namespace iga {
@@ -569,7 +570,9 @@ struct SolverState {
 
 using namespace iga;
 
-static void fem_1d(const std::vector<double> &g, std::vector<double> &kd, std::vector<double> &ko,
+namespace iga {
+
+void fem_1d(const std::vector<double> &g, std::vector<double> &kd, std::vector<double> &ko,
                    std::vector<double> &md, std::vector<double> &mo)
 {
     const int n = (int)g.size();
@@ -588,7 +591,7 @@ static void fem_1d(const std::vector<double> &g, std::vector<double> &kd, std::v
     }
 }
 
-static std::vector<double> fem_nodes_1d(int p, int ne, double L)
+std::vector<double> fem_nodes_1d(int p, int ne, double L)
 {
     if (p >= 3) {   // matrix_free/preprocess_fem.cpp:38-60
         std::vector<double> S;
@@ -603,7 +606,7 @@ static std::vector<double> fem_nodes_1d(int p, int ne, double L)
 
 // Lengths of the FEM grid: mean polyline length of the control-net rows
 // (x direction) and columns (y direction); 1 x 1 on the unit square.
-static void net_lengths(const Patch &P, double &Lx, double &Ly)
+void net_lengths(const Patch &P, double &Lx, double &Ly)
 {
     double sx = 0.0, sy = 0.0;
     for (int j = 0; j < P.n; ++j)
@@ -619,6 +622,8 @@ static void net_lengths(const Patch &P, double &Lx, double &Ly)
     Lx = sx / P.n;
     Ly = sy / P.m;
 }
+
+}  // namespace iga
 
 #define SOLVE_TRY(call)                                                              \
     do {                                                                             \
@@ -754,7 +759,8 @@ static int inner_chunk_graph(PrecState<T> &ps, const iga_plan *pl, SolverState *
     return IGA_OK;
 }
 
-static void interior_pencil(const std::vector<double> &g, std::vector<double> &Kd, std::vector<double> &Ko,
+namespace iga {
+void interior_pencil(const std::vector<double> &g, std::vector<double> &Kd, std::vector<double> &Ko,
                             std::vector<double> &Md, std::vector<double> &Mo)
 {
     std::vector<double> kd, ko, md, mo;
@@ -765,6 +771,7 @@ static void interior_pencil(const std::vector<double> &g, std::vector<double> &K
     Ko.assign(ko.begin() + 1, ko.begin() + 1 + n);
     Mo.assign(mo.begin() + 1, mo.begin() + 1 + n);
 }
+}  // namespace iga
 
 // Eigenpairs of the 1-D FEM pencils on the free nodes, built once per plan.
 static int fd_setup(PrecState<double> &, const iga_plan *pl, SolverState *S)

@@ -1,4 +1,5 @@
-"""Python binding (ctypes) of the C ABI in include/iga_mf.h and include/iga_solve.h.
+"""Python binding (ctypes) of the C ABI in include/iga_mf.h, include/iga_solve.h
+and include/iga_batch.h.
 
 A thin layer for tests, the benchmark and Python users: it loads the in-tree
 libiga_b200.so (built by `make -C parallel-computing_b200`) and fails loudly if
@@ -15,6 +16,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIBPATH = os.path.join(HERE, "libiga_b200.so")
+# Tile shapes of the batched operator tuned on B200 for the 256-problem
+# p in {2, 3}, 32..256-element batch (written by iga_batch_autotune).
+TUNE_FILE = os.path.join(HERE, "tune_b200.json")
 VP = ctypes.c_void_p
 
 IGA_OK = 0
@@ -60,6 +64,16 @@ class SolveStats(ctypes.Structure):
                 ("sweeps", ctypes.c_int), ("relres", ctypes.c_double), ("seconds", ctypes.c_double)]
 
 
+class BatchOpts(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("device", ctypes.c_int), ("tune_file", ctypes.c_char_p)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("converged", ctypes.c_int), ("max_iterations", ctypes.c_int),
+                ("total_iterations", ctypes.c_int64), ("max_sweeps", ctypes.c_int),
+                ("max_relres", ctypes.c_double), ("seconds", ctypes.c_double)]
+
+
 PC_NONE, PC_FEM_CG, PC_FEM_EXACT = 0, 1, 2
 
 _LIB = None
@@ -91,6 +105,20 @@ SIGNATURES = [
     ("iga_pc_apply", ctypes.c_int, [VP, ctypes.c_int, ctypes.c_int, VP, VP, ctypes.c_double, ctypes.c_int, VP]),
     ("iga_plan_set_kappa", ctypes.c_int, [VP, VP, VP]),
     ("iga_adjoint_grad", ctypes.c_int, [VP, VP, VP, VP, VP]),
+    ("iga_batch_opts_default", None, [ctypes.POINTER(BatchOpts)]),
+    ("iga_batch_create", ctypes.c_int, [VP, ctypes.c_int, ctypes.POINTER(BatchOpts), ctypes.POINTER(VP)]),
+    ("iga_batch_destroy", ctypes.c_int, [VP]),
+    ("iga_batch_offsets", ctypes.c_int, [VP, VP]),
+    ("iga_batch_plan", VP, [VP, ctypes.c_int]),
+    ("iga_batch_shape", ctypes.c_int, [VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
+    ("iga_batch_apply", ctypes.c_int, [VP, ctypes.c_int, VP, VP, VP]),
+    ("iga_batch_pc_apply", ctypes.c_int, [VP, ctypes.c_int, ctypes.c_int, VP, VP, VP]),
+    ("iga_batch_solve", ctypes.c_int, [VP, VP, VP, ctypes.POINTER(SolveOpts), ctypes.POINTER(BatchStats), VP, VP,
+                                       VP]),
+    ("iga_batch_autotune", ctypes.c_int, [VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]),
+    ("iga_tune_lookup", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
 ]
 
 
@@ -165,16 +193,22 @@ def quarter_annulus(p, nex, ney=None, r_in=1.0, r_out=2.0):
                 h1=np.full(nex, 1.0 / nex), h2=np.full(ney, 1.0 / ney))
 
 
-def splitmix_normal(seed, n, offset=0):
-    """N(0,1) from the SplitMix64 counter stream (Box-Muller on consecutive pairs)."""
-    m = (n + 1) // 2
-    i = np.arange(2 * offset + 1, 2 * offset + 2 * m + 1, dtype=np.uint64)
+def splitmix_uniform(seed, n, offset=0):
+    """u53 in [0, 1) from the SplitMix64 counter stream (entries offset .. offset+n-1)."""
+    i = np.arange(offset + 1, offset + n + 1, dtype=np.uint64)
     with np.errstate(over="ignore"):
         z = np.uint64(seed) + i * np.uint64(0x9E3779B97F4A7C15)
         z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
         z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
         z = z ^ (z >> np.uint64(31))
-    u = (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+    return (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+
+
+def splitmix_normal(seed, n, offset=0):
+    """N(0,1) from the SplitMix64 counter stream (Box-Muller on consecutive
+    pairs; offset counts pairs)."""
+    m = (n + 1) // 2
+    u = splitmix_uniform(seed, 2 * m, 2 * offset)
     r = np.sqrt(-2.0 * np.log(1.0 - u[0::2]))
     out = np.empty(2 * m)
     out[0::2] = r * np.cos(2 * np.pi * u[1::2])
@@ -206,6 +240,144 @@ def grf_qp(mesh, sigma=1.0, ell=0.1, seed=3):
     return np.ascontiguousarray(G).ravel()
 
 
+def _mesh_desc(mesh, keep, IEN=None, ID=None, Dir=None):
+    """iga_mesh_desc of a mesh dict; the arrays it points to are appended to keep."""
+    def arr(v, dt=np.float64):
+        if v is None:
+            return None
+        a = np.ascontiguousarray(v, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    d = MeshDesc()
+    d.p, d.q, d.nElemX, d.nElemY = mesh["p"], mesh.get("q", mesh["p"]), mesh["nex"], mesh["ney"]
+    d.CP = arr(mesh["CP"])
+    d.weights = arr(mesh.get("W"))
+    d.C1 = arr(mesh.get("C1"))
+    d.C2 = arr(mesh.get("C2"))
+    d.h1 = arr(mesh.get("h1"))
+    d.h2 = arr(mesh.get("h2"))
+    d.IEN = arr(IEN, np.int32)
+    d.ID = arr(ID, np.int32)
+    d.Dir = arr(Dir, np.int32)
+    d.nDir = 0 if Dir is None else len(Dir)
+    d.kappa = arr(mesh.get("kappa"))
+    return d
+
+
+def batch_problems(count=256, seed=2, sizes=tuple(range(32, 257, 16)), degrees=(2, 3)):
+    """Shapes of a batch of unit-square problems: per problem the degree and the
+    element counts per direction, each drawn uniformly (SplitMix64 stream of
+    `seed`: three draws per problem, degree, nElemX, nElemY). Returns a list of
+    (p, nex, ney)."""
+    u = splitmix_uniform(seed, 3 * count).reshape(count, 3)
+    out = []
+    for a, b, c in u:
+        out.append((int(degrees[min(int(a * len(degrees)), len(degrees) - 1)]),
+                    int(sizes[min(int(b * len(sizes)), len(sizes) - 1)]),
+                    int(sizes[min(int(c * len(sizes)), len(sizes) - 1)])))
+    return out
+
+
+def batch_rhs(shapes, seed=2):
+    """Concatenated right-hand sides: N(0,1) entries (SplitMix64 normal stream
+    of `seed`, one contiguous slice per problem in batch order) with zeros on
+    the boundary ring (homogeneous Dirichlet data)."""
+    parts, off = [], 0
+    for p, nex, ney in shapes:
+        m, n = nex + p, ney + p
+        b = splitmix_normal(seed, m * n, offset=off).reshape(n, m)
+        off += (m * n + 1) // 2
+        b[0, :] = b[-1, :] = 0.0
+        b[:, 0] = b[:, -1] = 0.0
+        parts.append(b.ravel())
+    return np.concatenate(parts)
+
+
+class Batch:
+    """Owns an iga_batch: many independent unit-square-type problems solved together."""
+
+    def __init__(self, meshes, precision=FP64, device=0, tune_file=None):
+        L = _lib()
+        keep = []
+        descs = (MeshDesc * len(meshes))()
+        for i, m in enumerate(meshes):
+            descs[i] = _mesh_desc(m, keep)
+        o = BatchOpts()
+        L.iga_batch_opts_default(ctypes.byref(o))
+        o.precision, o.device = precision, device
+        o.tune_file = tune_file.encode() if tune_file else None
+        h = VP()
+        _check(L.iga_batch_create(descs, len(meshes), ctypes.byref(o), ctypes.byref(h)), "iga_batch_create")
+        self.h = h
+        self.count = len(meshes)
+        self.precision = precision
+        offs = np.empty(self.count + 1, dtype=np.int64)
+        _check(L.iga_batch_offsets(h, _ptr(offs)), "iga_batch_offsets")
+        self.offsets = offs
+        self.ntot = int(offs[-1])
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().iga_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def plan_handle(self, i):
+        return _lib().iga_batch_plan(self.h, i)
+
+    def shape(self, i, precision=FP64):
+        r, w = ctypes.c_int(), ctypes.c_int()
+        _check(_lib().iga_batch_shape(self.h, i, precision, ctypes.byref(r), ctypes.byref(w)), "iga_batch_shape")
+        return r.value, w.value
+
+    def apply(self, x, y, precision=FP64, stream=None):
+        _check(_lib().iga_batch_apply(self.h, precision, _ptr(x), _ptr(y), _stream(stream)), "iga_batch_apply")
+
+    def pc_apply(self, r, z, pc=PC_FEM_EXACT, precision=FP64, stream=None):
+        _check(_lib().iga_batch_pc_apply(self.h, pc, precision, _ptr(r), _ptr(z), _stream(stream)),
+               "iga_batch_pc_apply")
+
+    def solve(self, b, x, stream=None, check=True, **kw):
+        """Solve every problem; returns (BatchStats, iterations[count], relres[count])."""
+        o = SolveOpts()
+        _lib().iga_solve_opts_default(ctypes.byref(o))
+        o.pc = PC_FEM_EXACT
+        for k, v in kw.items():
+            setattr(o, k, v)
+        st = BatchStats()
+        its = np.zeros(self.count, dtype=np.int32)
+        rel = np.zeros(self.count)
+        status = _lib().iga_batch_solve(self.h, _ptr(b), _ptr(x), ctypes.byref(o), ctypes.byref(st), _ptr(its),
+                                        _ptr(rel), _stream(stream))
+        if check:
+            _check(status, "iga_batch_solve")
+        return st, its, rel
+
+
+def batch_autotune(meshes, tune_file, precision=FP64, device=0):
+    """Times candidate tile shapes for these problems and merges the winners into tune_file."""
+    keep = []
+    descs = (MeshDesc * len(meshes))()
+    for i, m in enumerate(meshes):
+        descs[i] = _mesh_desc(m, keep)
+    _check(_lib().iga_batch_autotune(descs, len(meshes), precision, device, tune_file.encode()),
+           "iga_batch_autotune")
+
+
+def tune_lookup(tune_file, p, precision, nex, ney):
+    """(rows_per_strip, warps_per_cta) the tuning table gives (0 = no entry); host only."""
+    r, w = ctypes.c_int(), ctypes.c_int()
+    _check(_lib().iga_tune_lookup(tune_file.encode(), p, precision, nex, ney, ctypes.byref(r), ctypes.byref(w)),
+           "iga_tune_lookup")
+    return r.value, w.value
+
+
 class Plan:
     """Owns an iga_plan (device tables, precomputed geometry)."""
 
@@ -213,27 +385,7 @@ class Plan:
                  bc=BC_REFERENCE, device=0, rows_per_strip=0, IEN=None, ID=None, Dir=None):
         L = _lib()
         self._keep = []
-
-        def arr(v, dt=np.float64):
-            if v is None:
-                return None
-            a = np.ascontiguousarray(v, dtype=dt)
-            self._keep.append(a)
-            return a.ctypes.data
-
-        d = MeshDesc()
-        d.p, d.q, d.nElemX, d.nElemY = mesh["p"], mesh.get("q", mesh["p"]), mesh["nex"], mesh["ney"]
-        d.CP = arr(mesh["CP"])
-        d.weights = arr(mesh.get("W"))
-        d.C1 = arr(mesh.get("C1"))
-        d.C2 = arr(mesh.get("C2"))
-        d.h1 = arr(mesh.get("h1"))
-        d.h2 = arr(mesh.get("h2"))
-        d.IEN = arr(IEN, np.int32)
-        d.ID = arr(ID, np.int32)
-        d.Dir = arr(Dir, np.int32)
-        d.nDir = 0 if Dir is None else len(Dir)
-        d.kappa = arr(mesh.get("kappa"))
+        d = _mesh_desc(mesh, self._keep, IEN, ID, Dir)
         o = Opts()
         L.iga_opts_default(ctypes.byref(o))
         o.precision, o.geometry, o.sign, o.bc, o.device, o.rows_per_strip = (
