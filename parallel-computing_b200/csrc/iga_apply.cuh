@@ -447,11 +447,10 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, 0>(), 1)
 // Sums the frames of the strips covering each seam control point, strip
 // (row, then column) in ascending order, and stores sign * sum (boundary
 // rules as in apply_kernel). idx enumerates the seam points of grid g.
-template <typename T>
+template <int P, typename T>
 __device__ __forceinline__ void seam_point(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
                                            const StripGrid &g, T sign, int bc, long long idx)
 {
-    const int P = g.P;
     const long long nvc = (long long)(g.NSX - 1) * P;   // vertical seam columns
     const long long nV = nvc * g.n;
     int R, C;
@@ -497,7 +496,16 @@ __global__ void seam_fixup_kernel(const T *__restrict__ frame, const T *__restri
     const long long total = seam_count(g);
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x)
-        seam_point<T>(frame, x, y, g, sign, bc, idx);
+        seam_point<P, T>(frame, x, y, g, sign, bc, idx);
+}
+
+template <int P, typename T>
+__device__ __forceinline__ void seam_loop(const ApplyParams<T> &a, const T *__restrict__ x, T *__restrict__ y)
+{
+    const long long total = seam_count(a.g);
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x)
+        seam_point<P, T>(a.frame, x, y, a.g, a.sign, a.bc, idx);
 }
 
 // Seams of every active problem of a batch: blockIdx.y = problem.
@@ -509,11 +517,14 @@ __global__ void seam_fixup_batch_kernel(const ApplyParams<T> *__restrict__ param
     const int pr = blockIdx.y;
     if (!active[pr]) return;
     const ApplyParams<T> &a = params[pr];
-    const long long total = seam_count(a.g);
     const long long o = offs[pr];
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x)
-        seam_point<T>(a.frame, xb + o, yb + o, a.g, a.sign, a.bc, idx);
+    switch (a.g.P) {
+    case 1: seam_loop<1, T>(a, xb + o, yb + o); break;
+    case 2: seam_loop<2, T>(a, xb + o, yb + o); break;
+    case 3: seam_loop<3, T>(a, xb + o, yb + o); break;
+    case 4: seam_loop<4, T>(a, xb + o, yb + o); break;
+    default: seam_loop<5, T>(a, xb + o, yb + o); break;
+    }
 }
 
 }  // namespace iga

@@ -374,27 +374,69 @@ struct FdProb {
     int m, n, nx, ny;
 };
 
+// Tensor-core tiles: FP64 through DMMA (mma.sync m8n8k4, FP64 accumulate),
+// FP32 through TF32 MMA (mma.sync m16n8k8, operands rounded to TF32 once when
+// staged, FP32 accumulate): the FP32 preconditioner only has to be a close
+// SPD approximation of K_fem^-1 (the flexible PCG and the FP64 refinement
+// absorb the difference).
+__device__ __forceinline__ void mma_tile(double (&d)[2], double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void mma_tile(float (&d)[4], const float (&a)[4], const float (&b)[2])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(__float_as_uint(a[0])), "r"(__float_as_uint(a[1])), "r"(__float_as_uint(a[2])),
+          "r"(__float_as_uint(a[3])), "r"(__float_as_uint(b[0])), "r"(__float_as_uint(b[1])));
+}
+
+__device__ __forceinline__ double to_operand(double v) { return v; }
+__device__ __forceinline__ float to_operand(float v)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+    return __uint_as_float(r);
+}
+
+// 64 x 64 output tile of one problem per CTA of 4 warps (2 x 2 warp tiles of
+// 32 x 32). Operands contiguous along k in memory are staged as [row][k]
+// (ld 20), the others as [k][row] (ld 72): both make the fragment loads of a
+// warp conflict-free. Row / column blocks entirely outside the problem skip
+// their MMAs.
 template <typename T, int STAGE>
-__global__ void __launch_bounds__(256) fd_gemm_kernel(const FdProb<T> *__restrict__ fps, const int4 *__restrict__ tiles,
+__global__ void __launch_bounds__(128) fd_gemm_kernel(const FdProb<T> *__restrict__ fps, const int4 *__restrict__ tiles,
                                                       const int *__restrict__ act, const T *__restrict__ rb,
                                                       T *__restrict__ zb)
 {
-    __shared__ T As[2][kTK][kTile + 1];
-    __shared__ T Bs[2][kTK][kTile + 1];
+    constexpr bool A_KF = STAGE == 1;   // A contiguous along k: staged [a][k]
+    constexpr bool B_KF = STAGE != 4;   // B contiguous along k: staged [b][k]
+    constexpr int LKF = 20, LRF = 72;
+    constexpr int SA = A_KF ? kTile * LKF : kTK * LRF;
+    constexpr int SB = B_KF ? kTile * LKF : kTK * LRF;
+    __shared__ __align__(16) T As[2][SA];
+    __shared__ __align__(16) T Bs[2][SB];
     const int4 tl = tiles[blockIdx.x];
     if (!act[tl.x]) return;
     const FdProb<T> &f = fps[tl.x];
     const int nx = f.nx, ny = f.ny, m = f.m;
     const int K = (STAGE == 1 || STAGE == 3) ? nx : ny;
     const int a0 = tl.y * kTile, b0 = tl.z * kTile;
-    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int wm = (w & 1) * 32, wn = (w >> 1) * 32;
     const T *r = rb + f.off;
     T *z = zb + f.off;
 
     if (STAGE == 1 && tl.y == 0 && tl.z == 0) {   // boundary ring: identity rows of K_fem
         const int n = f.n;
         const int nb = 2 * m + 2 * (n - 2);
-        for (int u = t; u < nb; u += 256) {
+        for (int u = tid; u < nb; u += 128) {
             int idx;
             if (u < m) idx = u;
             else if (u < 2 * m) idx = (n - 1) * m + (u - m);
@@ -406,7 +448,6 @@ __global__ void __launch_bounds__(256) fd_gemm_kernel(const FdProb<T> *__restric
         }
     }
 
-    // Operand element loaders (zero outside the matrices).
     auto ldA = [&](int a, int k) -> T {
         if (a >= nx || k >= K) return T(0);
         if (STAGE == 1) return f.Vx[(size_t)a * nx + k];          // Vx^T
@@ -420,37 +461,57 @@ __global__ void __launch_bounds__(256) fd_gemm_kernel(const FdProb<T> *__restric
         if (STAGE == 3) return f.W2[(size_t)b * nx + k];          // W2
         return f.Vy[(size_t)k * ny + b];                          // Vy^T
     };
-    // Coalesced fetch order: along a for column-major A, along k otherwise.
-    constexpr bool A_A_FAST = STAGE != 1;
-    constexpr bool B_B_FAST = STAGE == 4;
-    T ra[4], rbv[4];
+    // element (row, k) of this thread's i-th fetch, coalesced along the contiguous index
+    auto coord = [&](bool kf, int i, int &row, int &k) {
+        if (kf) {
+            k = tid & 15;
+            row = (tid >> 4) + 8 * i;
+        } else {
+            row = tid & 63;
+            k = (tid >> 6) + 2 * i;
+        }
+    };
+    T ra[8], rbv[8];
     auto fetch = [&](int k0) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int a = A_A_FAST ? (t & 63) : (t >> 4) + 16 * i;
-            const int k = A_A_FAST ? (t >> 6) + 4 * i : (t & 15);
-            ra[i] = ldA(a0 + a, k0 + k);
-            const int b = B_B_FAST ? (t & 63) : (t >> 4) + 16 * i;
-            const int kb = B_B_FAST ? (t >> 6) + 4 * i : (t & 15);
-            rbv[i] = ldB(k0 + kb, b0 + b);
+        for (int i = 0; i < 8; ++i) {
+            int row, k;
+            coord(A_KF, i, row, k);
+            ra[i] = ldA(a0 + row, k0 + k);
+            coord(B_KF, i, row, k);
+            rbv[i] = ldB(k0 + k, b0 + row);
         }
     };
     auto stash = [&](int buf) {
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int a = A_A_FAST ? (t & 63) : (t >> 4) + 16 * i;
-            const int k = A_A_FAST ? (t >> 6) + 4 * i : (t & 15);
-            As[buf][k][a] = ra[i];
-            const int b = B_B_FAST ? (t & 63) : (t >> 4) + 16 * i;
-            const int kb = B_B_FAST ? (t >> 6) + 4 * i : (t & 15);
-            Bs[buf][kb][b] = rbv[i];
+        for (int i = 0; i < 8; ++i) {
+            int row, k;
+            coord(A_KF, i, row, k);
+            As[buf][A_KF ? row * LKF + k : k * LRF + row] = to_operand(ra[i]);
+            coord(B_KF, i, row, k);
+            Bs[buf][B_KF ? row * LKF + k : k * LRF + row] = to_operand(rbv[i]);
         }
     };
-    T acc[4][4];
+    auto Aat = [&](int buf, int row, int k) -> T { return As[buf][A_KF ? row * LKF + k : k * LRF + row]; };
+    auto Bat = [&](int buf, int k, int col) -> T { return Bs[buf][B_KF ? col * LKF + k : k * LRF + col]; };
+
+    constexpr bool F64 = sizeof(T) == 8;
+    constexpr int MB = F64 ? 4 : 2;      // row blocks of the warp tile (8 or 16 rows)
+    constexpr int RB = F64 ? 8 : 16;
+    constexpr int NACC = F64 ? 2 : 4;
+    T acc[MB][4][NACC];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < MB; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int c = 0; c < NACC; ++c) acc[i][j][c] = T(0);
+    bool rv[MB], cv[4];
+#pragma unroll
+    for (int i = 0; i < MB; ++i) rv[i] = a0 + wm + i * RB < nx;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cv[j] = b0 + wn + j * 8 < ny;
+
     const int nk = (K + kTK - 1) / kTK;
     fetch(0);
     stash(0);
@@ -458,35 +519,63 @@ __global__ void __launch_bounds__(256) fd_gemm_kernel(const FdProb<T> *__restric
     for (int kt = 0; kt < nk; ++kt) {
         const int buf = kt & 1;
         if (kt + 1 < nk) fetch((kt + 1) * kTK);
+        if constexpr (F64) {
 #pragma unroll
-        for (int k = 0; k < kTK; ++k) {
-            T av[4], bv[4];
+            for (int kk = 0; kk < kTK; kk += 4) {
+                double av[4], bv[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) av[i] = As[buf][k][tx + 16 * i];
+                for (int i = 0; i < 4; ++i) av[i] = Aat(buf, wm + i * 8 + g, kk + t4);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) bv[j] = Bs[buf][k][ty + 16 * j];
+                for (int j = 0; j < 4; ++j) bv[j] = Bat(buf, kk + t4, wn + j * 8 + g);
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+                for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+                    for (int j = 0; j < 4; ++j)
+                        if (rv[i] && cv[j]) mma_tile(reinterpret_cast<double(&)[2]>(acc[i][j]), av[i], bv[j]);
+            }
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < kTK; kk += 8) {
+                float av[2][4], bv[4][2];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const int r0 = wm + i * 16 + g;
+                    av[i][0] = Aat(buf, r0, kk + t4);
+                    av[i][1] = Aat(buf, r0 + 8, kk + t4);
+                    av[i][2] = Aat(buf, r0, kk + t4 + 4);
+                    av[i][3] = Aat(buf, r0 + 8, kk + t4 + 4);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    bv[j][0] = Bat(buf, kk + t4, wn + j * 8 + g);
+                    bv[j][1] = Bat(buf, kk + t4 + 4, wn + j * 8 + g);
+                }
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (rv[i] && cv[j]) mma_tile(reinterpret_cast<float(&)[4]>(acc[i][j]), av[i], bv[j]);
+            }
         }
         if (kt + 1 < nk) stash(buf ^ 1);
         __syncthreads();
     }
+    // accumulator element c of block (i, j): row i*RB + g (+8 for c >= 2 in
+    // FP32), column j*8 + 2 t4 + (c & 1)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int b = b0 + ty + 16 * j;
-        if (b >= ny) continue;
+    for (int i = 0; i < MB; ++i)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int a = a0 + tx + 16 * i;
-            if (a >= nx) continue;
-            const T c = acc[i][j];
-            if (STAGE == 1 || STAGE == 3) f.W1[(size_t)b * nx + a] = c;
-            else if (STAGE == 2) f.W2[(size_t)b * nx + a] = c / (f.lx[a] + f.ly[b]);
-            else z[(size_t)(b + 1) * m + (a + 1)] = c;
-        }
-    }
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int c = 0; c < NACC; ++c) {
+                const int a = a0 + wm + i * RB + g + (c >> 1) * 8;
+                const int b = b0 + wn + j * 8 + 2 * t4 + (c & 1);
+                if (a >= nx || b >= ny) continue;
+                const T v = acc[i][j][c];
+                if (STAGE == 1 || STAGE == 3) f.W1[(size_t)b * nx + a] = v;
+                else if (STAGE == 2) f.W2[(size_t)b * nx + a] = v / (f.lx[a] + f.ly[b]);
+                else z[(size_t)(b + 1) * m + (a + 1)] = v;
+            }
 }
 
 // ------------------------------------------------------------ host state
@@ -671,10 +760,10 @@ int batch_pc(iga_batch *B, int pc, const T *r, T *z, const int *act, cudaStream_
         bk_copy<T><<<B->nchunks, kBT, 0, s>>>(d, act, r, z);
     } else {
         const FdProb<T> *fd = vecs<T>(B).fd;
-        fd_gemm_kernel<T, 1><<<B->ntiles, 256, 0, s>>>(fd, B->tiles, act, r, z);
-        fd_gemm_kernel<T, 2><<<B->ntiles, 256, 0, s>>>(fd, B->tiles, act, r, z);
-        fd_gemm_kernel<T, 3><<<B->ntiles, 256, 0, s>>>(fd, B->tiles, act, r, z);
-        fd_gemm_kernel<T, 4><<<B->ntiles, 256, 0, s>>>(fd, B->tiles, act, r, z);
+        fd_gemm_kernel<T, 1><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
+        fd_gemm_kernel<T, 2><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
+        fd_gemm_kernel<T, 3><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
+        fd_gemm_kernel<T, 4><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
     }
     BT_TRY(cudaGetLastError());
     return IGA_OK;

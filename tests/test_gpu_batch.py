@@ -77,7 +77,9 @@ def test_batch_apply_matches_oracle(torch_cuda, ib, orc):
         assert rel(y[a:b], orc.apply_mf(m, x[a:b], sign=1.0, bc=1)) < 1e-12
 
 
-@pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 2e-5)])
+# FP64 GEMMs (DMMA) match the single-problem cuBLAS DGEMMs to rounding; the FP32
+# preconditioner runs its GEMMs on TF32 operands (10-bit mantissa).
+@pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 1e-2)])
 def test_batch_preconditioner_matches_single(torch_cuda, ib, prec, tol):
     torch = torch_cuda
     meshes = meshes_of(ib, SHAPES)
