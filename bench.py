@@ -200,7 +200,7 @@ def reference_arm(args):
     out = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "GDOF/s", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "matmul_c2_p3_2048x2048_fp64", "p": P, "nElem": [NE, NE],
+           "config": {"workload": f"matmul_p3_{NE}x{NE}_fp64_precomputed_geometry", "p": P, "nElem": [NE, NE],
                       "dofs": (NE + P) ** 2, "reference_path": "matrix_free ElementMF+LocalAssemblyMF (CPU)"},
            "cpu_baseline": {"value": rate, "unit": "GDOF/s", "cores": threads, "kind": kind, "sample": sample},
            "e2e": {"value": rate, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -274,18 +274,20 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
     # noise, J = |u - u_obs|^2 / 2; forward solve + adjoint solve + dJ/dkappa.
     out["adjoint_p3_512"] = time_adjoint(ib, torch, stream, barrier, max_over_ranks)
     out["batched_256"] = time_batch(ib, torch, stream, barrier, max_over_ranks)
-    # reference preconditioner, p=2 64x64 (the CPU-runnable configuration)
+    # reference preconditioner, p=2 64x64 (the CPU-runnable configuration), for
+    # f = 2 pi^2 sin sin and for the reference's own load x(1-x)y(1-y)
     m2 = ib.unit_square(2, 64)
     p2 = ib.Plan(m2)
     b2 = torch.empty(p2.nfunc, dtype=torch.float64, device="cuda")
-    p2.rhs(b2, ib.F_SINSIN)
     x2 = torch.zeros_like(b2)
-    p2.solve(b2, x2, pc=ib.PC_FEM_CG)
-    x2.zero_()
-    st = p2.solve(b2, x2, pc=ib.PC_FEM_CG)
-    out["p2_64x64_reference_pc"] = {"seconds": st.seconds, "iterations": st.iterations,
-                                    "inner_iterations": st.pc_iterations, "relres": st.relres,
-                                    "pc": "inner Jacobi-CG on the FEM matrix to 1e-10 (the reference's PCSHELL)"}
+    ref_pc = {"pc": "inner Jacobi-CG on the FEM matrix to 1e-10 (the reference's PCSHELL)"}
+    for name, fk in (("f_sinsin", ib.F_SINSIN), ("f_reference", ib.F_REFERENCE)):
+        p2.rhs(b2, fk)
+        p2.solve(b2, x2, pc=ib.PC_FEM_CG)
+        st = p2.solve(b2, x2, pc=ib.PC_FEM_CG)
+        ref_pc[name] = {"seconds": st.seconds, "iterations": st.iterations, "inner_iterations": st.pc_iterations,
+                        "relres": st.relres}
+    out["p2_64x64_reference_pc"] = ref_pc
     p2.close()
     torch.cuda.empty_cache()
     return out
@@ -464,6 +466,28 @@ def our_arm(args):
             "algo_bytes_per_step": plan_mf.info.algo_bytes_f64, "l2": "flushed between timed applies"}
         plan_mf.close()
         del flush
+        torch.cuda.empty_cache()
+        # FP32 operator (precomputed FP32 G): the operator of the mixed-precision sweeps
+        plan32 = ib.Plan(mesh, precision=ib.FP32, geometry=ib.GEOM_PRECOMPUTED)
+        x32, y32 = xd.float(), torch.empty(N, dtype=torch.float32, device="cuda")
+        for _ in range(args.warmup):
+            plan32.apply(x32, y32, stream)
+        barrier()
+        k32 = max(1, min(args.steps, 200))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k32):
+            plan32.apply(x32, y32, stream)
+        e1.record(stream)
+        barrier()
+        ms32 = max_over_ranks(e0.elapsed_time(e1))
+        variants["fp32_precomputed_geometry"] = {
+            "value": ws * N * k32 / (ms32 * 1e-3) / 1e9, "unit": "GDOF/s", "ms_per_step": ms32 / k32,
+            "algo_bytes_per_step": plan32.info.algo_bytes_f32,
+            "achieved_gbs": plan32.info.algo_bytes_f32 / (ms32 / k32 * 1e-3) / 1e9,
+            "l2": "inputs larger than L2 (0.8 GB of FP32 geometry per apply)"}
+        plan32.close()
+        del x32, y32
         torch.cuda.empty_cache()
 
     plan = ib.Plan(mesh, geometry=ib.GEOM_PRECOMPUTED)
