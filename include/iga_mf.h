@@ -54,7 +54,10 @@ enum {
 enum { IGA_FP64 = 0, IGA_FP32 = 1, IGA_MIXED = 2 };          /* operator precision(s) */
 enum { IGA_GEOM_PRECOMPUTED = 0, IGA_GEOM_ON_THE_FLY = 1 };  /* mult_sf / mult_mf paths */
 enum { IGA_SIGN_REFERENCE = -1, IGA_SIGN_SPD = 1 };
-enum { IGA_BC_REFERENCE = 0, IGA_BC_IDENTITY = 1 };           /* y[Dir]=0 / y[Dir]=x[Dir] */
+/* y[Dir]=0 / y[Dir]=x[Dir] / no boundary rows: every row is the full sum over
+ * the patch's elements and x is read everywhere (the sub-patch of one part of
+ * a partitioned mesh, whose ring rows are partial sums; include/iga_part.h) */
+enum { IGA_BC_REFERENCE = 0, IGA_BC_IDENTITY = 1, IGA_BC_NONE = 2 };
 enum { IGA_F_REFERENCE = 0, IGA_F_SINSIN = 1, IGA_F_ANNULUS = 2 }; /* load functions */
 
 /* One single-patch tensor-product mesh, in the reference's arrays (all HOST
@@ -80,7 +83,7 @@ typedef struct {
     int precision;  /* IGA_FP64, IGA_FP32 or IGA_MIXED (both operators) */
     int geometry;   /* IGA_GEOM_PRECOMPUTED or IGA_GEOM_ON_THE_FLY */
     int sign;       /* IGA_SIGN_REFERENCE (default for the drop-in) or IGA_SIGN_SPD */
-    int bc;         /* IGA_BC_REFERENCE or IGA_BC_IDENTITY */
+    int bc;         /* IGA_BC_REFERENCE, IGA_BC_IDENTITY or IGA_BC_NONE */
     int device;     /* CUDA device ordinal */
     int rows_per_strip; /* element rows per warp strip, 0 = default (tuned) */
 } iga_opts;

@@ -299,12 +299,12 @@ void orc_apply_mf(const orc_patch *P, const double *x, double *y, double sign, i
             for (int j = 0; j <= q; ++j)
                 for (int i = 0; i <= p; ++i) {
                     const int I = ex + i, J = ey + j;
-                    if (!on_boundary(I, J, m, nn)) y[(size_t)J * m + I] += ye[j * (p + 1) + i];
+                    if (bc == 2 || !on_boundary(I, J, m, nn)) y[(size_t)J * m + I] += ye[j * (p + 1) + i];
                 }
         }
     for (int J = 0; J < nn; ++J)
         for (int I = 0; I < m; ++I)
-            if (on_boundary(I, J, m, nn)) y[(size_t)J * m + I] = (bc == 1) ? x[(size_t)J * m + I] : 0.0;
+            if (bc != 2 && on_boundary(I, J, m, nn)) y[(size_t)J * m + I] = (bc == 1) ? x[(size_t)J * m + I] : 0.0;
 }
 
 /* The reference mult_sf: ElementMFSF::GenerateElement (matrix_free/src/ElementMFSF.cpp:237-297:

@@ -47,7 +47,8 @@ typedef struct {
  * (ElementMF::GenerateElementSingleQP + LocalAssemblyMF::LocalMatMulMF, loop of
  * GlobalAssemblyMF::MatMulMF). sign = -1 is the reference operator. Boundary
  * rows: bc = 0 -> y[Dir] = 0 (matrix-free reference), bc = 1 -> y[Dir] = x[Dir]
- * with x[Dir] not read (the SPD operator the solver uses). */
+ * with x[Dir] not read (the SPD operator the solver uses), bc = 2 -> no
+ * boundary rule (every row the full element sum: one part's sub-patch). */
 void orc_apply_mf(const orc_patch *P, const double *x, double *y, double sign, int bc);
 /* Reference mult_sf formula (LocalAssemblyMFSF::LocalMatMulMF); y[Dir] = 0. */
 void orc_apply_sf(const orc_patch *P, const double *x, double *y, double sign);

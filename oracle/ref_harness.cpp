@@ -24,7 +24,15 @@
 //   * Control points: ControlPointGenerator needs Eigen (absent); its output
 //     for the linear parameterisation equals the degree-p Greville abscissae,
 //     which are computed here with the reference's AbscissaeGenerator.
+//   * Partitioned meshes: matrix_free/preprocess.cpp:16-87 drives the
+//     reference's own Partition + FileManager (compiled unmodified) to write
+//     info.txt and <base>_<rank>.txt; the partitioned MatMulMF restates the
+//     glue of matrix_free/src/GlobalAssemblyMF.cpp:141-210 with the PETSc
+//     ghosted vector replaced by arrays: local form = owned entries (the
+//     part's contiguous range of the partition numbering) then the ghosts
+//     (ghostID), y scattered to global indices ID >= 0, then y[Dir] = 0.
 #include <cstring>
+#include <string>
 #include <cmath>
 #include <thread>
 #include <vector>
@@ -35,12 +43,14 @@
 #include "ElementFEM.hpp"
 #include "ElementMF.hpp"
 #include "ElementMFSF.hpp"
+#include "FileManager.hpp"
 #include "IDGenerator.hpp"
 #include "IENGenerator.hpp"
 #include "LocalAssembly.hpp"
 #include "LocalAssemblyMF.hpp"
 #include "LocalAssemblyMFSF.hpp"
 #include "NURBSExtractionGenerator.hpp"
+#include "Partition.hpp"
 #include "QuadraturePoint.hpp"
 
 namespace {
@@ -359,6 +369,85 @@ int ref_fem_matvec(int nfx, int nfy, const double *CP, const int *IEN, const int
         }
     for (int d = 0; d < nDir; ++d) y[Dir[d]] += x[Dir[d]];
     return 0;
+}
+
+// info.txt and the partition files of matrix_free/preprocess.cpp, written by
+// the reference's Partition / FileManager into dir (files dir/<base>_<rank>.txt).
+int ref_write_partition(int p, int q, int nex, int ney, double Lx, double Ly, int part_num_1d, const char *dir,
+                        const char *base)
+{
+    const std::vector<double> S = open_knots(p, nex, Lx), T = open_knots(q, ney, Ly);
+    BSplineBasis b1(p, S), b2(q, T);
+    IENGenerator ig;
+    IDGenerator idg;
+    NURBSExtractionGenerator ng;
+    AbscissaeGenerator ag;
+    const auto ien = ig.GenerateIEN2D(&b1, &b2);
+    const auto id = idg.GenerateID2D(&b1, &b2);
+    const auto g1 = ag.GrevilleAbscissae(S, p), g2 = ag.GrevilleAbscissae(T, q);
+    const auto c1 = ng.GenerateExtraction1D(&b1), c2 = ng.GenerateExtraction1D(&b2);
+    const int m = nex + p, n = ney + q;
+    std::vector<double> CP(2 * m * n);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < m; ++i) {
+            CP[2 * (j * m + i)] = g1[i];
+            CP[2 * (j * m + i) + 1] = g2[j];
+        }
+    const std::string d(dir), bn(base);
+    FileManager fm;
+    fm.WritePreprocessInfo(d + "/info.txt", p, q, Lx, Ly, nex, ney, part_num_1d, 2, bn);
+    Partition part(part_num_1d, part_num_1d, 2, d + "/" + bn);
+    part.GeneratePartition(&b1, &b2, CP, ien, id, c1, c2);
+    return 0;
+}
+
+// y = A_ref x over all parts of a partitioned mesh (x, y in the partition
+// numbering, length nfunc): per part, the MatMulMF element loop on its local
+// form, scattering to the global rows ID >= 0; then every part's Dir rows = 0.
+int ref_apply_partitioned(const char *dir, const char *base, int p, int q, int nparts, const double *x, double *y,
+                          int nfunc)
+{
+    std::fill(y, y + nfunc, 0.0);
+    FileManager fm;
+    const int nloc = (p + 1) * (q + 1), pp = p + 1, qq = q + 1;
+    LocalAssemblyMF la(p, q);
+    ElementMF el(p, q);
+    std::vector<std::vector<int>> dirs;
+    int offset = 0;
+    for (int r = 0; r < nparts; ++r) {
+        int nlf = 0, nlx = 0, nly = 0;
+        std::vector<double> h1, h2, CP, C1, C2;
+        std::vector<int> ID, ghost, Dir, IEN;
+        fm.ReadPartition(fm.GetPartitionFilename(std::string(dir) + "/" + base, r), nlf, nlx, nly, h1, h2, CP, ID,
+                         ghost, Dir, IEN, C1, C2);
+        std::vector<double> xl(nlf + ghost.size());
+        for (int k = 0; k < nlf; ++k) xl[k] = x[offset + k];
+        for (size_t g = 0; g < ghost.size(); ++g) xl[nlf + g] = x[ghost[g]];
+        std::vector<double> eCP(2 * nloc), e1(pp * pp), e2(qq * qq);
+        for (int jj = 0; jj < nly; ++jj)
+            for (int ii = 0; ii < nlx; ++ii) {
+                const int e = jj * nlx + ii;
+                for (int j = 0; j < nloc; ++j) {
+                    const int A = IEN[e * nloc + j];
+                    eCP[2 * j] = CP[2 * A];
+                    eCP[2 * j + 1] = CP[2 * A + 1];
+                    la.Floc_in[j] = xl[A];
+                }
+                std::copy(C1.begin() + ii * pp * pp, C1.begin() + (ii + 1) * pp * pp, e1.begin());
+                std::copy(C2.begin() + jj * qq * qq, C2.begin() + (jj + 1) * qq * qq, e2.begin());
+                el.SetElement(e1, e2, h1[ii], h2[jj]);
+                la.LocalMatMulMF(&el, eCP);
+                for (int j = 0; j < nloc; ++j) {
+                    const int row = ID[IEN[e * nloc + j]];
+                    if (row >= 0) y[row] += la.Floc_out[j];
+                }
+            }
+        dirs.push_back(Dir);
+        offset += nlf;
+    }
+    for (const auto &D : dirs)
+        for (int d : D) y[d] = 0.0;
+    return offset;
 }
 
 }  // extern "C"

@@ -256,7 +256,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
 
     auto store = [&](int R, int C, T v) {
         const size_t i = (size_t)R * g.m + C;
-        const bool bnd = (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
+        const bool bnd = a.bc != 2 && (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
         y[i] = bnd ? (a.bc == 1 ? x[i] : T(0)) : a.sign * v;
     };
     T *frame = a.frame + (size_t)(gx * g.NSY + gy) * g.FS;
@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, 0>(), 1)
 
 // Sums the frames of the strips covering each seam control point, strip
 // (row, then column) in ascending order, and stores sign * sum (boundary
-// rules as in apply_kernel). idx enumerates the seam points of grid g.
+// rules as in apply_kernel: bc 0 zero, 1 identity, 2 none). idx enumerates the seam points of grid g.
 template <int P, typename T>
 __device__ __forceinline__ void seam_point(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
                                            const StripGrid &g, T sign, int bc, long long idx)
@@ -480,7 +480,7 @@ __device__ __forceinline__ void seam_point(const T *__restrict__ frame, const T 
         }
     }
     const size_t i = (size_t)R * g.m + C;
-    const bool bnd = (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
+    const bool bnd = bc != 2 && (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
     y[i] = bnd ? (bc == 1 ? x[i] : T(0)) : sign * v;
 }
 

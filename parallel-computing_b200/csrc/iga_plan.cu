@@ -437,7 +437,7 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     if (opts.precision < IGA_FP64 || opts.precision > IGA_MIXED) return IGA_ERR_ARG;
     if (opts.geometry != IGA_GEOM_PRECOMPUTED && opts.geometry != IGA_GEOM_ON_THE_FLY) return IGA_ERR_ARG;
     if (opts.sign != IGA_SIGN_REFERENCE && opts.sign != IGA_SIGN_SPD) return IGA_ERR_ARG;
-    if (opts.bc != IGA_BC_REFERENCE && opts.bc != IGA_BC_IDENTITY) return IGA_ERR_ARG;
+    if (opts.bc != IGA_BC_REFERENCE && opts.bc != IGA_BC_IDENTITY && opts.bc != IGA_BC_NONE) return IGA_ERR_ARG;
     Patch P;
     MeshDescView v{d->p, d->q, d->nElemX, d->nElemY, d->CP, d->weights, d->C1, d->C2, d->IEN, d->ID, d->Dir,
                    d->nDir, d->kappa};

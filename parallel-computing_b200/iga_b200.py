@@ -1,5 +1,5 @@
-"""Python binding (ctypes) of the C ABI in include/iga_mf.h, include/iga_solve.h
-and include/iga_batch.h.
+"""Python binding (ctypes) of the C ABI in include/iga_mf.h, include/iga_solve.h,
+include/iga_batch.h and include/iga_part.h.
 
 A thin layer for tests, the benchmark and Python users: it loads the in-tree
 libiga_b200.so (built by `make -C parallel-computing_b200`) and fails loudly if
@@ -25,7 +25,7 @@ IGA_OK = 0
 FP64, FP32, MIXED = 0, 1, 2
 GEOM_PRECOMPUTED, GEOM_ON_THE_FLY = 0, 1
 SIGN_REFERENCE, SIGN_SPD = -1, 1
-BC_REFERENCE, BC_IDENTITY = 0, 1
+BC_REFERENCE, BC_IDENTITY, BC_NONE = 0, 1, 2
 F_REFERENCE, F_SINSIN, F_ANNULUS = 0, 1, 2
 
 
@@ -74,6 +74,16 @@ class BatchStats(ctypes.Structure):
                 ("max_relres", ctypes.c_double), ("seconds", ctypes.c_double)]
 
 
+class PartInfo(ctypes.Structure):
+    _fields_ = [("p", ctypes.c_int), ("q", ctypes.c_int), ("nElemX", ctypes.c_int), ("nElemY", ctypes.c_int),
+                ("part_num_1d", ctypes.c_int), ("dim", ctypes.c_int), ("Lx", ctypes.c_double),
+                ("Ly", ctypes.c_double), ("rank", ctypes.c_int), ("part_x", ctypes.c_int), ("part_y", ctypes.c_int),
+                ("nlocalfunc", ctypes.c_int), ("nghost", ctypes.c_int), ("nlocalelemx", ctypes.c_int),
+                ("nlocalelemy", ctypes.c_int), ("elem_x0", ctypes.c_int), ("elem_y0", ctypes.c_int),
+                ("block_m", ctypes.c_int), ("block_n", ctypes.c_int), ("owned_offset", ctypes.c_int64),
+                ("nfunc_global", ctypes.c_int64)]
+
+
 PC_NONE, PC_FEM_CG, PC_FEM_EXACT = 0, 1, 2
 
 _LIB = None
@@ -119,6 +129,15 @@ SIGNATURES = [
     ("iga_batch_autotune", ctypes.c_int, [VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]),
     ("iga_tune_lookup", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    ("iga_part_open", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(VP)]),
+    ("iga_part_close", ctypes.c_int, [VP]),
+    ("iga_part_get_info", ctypes.c_int, [VP, ctypes.POINTER(PartInfo)]),
+    ("iga_part_ghosts", ctypes.c_int, [VP, VP]),
+    ("iga_part_block_map", ctypes.c_int, [VP, VP]),
+    ("iga_part_local_id", ctypes.c_int, [VP, VP]),
+    ("iga_part_mesh", ctypes.c_int, [VP, ctypes.POINTER(MeshDesc)]),
+    ("iga_part_build", ctypes.c_int, [VP, ctypes.POINTER(Opts)]),
+    ("iga_part_apply", ctypes.c_int, [VP, VP, VP, VP]),
 ]
 
 
@@ -358,6 +377,71 @@ class Batch:
         if check:
             _check(status, "iga_batch_solve")
         return st, its, rel
+
+
+def partition_filename(base_name, rank):
+    """<base_name>_<rank>.txt, the reference's partition file name."""
+    return f"{base_name}_{rank}.txt"
+
+
+class Part:
+    """One part of a partitioned mesh read from the reference's files (info.txt
+    and <base_name>_<rank>.txt). Host arrays: ghosts (partition numbering),
+    block_to_local, local_id; mesh() gives the sub-patch. build() creates the
+    device state; apply(x_local, y_local) is the part's ghosted MatMult."""
+
+    def __init__(self, info_file, part_file, rank):
+        h = VP()
+        _check(_lib().iga_part_open(info_file.encode(), part_file.encode(), rank, ctypes.byref(h)), "iga_part_open")
+        self.h = h
+        info = PartInfo()
+        _check(_lib().iga_part_get_info(h, ctypes.byref(info)), "iga_part_get_info")
+        self.info = info
+        self.rank = rank
+        self.nowned, self.nghost = info.nlocalfunc, info.nghost
+        self.owned_offset = int(info.owned_offset)
+        self.ghosts = np.empty(info.nghost, dtype=np.int64)
+        if info.nghost:
+            _check(_lib().iga_part_ghosts(h, _ptr(self.ghosts)), "iga_part_ghosts")
+        nl = info.nlocalfunc + info.nghost
+        self.block_to_local = np.empty(nl, dtype=np.int32)
+        _check(_lib().iga_part_block_map(h, _ptr(self.block_to_local)), "iga_part_block_map")
+        self.local_id = np.empty(nl, dtype=np.int32)
+        _check(_lib().iga_part_local_id(h, _ptr(self.local_id)), "iga_part_local_id")
+
+    def mesh(self):
+        """Sub-patch as a mesh dict (host copies)."""
+        d = MeshDesc()
+        _check(_lib().iga_part_mesh(self.h, ctypes.byref(d)), "iga_part_mesh")
+        i = self.info
+        m, n = i.block_m, i.block_n
+
+        def arr(ptr, k):
+            return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)), shape=(k,)).copy()
+        return dict(p=i.p, q=i.q, nex=i.nlocalelemx, ney=i.nlocalelemy, CP=arr(d.CP, 2 * m * n),
+                    C1=arr(d.C1, i.nlocalelemx * (i.p + 1) ** 2), C2=arr(d.C2, i.nlocalelemy * (i.q + 1) ** 2),
+                    h1=arr(d.h1, i.nlocalelemx), h2=arr(d.h2, i.nlocalelemy), W=None, kappa=None)
+
+    def build(self, sign=SIGN_REFERENCE, bc=BC_REFERENCE, geometry=GEOM_PRECOMPUTED, device=0):
+        o = Opts()
+        _lib().iga_opts_default(ctypes.byref(o))
+        o.precision, o.geometry, o.sign, o.bc, o.device = FP64, geometry, sign, bc, device
+        _check(_lib().iga_part_build(self.h, ctypes.byref(o)), "iga_part_build")
+        return self
+
+    def apply(self, x_local, y_local, stream=None):
+        _check(_lib().iga_part_apply(self.h, _ptr(x_local), _ptr(y_local), _stream(stream)), "iga_part_apply")
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().iga_part_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def batch_autotune(meshes, tune_file, precision=FP64, device=0):

@@ -1,0 +1,139 @@
+"""Multi-rank MatMult over a partitioned mesh: one part per rank (one rank per
+GPU), the ghost traffic of the reference's PETSc ghosted vectors done with
+torch.distributed (NCCL between GPUs, gloo on CPU).
+
+The reference's MatMult (matrix_free/src/GlobalAssemblyMF.cpp:141-210 on the
+vectors of matrix_free/iteration_number_fempc_mf.cpp:62-72) is
+    VecGhostUpdate(x, INSERT, FORWARD)     owners' values into every ghost copy
+    element loop into y's local form       iga_part_apply (include/iga_part.h)
+    VecAssembly(y)                         ghost contributions added to owners
+    y[Dir] = 0                             done by iga_part_apply's local ID rule
+The exchange here does the first and last steps: every rank learns once which
+of its owned entries are ghosts of which peer (from all ranks' ghost lists);
+a forward update sends owned values to the peers that hold them as ghosts, a
+reverse update sends ghost contributions back, and each owner adds them peer
+by peer in ascending rank order (a fixed summation order: bitwise
+reproducible across runs).
+"""
+import numpy as np
+
+
+def build_exchange(offsets, ghost_lists):
+    """Exchange maps of every rank from the owned ranges (offsets[r] ..
+    offsets[r+1]-1 in the partition numbering) and every rank's ghost list.
+    Returns, per rank r, (recv_pos, send_idx): recv_pos[q] = positions in r's
+    ghost list of the ghosts q owns (ascending); send_idx[q] = owned-local
+    indices of r's entries that q holds as ghosts, in q's ghost-list order."""
+    offsets = np.asarray(offsets, dtype=np.int64)
+    world = len(ghost_lists)
+    owners = [np.searchsorted(offsets, np.asarray(g, dtype=np.int64), side="right") - 1 for g in ghost_lists]
+    for r, (g, o) in enumerate(zip(ghost_lists, owners)):
+        if len(g) and (o.min() < 0 or o.max() >= world or np.any(o == r)):
+            raise ValueError(f"rank {r}: ghost outside the other ranks' owned ranges")
+    plans = []
+    for r in range(world):
+        recv_pos, send_idx = {}, {}
+        for q in range(world):
+            if q == r:
+                continue
+            pos = np.nonzero(owners[r] == q)[0]
+            if len(pos):
+                recv_pos[q] = pos
+            mine = np.asarray(ghost_lists[q], dtype=np.int64)[owners[q] == r]
+            if len(mine):
+                send_idx[q] = mine - offsets[r]
+        plans.append((recv_pos, send_idx))
+    return plans
+
+
+class DistPartOperator:
+    """y_owned = A x_owned for this rank's part (torch tensors on `device`).
+
+    part: an iga_b200.Part (built); dist: torch.distributed with an initialised
+    process group, one part per rank (rank r reads <base_name>_<r>.txt).
+    local_apply(x_local, y_local) defaults to part.apply (the GPU kernels)."""
+
+    def __init__(self, part, dist, device, local_apply=None):
+        import torch
+        self.torch, self.dist, self.device = torch, dist, device
+        self.part = part
+        self.local_apply = local_apply or part.apply
+        world, rank = dist.get_world_size(), dist.get_rank()
+        if part.rank != rank:
+            raise ValueError("the part's rank differs from the process rank")
+        mine = (part.owned_offset, part.nowned, part.ghosts.tolist())
+        everyone = [None] * world
+        dist.all_gather_object(everyone, mine)
+        offsets = [e[0] for e in everyone] + [everyone[-1][0] + everyone[-1][1]]
+        for r in range(world - 1):
+            if offsets[r] + everyone[r][1] != offsets[r + 1]:
+                raise ValueError("owned ranges are not contiguous in rank order")
+        recv_pos, send_idx = build_exchange(offsets, [e[2] for e in everyone])[rank]
+        self.recv_pos = {q: torch.as_tensor(v, device=device) for q, v in recv_pos.items()}
+        self.send_idx = {q: torch.as_tensor(v, device=device) for q, v in send_idx.items()}
+        self.nowned = part.nowned
+        self.x_local = torch.zeros(part.nowned + part.nghost, dtype=torch.float64, device=device)
+        self.y_local = torch.empty_like(self.x_local)
+
+    def _exchange(self, sends, recv_sizes):
+        """Point-to-point exchange: sends {peer: tensor}, receives {peer: size}."""
+        torch, dist = self.torch, self.dist
+        recvs = {q: torch.empty(n, dtype=torch.float64, device=self.device) for q, n in recv_sizes.items()}
+        ops = [dist.P2POp(dist.isend, t.contiguous(), q) for q, t in sorted(sends.items())]
+        ops += [dist.P2POp(dist.irecv, t, q) for q, t in sorted(recvs.items())]
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        return recvs
+
+    def forward_update(self, x_owned):
+        """x_local = [x_owned | ghost values from their owners]."""
+        self.x_local[:self.nowned] = x_owned
+        got = self._exchange({q: x_owned[i] for q, i in self.send_idx.items()},
+                             {q: len(p) for q, p in self.recv_pos.items()})
+        for q, buf in got.items():
+            self.x_local[self.nowned + self.recv_pos[q]] = buf
+        return self.x_local
+
+    def reverse_add(self, y_local, y_owned):
+        """y_owned = owned rows of y_local + the peers' ghost contributions (ascending peer order)."""
+        y_owned.copy_(y_local[:self.nowned])
+        got = self._exchange({q: y_local[self.nowned + p] for q, p in self.recv_pos.items()},
+                             {q: len(i) for q, i in self.send_idx.items()})
+        for q in sorted(got):
+            y_owned.index_add_(0, self.send_idx[q], got[q])
+        return y_owned
+
+    def matmult(self, x_owned, y_owned):
+        x_local = self.forward_update(x_owned)
+        self.local_apply(x_local, self.y_local)
+        return self.reverse_add(self.y_local, y_owned)
+
+
+def emulate_partitioned_matmult(parts, x_global, local_apply=None):
+    """All parts of a partitioned mesh in one process (for a single GPU, or on
+    CPU): the same maps and summation order as DistPartOperator, with the
+    transfers done in memory. x_global in the partition numbering (torch
+    tensor); returns y_global."""
+    import torch
+    offsets = [p.owned_offset for p in parts] + [parts[-1].owned_offset + parts[-1].nowned]
+    plans = build_exchange(offsets, [p.ghosts for p in parts])
+    dev = x_global.device
+    y_locals = []
+    for p, (recv_pos, _) in zip(parts, plans):
+        x_local = torch.empty(p.nowned + p.nghost, dtype=torch.float64, device=dev)
+        x_local[:p.nowned] = x_global[p.owned_offset:p.owned_offset + p.nowned]
+        if p.nghost:
+            x_local[p.nowned:] = x_global[torch.as_tensor(p.ghosts, device=dev)]
+        y_local = torch.empty_like(x_local)
+        (local_apply or (lambda part, a, b: part.apply(a, b)))(p, x_local, y_local)
+        y_locals.append(y_local)
+    y_global = torch.empty_like(x_global)
+    for r, (p, (_, send_idx)) in enumerate(zip(parts, plans)):
+        y_owned = y_locals[r][:p.nowned].clone()
+        for q in sorted(send_idx):
+            recv_pos_q = plans[q][0][r]
+            contrib = y_locals[q][parts[q].nowned + torch.as_tensor(recv_pos_q, device=dev)]
+            y_owned.index_add_(0, torch.as_tensor(send_idx[q], device=dev), contrib)
+        y_global[p.owned_offset:p.owned_offset + p.nowned] = y_owned
+    return y_global

@@ -1,4 +1,5 @@
-"""Generate tests/golden/ref_vectors.npz from the REFERENCE's own element code.
+"""Generate tests/golden/ref_vectors.npz and tests/golden/partitions/ from the
+REFERENCE's own code.
 
 Runs only where the reference tree is available: it builds oracle/_ref/libigaref.so
 (oracle/Makefile target "ref": the reference's PETSc-free sources compiled in
@@ -7,7 +8,13 @@ The reference ships no golden vectors, so these recorded outputs are the pins fo
 the oracle restatement (tests/test_oracle_pin.py) and, through it, for the CUDA
 kernels.
 
-    python tests/golden/make_golden.py
+The partition fixtures are the reference preprocessor's files (info.txt and
+<base>_<rank>.txt written by its Partition + FileManager) for small meshes,
+with a seeded x in the partition numbering and y = the reference's partitioned
+MatMulMF (every part's element loop on its ghosted local form).
+
+    python tests/golden/make_golden.py                   # everything
+    python tests/golden/make_golden.py --partitions-only
 """
 import ctypes
 import os
@@ -144,5 +151,29 @@ def main():
     print(f"wrote {path}: {len(out)} arrays, {os.path.getsize(path)} bytes")
 
 
+# (name, p, nElemX, nElemY, part_num_1d)
+PARTITION_CASES = [("p3_9x7_2", 3, 9, 7, 2), ("p2_10x12_3", 2, 10, 12, 3), ("p4_8x11_2", 4, 8, 11, 2)]
+
+
+def write_partitions(L):
+    L.ref_write_partition.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 2 + [ctypes.c_int, ctypes.c_char_p,
+                                                                                    ctypes.c_char_p]
+    L.ref_apply_partitioned.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        VP, VP, ctypes.c_int]
+    for k, (name, p, nex, ney, P) in enumerate(PARTITION_CASES):
+        d = os.path.join(HERE, "partitions", name)
+        os.makedirs(d, exist_ok=True)
+        L.ref_write_partition(p, p, nex, ney, 1.0, 1.0, P, d.encode(), b"part")
+        nf = (nex + p) * (ney + p)
+        x = splitmix_uniform(40 + k, -1.0, 1.0, nf)
+        y = np.zeros(nf)
+        got = L.ref_apply_partitioned(d.encode(), b"part", p, p, P * P, _p(x), _p(y), nf)
+        assert got == nf, (got, nf)
+        np.savez_compressed(os.path.join(d, "vectors.npz"), x=x, y=y)
+        print(f"wrote {d}: {P * P} parts")
+
+
 if __name__ == "__main__":
-    main()
+    if "--partitions-only" not in sys.argv:
+        main()
+    write_partitions(load_ref())

@@ -269,3 +269,103 @@ def window_rows(mesh, ex_a, ex_b, ey_a, ey_b):
     r0 = 0 if ey_a == 0 else ey_a + q
     r1 = n if ey_b == mesh["ney"] else ey_b
     return (r0, r1, c0, c1)
+
+
+PARTITIONS = os.path.join(os.path.dirname(GOLDEN), "partitions")
+
+
+def read_info(path):
+    """info.txt of the reference preprocessor as a dict."""
+    out = {}
+    for line in open(path):
+        if ": " in line:
+            k, v = line.rstrip("\n").split(": ", 1)
+            out[k] = v
+    return out
+
+
+def partition_numbering(p, q, nex, ney, P):
+    """new[natural index j*m + i] = the partition numbering of
+    matrix_free/src/Partition.cpp:23-92 (parts y outer, x inner; each part's
+    functions x fastest; runs of ceil(m / P) functions, the last shorter)."""
+    m, n = nex + p, ney + q
+    sx, sy = -(-m // P), -(-n // P)
+    cx = [sx] * (P - 1) + [m - (P - 1) * sx]
+    cy = [sy] * (P - 1) + [n - (P - 1) * sy]
+    new = np.empty(m * n, dtype=np.int64)
+    k = 0
+    for jj in range(P):
+        for ii in range(P):
+            for lj in range(cy[jj]):
+                for li in range(cx[ii]):
+                    new[(jj * sy + lj) * m + ii * sx + li] = k
+                    k += 1
+    return new
+
+
+def write_partition_files(mesh, P, out_dir, base="part"):
+    """Test-only restatement of the reference preprocessor's partition output
+    (matrix_free/src/Partition.cpp:3-235 with FileManager::WritePartition /
+    WritePreprocessInfo, matrix_free/src/FileManager.cpp:3-69,375-396) for a
+    unit-square mesh dict, so GPU tests can use meshes larger than the
+    committed fixtures. test_partition_host.py checks that it reproduces the
+    reference-written fixtures byte for byte."""
+    p, q, nex, ney = mesh["p"], mesh.get("q", mesh["p"]), mesh["nex"], mesh["ney"]
+    m, n = nex + p, ney + q
+    nloc = (p + 1) * (q + 1)
+    new = partition_numbering(p, q, nex, ney, P)
+    sx, sy = -(-m // P), -(-n // P)
+    cx = [sx] * (P - 1) + [m - (P - 1) * sx]
+    cy = [sy] * (P - 1) + [n - (P - 1) * sy]
+    fx = [i * sx for i in range(P)]
+    fy = [j * sy for j in range(P)]
+    ex0 = [0] + [fx[i] - p // 2 for i in range(1, P)]
+    ey0 = [0] + [fy[j] - q // 2 for j in range(1, P)]
+    ex1 = [ex0[i + 1] - 1 for i in range(P - 1)] + [nex - 1]
+    ey1 = [ey0[j + 1] - 1 for j in range(P - 1)] + [ney - 1]
+    on_bnd = np.zeros((n, m), bool)
+    on_bnd[0, :] = on_bnd[-1, :] = on_bnd[:, 0] = on_bnd[:, -1] = True
+    new_id = np.where(on_bnd.ravel(), -1, new)          # ID by natural index
+    cp = np.asarray(mesh["CP"]).reshape(n, m, 2)
+    C1 = np.asarray(mesh["C1"])
+    C2 = np.asarray(mesh["C2"])
+
+    def ints(v):
+        return "".join(f"{int(t)} " for t in v)
+
+    def dbls(v):
+        return "".join(f"{float(t):.16g} " for t in v)
+    os.makedirs(out_dir, exist_ok=True)
+    with open(os.path.join(out_dir, "info.txt"), "w") as f:
+        f.write(f"p: {p}\nq: {q}\nLx: {1:g}\nLy: {1:g}\nnElemX: {nex}\nnElemY: {ney}\n"
+                f"part_num_1d: {P}\ndim: 2\nbase_name: {base}\n")
+    for j in range(P):
+        for i in range(P):
+            elems = [(ey, ex) for ey in range(ey0[j], ey1[j] + 1) for ex in range(ex0[i], ex1[i] + 1)]
+            owned_nat = [(fy[j] + lj) * m + fx[i] + li for lj in range(cy[j]) for li in range(cx[i])]
+            owned_new = [int(new[a]) for a in owned_nat]
+            touched = sorted({int(new[(ey + jl) * m + ex + il]) for ey, ex in elems
+                              for jl in range(q + 1) for il in range(p + 1)})
+            ownset = set(owned_new)
+            ghosts = [g for g in touched if g not in ownset]
+            local_new = owned_new + ghosts
+            pos = {g: k for k, g in enumerate(local_new)}
+            nat_of_new = np.empty(m * n, dtype=np.int64)
+            nat_of_new[new] = np.arange(m * n)
+            loc_nat = nat_of_new[np.asarray(local_new)]
+            ien = [pos[int(new[(ey + jl) * m + ex + il])] for ey, ex in elems
+                   for jl in range(q + 1) for il in range(p + 1)]
+            lid = new_id[loc_nat]
+            ldir = [g for g, t in zip(owned_new, lid[:len(owned_new)]) if t == -1]
+            lcp = np.stack([cp.reshape(-1, 2)[a] for a in loc_nat]).ravel()
+            e1, e2 = (p + 1) ** 2, (q + 1) ** 2
+            with open(os.path.join(out_dir, f"{base}_{j * P + i}.txt"), "w") as f:
+                f.write(f"nlocalfunc: {len(owned_new)}\nnlocalelemx: {ex1[i] - ex0[i] + 1}\n"
+                        f"nlocalelemy: {ey1[j] - ey0[j] + 1}\n")
+                f.write("ID\n" + ints(lid) + "\nghostID\n" + ints(ghosts) + "\nDir\n" + ints(ldir) + "\n")
+                f.write("IEN\n" + ints(ien) + "\n")
+                f.write("ElemSize1\n" + dbls([1.0 / nex] * (ex1[i] - ex0[i] + 1)) + "\n")
+                f.write("ElemSize2\n" + dbls([1.0 / ney] * (ey1[j] - ey0[j] + 1)) + "\n")
+                f.write("CP\n" + dbls(lcp) + "\n")
+                f.write("NURBSExtraction1\n" + dbls(C1[ex0[i] * e1:(ex1[i] + 1) * e1]) + "\n")
+                f.write("NURBSExtraction2\n" + dbls(C2[ey0[j] * e2:(ey1[j] + 1) * e2]) + "\n")

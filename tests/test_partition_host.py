@@ -1,0 +1,202 @@
+"""Partitioned meshes on the host (no GPU): the reader of the reference's
+partition files (include/iga_part.h) against files written by the
+reference's own Partition + FileManager (tests/golden/partitions/), and the
+multi-rank ghost exchange (parallel-computing_b200/iga_dist.py) over gloo
+with one process per part, the local element loop done by the CPU oracle.
+"""
+import os
+import shutil
+import socket
+
+import numpy as np
+import pytest
+
+from iga_testlib import PARTITIONS, load_binding, partition_numbering, read_info, splitmix_uniform, unit_square_mesh
+
+CASES = ["p3_9x7_2", "p2_10x12_3", "p4_8x11_2"]
+
+
+@pytest.fixture(scope="module")
+def ib():
+    return load_binding()
+
+
+def case_info(name):
+    d = os.path.join(PARTITIONS, name)
+    info = read_info(os.path.join(d, "info.txt"))
+    p, q, nex, ney, P = (int(info[k]) for k in ("p", "q", "nElemX", "nElemY", "part_num_1d"))
+    return d, p, q, nex, ney, P
+
+
+def open_parts(ib, name):
+    d, p, q, nex, ney, P = case_info(name)
+    return [ib.Part(os.path.join(d, "info.txt"), ib.partition_filename(os.path.join(d, "part"), r), r)
+            for r in range(P * P)]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_reader_accepts_reference_partitions(ib, name):
+    d, p, q, nex, ney, P = case_info(name)
+    parts = open_parts(ib, name)
+    off = 0
+    for r, pt in enumerate(parts):
+        i = pt.info
+        assert (i.p, i.q, i.nElemX, i.nElemY, i.part_num_1d, i.rank) == (p, q, nex, ney, P, r)
+        assert pt.owned_offset == off
+        off += pt.nowned
+        assert np.all(np.diff(pt.ghosts) > 0)                       # the reference sorts them
+        assert sorted(pt.block_to_local.tolist()) == list(range(pt.nowned + pt.nghost))
+        assert i.block_m * i.block_n == pt.nowned + pt.nghost
+    assert off == (nex + p) * (ney + q)
+    # every element belongs to exactly one part
+    assert sum(pt.info.nlocalelemx * pt.info.nlocalelemy for pt in parts) == nex * ney
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_reference_partitioned_matmult_equals_serial(orc, name):
+    """Pins the fixtures: the reference's partitioned element loop (recorded
+    y) equals the serial oracle MatMult in the partition numbering."""
+    d, p, q, nex, ney, P = case_info(name)
+    v = np.load(os.path.join(d, "vectors.npz"))
+    new = partition_numbering(p, q, nex, ney, P)
+    mesh = unit_square_mesh(orc, p, q, nex, ney)
+    y_nat = orc.apply_mf(mesh, v["x"][new], sign=-1.0, bc=0)
+    y = np.empty_like(y_nat)
+    y[new] = y_nat
+    assert np.abs(y - v["y"]).max() <= 1e-12 * np.abs(v["y"]).max()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_sub_patch_is_the_global_block(ib, orc, name):
+    d, p, q, nex, ney, P = case_info(name)
+    g = unit_square_mesh(orc, p, q, nex, ney)
+    m = nex + p
+    cp = g["CP"].reshape(ney + q, m, 2)
+    for pt in open_parts(ib, name):
+        i = pt.info
+        sm = pt.mesh()
+        blk = cp[i.elem_y0:i.elem_y0 + i.block_n, i.elem_x0:i.elem_x0 + i.block_m]
+        # the files hold 16 significant digits (std::setprecision(16))
+        assert np.abs(sm["CP"].reshape(i.block_n, i.block_m, 2) - blk).max() < 1e-15
+        e1 = (p + 1) ** 2
+        assert np.abs(sm["C1"] - g["C1"][i.elem_x0 * e1:(i.elem_x0 + i.nlocalelemx) * e1]).max() < 1e-15
+
+
+def local_oracle(orc, part, sub, x_local, sign=-1.0):
+    """The part's element loop on the CPU (checker): block gather, oracle
+    sub-patch MatMult with no boundary rule, scatter, rows ID < 0 zero."""
+    xb = x_local[part.block_to_local]
+    yb = orc.apply_mf(sub, xb, sign=sign, bc=2)
+    y = np.empty_like(x_local)
+    y[part.block_to_local] = yb
+    y[part.local_id < 0] = 0.0
+    return y
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_emulated_exchange_matches_reference(ib, orc, name):
+    import torch
+    from iga_dist import emulate_partitioned_matmult
+    d, p, q, nex, ney, P = case_info(name)
+    v = np.load(os.path.join(d, "vectors.npz"))
+    parts = open_parts(ib, name)
+    subs = [pt.mesh() for pt in parts]
+
+    def apply(part, xl, yl):
+        yl.copy_(torch.from_numpy(local_oracle(orc, part, subs[part.rank], xl.numpy())))
+    y = emulate_partitioned_matmult(parts, torch.from_numpy(v["x"]), local_apply=apply).numpy()
+    assert np.abs(y - v["y"]).max() <= 1e-12 * np.abs(v["y"]).max()
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _gloo_rank(rank, world, port, name, out_dir):
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from iga_testlib import Oracle
+        import iga_b200 as ib
+        from iga_dist import DistPartOperator
+        orc = Oracle()
+        d = os.path.join(PARTITIONS, name)
+        part = ib.Part(os.path.join(d, "info.txt"), ib.partition_filename(os.path.join(d, "part"), rank), rank)
+        sub = part.mesh()
+
+        def apply(xl, yl):
+            yl.copy_(torch.from_numpy(local_oracle(orc, part, sub, xl.numpy())))
+        op = DistPartOperator(part, dist, "cpu", local_apply=apply)
+        v = np.load(os.path.join(d, "vectors.npz"))
+        x_owned = torch.from_numpy(v["x"][part.owned_offset:part.owned_offset + part.nowned].copy())
+        y_owned = torch.empty_like(x_owned)
+        op.matmult(x_owned, y_owned)
+        np.save(os.path.join(out_dir, f"y{rank}.npy"), y_owned.numpy())
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("name", ["p3_9x7_2", "p2_10x12_3"])
+def test_gloo_ranks_match_reference(name, tmp_path):
+    """One process per part over gloo: forward ghost update, local element
+    loop, reverse add; the assembled owned rows equal the reference's
+    partitioned MatMult."""
+    import torch.multiprocessing as mp
+    d, p, q, nex, ney, P = case_info(name)
+    world = P * P
+    mp.start_processes(_gloo_rank, args=(world, _free_port(), name, str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    v = np.load(os.path.join(d, "vectors.npz"))
+    y = np.concatenate([np.load(os.path.join(tmp_path, f"y{r}.npy")) for r in range(world)])
+    assert np.abs(y - v["y"]).max() <= 1e-12 * np.abs(v["y"]).max()
+
+
+def test_reader_rejects_bad_files(ib, tmp_path):
+    src = os.path.join(PARTITIONS, "p3_9x7_2")
+    info = os.path.join(src, "info.txt")
+    good = os.path.join(src, "part_1.txt")
+    with pytest.raises(ib.IgaError):
+        ib.Part(info, good, 2)                     # wrong rank for this file
+    with pytest.raises(ib.IgaError):
+        ib.Part(info, good, 7)                     # rank outside the partition
+    lines = open(good).read().split("\n")
+
+    def variant(fn):
+        path = str(tmp_path / "bad.txt")
+        out = fn(list(lines))
+        open(path, "w").write("\n".join(out))
+        return path
+    bad_count = variant(lambda L: ["nlocalfunc: 31"] + L[1:])
+    gi = lines.index("ghostID") + 1
+    swapped = lines[gi].split()
+    swapped[0], swapped[1] = swapped[1], swapped[0]
+    bad_ghost = variant(lambda L: L[:gi] + [" ".join(swapped)] + L[gi + 1:])
+    ii = lines.index("IEN") + 1
+    short_ien = variant(lambda L: L[:ii] + [" ".join(L[ii].split()[:-1])] + L[ii + 1:])
+    no_cp = variant(lambda L: [x for k, x in enumerate(L) if k not in (lines.index("CP"), lines.index("CP") + 1)])
+    for path in (bad_count, bad_ghost, short_ien, no_cp):
+        with pytest.raises(ib.IgaError):
+            ib.Part(info, path, 1)
+    with pytest.raises(ib.IgaError):
+        ib.Part(str(tmp_path / "missing_info.txt"), good, 1)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_test_writer_reproduces_reference_files(orc, name, tmp_path):
+    """The test-only writer used for large GPU cases writes exactly the
+    reference preprocessor's files."""
+    import filecmp
+    from iga_testlib import write_partition_files
+    d, p, q, nex, ney, P = case_info(name)
+    write_partition_files(unit_square_mesh(orc, p, q, nex, ney), P, str(tmp_path))
+    for f in sorted(os.listdir(d)):
+        if f.endswith(".txt"):
+            assert filecmp.cmp(os.path.join(d, f), os.path.join(tmp_path, f), shallow=False), f
