@@ -213,13 +213,15 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
     both with the FEM preconditioner inverted exactly; plus the reference's
     preconditioner (inner Jacobi-CG to 1e-10) on the p=2 64x64 configuration."""
     out = {"problem": f"p=3 {ne}x{ne}, f=2pi^2 sin(pi x) sin(pi y), K u = F, rtol 1e-10 (true residual)",
-           "pc": "bilinear-FEM matrix, exact inverse (tensor-product fast diagonalisation; FP64 DGEMM / FP32 TF32)"}
+           "pc": "bilinear-FEM matrix, exact inverse (x eigenvectors by GEMM, y tridiagonal solves; FP64 DGEMM / FP32 TF32)"}
     plan = ib.Plan(mesh, precision=ib.MIXED)
     b = torch.empty(plan.nfunc, dtype=torch.float64, device="cuda")
     plan.rhs(b, ib.F_SINSIN)
     stream = torch.cuda.current_stream()
+    # FP32 sweeps to 1e-3 (the library default): shallow sweeps restart the
+    # Krylov space before FP32 rounding slows it down
     for name, kw in (("fp64", dict(pc=ib.PC_FEM_EXACT)),
-                     ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED))):
+                     ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED, sweep_rtol=1e-3))):
         x = torch.zeros_like(b)
         plan.solve(b, x, **kw)   # warm-up: eigen-decomposition, cuBLAS, allocations
         times, st = [], None
@@ -233,7 +235,7 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
             barrier()
             times.append(max_over_ranks(e0.elapsed_time(e1) / 1e3))
         out[name] = {"seconds": statistics.median(times), "iterations": st.iterations, "sweeps": st.sweeps,
-                     "relres": st.relres}
+                     "relres": st.relres, **({"sweep_rtol": kw["sweep_rtol"]} if "sweep_rtol" in kw else {})}
     out["speedup_fp32_refine_vs_fp64"] = out["fp64"]["seconds"] / out["fp32_refine"]["seconds"]
     plan.close()
     # mixed-precision configuration: NURBS quarter annulus, p=4, 1024x1024,
@@ -244,10 +246,9 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
     pa.rhs(ba, ib.F_ANNULUS)
     xs = {}
     ann = {"problem": "quarter annulus r in [1,2] (NURBS, p=4), 1024x1024, u = sin(pi r) sin(2 theta), rtol 1e-10"}
-    # FP32 sweeps to 1e-4: the p=4 FP32 operator's rounding makes a tighter
-    # sweep tolerance cost iterations without saving a sweep
+    # FP32 sweeps to 1e-2 (measured fastest here: five shallow sweeps)
     for name, kw in (("fp64", dict(pc=ib.PC_FEM_EXACT)),
-                     ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED, sweep_rtol=1e-4))):
+                     ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED, sweep_rtol=1e-2))):
         x = torch.zeros_like(ba)
         pa.solve(ba, x, **kw)
         times = []

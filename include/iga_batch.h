@@ -54,8 +54,9 @@ typedef struct {
 void iga_batch_opts_default(iga_batch_opts *opts);
 
 /* Builds the plans of every problem (meshes as for iga_plan_create; kappa must
- * be NULL), the work lists, and the preconditioner's 1-D eigenpairs (shared by
- * problems with equal 1-D FEM grids). */
+ * be NULL; at most 272 free control points in y, i.e. nElemY + q <= 274), the
+ * work lists, and the preconditioner's 1-D eigenpairs (shared by problems with
+ * equal 1-D FEM grids). */
 int iga_batch_create(const iga_mesh_desc *meshes, int count, const iga_batch_opts *opts, iga_batch **out);
 int iga_batch_destroy(iga_batch *batch);
 /* count+1 entries: start of every problem's vector, then the total length. */

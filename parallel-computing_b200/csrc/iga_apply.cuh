@@ -97,12 +97,15 @@ template <>
 __device__ __forceinline__ float recip<float>(float v) { return __frcp_rn(v); }
 
 // Threads per CTA the register budget allows (one CTA per SM): the kernel's
-// per-thread state grows with p and doubles in FP64.
+// per-thread state grows with p and doubles in FP64. FP64 precomputed p >= 4
+// runs 8 warps without register spills (at 10 warps it spilled and ran 1.8x
+// slower at p = 4); the FP64 on-the-fly kernels at p >= 4 need more than the
+// 255 registers a thread can have and spill at any bound.
 template <int P, typename T, int GEOM>
 __host__ __device__ constexpr int apply_max_threads()
 {
     return sizeof(T) == 4 ? (P <= 3 ? 512 : (GEOM ? 384 : 512))
-                          : (P <= 2 ? (GEOM ? 384 : 512) : P == 3 ? (GEOM ? 320 : 384) : (GEOM ? 256 : 320));
+                          : (P <= 2 ? (GEOM ? 384 : 512) : P == 3 ? (GEOM ? 320 : 384) : 256);
 }
 
 // One CTA: column strip gx, strips gyb*W .. gyb*W+W-1 of that column (one per warp).

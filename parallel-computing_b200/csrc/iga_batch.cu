@@ -360,19 +360,111 @@ __global__ void __launch_bounds__(kBT) bk_cond(const int *__restrict__ act, int 
 }
 
 // ------------------------------------------------------------ exact FEM inverse, batched
-// z = Vx [(Vx^T R Vy) ./ (lx_a + ly_b)] Vy^T on the free nodes of every
-// problem, R the interior block of r (column-major nx x ny, rows = x), and
-// z = r on the boundary ring. Four GEMM stages, each one launch over the
-// 64 x 64 output tiles of all active problems:
-//   1: W1 = Vx^T R          2: W2 = (W1 Vy) ./ (lx + ly)
-//   3: W1 = Vx W2           4: Z  = W1 Vy^T  (scattered into z)
+// z = K_fem^-1 r on the free nodes of every problem (R, Z the interior blocks
+// of r, z: column-major nx x ny, rows = x), z = r on the boundary ring. With
+// Kx Vx = Mx Vx diag(lx), K_fem = Kx (x) My + Mx (x) Ky becomes the tridiagonal
+// y system lx[a] My + Ky for every x mode a:
+//   stage 1: W1 = Vx^T R                     (GEMM tiles of all active problems)
+//   rows:    row a of W1 solved along y      (one thread per (problem, a))
+//   stage 3: Z = Vx W1, scattered into z     (GEMM tiles)
 template <typename T>
 struct FdProb {
-    const T *Vx, *Vy, *lx, *ly;   // eigenvectors (column-major, ld nx / ny) and eigenvalues
-    T *W1, *W2;                    // nx * ny work matrices
-    long long off;                 // vector offset of the problem
+    const T *Vx, *lx;      // x eigenvectors (column-major, ld nx) and eigenvalues
+    const T *Dv, *Cf;      // LDL^T factors of the y systems: 1 / pivot, upper off-diagonal; [b][a], ld nx
+    const double *yc;      // free y nodes' pencil Kd | Ko | Md | Mo (ny each)
+    T *W1;                 // nx * ny work matrix
+    long long off;         // vector offset of the problem
     int m, n, nx, ny;
 };
+
+// Row solves of the y systems: forward y_b = Dv_b w_b + beta_b y_{b-1},
+// beta_b = -e_{b-1} Dv_b, backward x_b = y_b - C_b x_{b+1}, e_b = lx[a] Mo_b +
+// Ko_b. A block takes 32 consecutive x modes (threadIdx.x, coalesced rows) and
+// cuts y into kRowSeg segments (threadIdx.y): each thread solves its segment
+// in registers with a zero carry-in, the segments' affine carry maps
+// (c -> end + prod c) are composed through shared memory, and each thread
+// adds its carry times the running coefficient product. One read of W, Dv, C
+// and one write of W. rows = (problem, first x mode) per block.
+constexpr int kRowSeg = 16;                // segments per row
+constexpr int kRowLen = 17;                // rows per segment: ny <= kRowSeg * kRowLen (patches up to 272 free nodes)
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kRowSeg, sizeof(T) == 4 ? 2 : 1) fd_rows_kernel(const FdProb<T> *__restrict__ fps,
+                                                              const int2 *__restrict__ rows,
+                                                              const int *__restrict__ act)
+{
+    using R = T;   // segment arithmetic in the preconditioner's precision (registers: 2 blocks per SM in FP32)
+    __shared__ R mE[kRowSeg][32], mP[kRowSeg][32];
+    const int2 rw = rows[blockIdx.x];
+    if (!act[rw.x]) return;
+    const FdProb<T> &f = fps[rw.x];
+    const int nx = f.nx, ny = f.ny;
+    const int a = rw.y + threadIdx.x, sg = threadIdx.y;
+    const int seglen = (ny + kRowSeg - 1) / kRowSeg;   // <= kRowLen
+    const int b0 = sg * seglen, len = max(0, min(seglen, ny - b0));
+    const bool live = a < nx;
+    const R lam = live ? f.lx[a] : R(0);
+    const double *yc = f.yc;
+    T *W = f.W1;
+    R w[kRowLen], c[kRowLen];
+#pragma unroll
+    for (int k = 0; k < kRowLen; ++k) {
+        const bool in = live && k < len;
+        w[k] = in ? W[a + (size_t)(b0 + k) * nx] : R(0);
+        c[k] = in ? f.Dv[a + (size_t)(b0 + k) * nx] : R(0);   // Dv now, C later
+    }
+    // forward, zero carry-in; c[k] becomes beta_k
+    R y = 0, pr = 1;
+#pragma unroll
+    for (int k = 0; k < kRowLen; ++k) {
+        if (k < len) {
+            const int b = b0 + k;
+            const R beta = b == 0 ? R(0) : -(lam * (R)yc[3 * ny + b - 1] + (R)yc[ny + b - 1]) * c[k];
+            y = c[k] * w[k] + beta * y;
+            pr *= beta;
+            w[k] = y;
+            c[k] = beta;
+        }
+    }
+    mE[sg][threadIdx.x] = y;
+    mP[sg][threadIdx.x] = pr;
+    __syncthreads();
+    R cin = 0;
+    for (int s2 = 0; s2 < sg; ++s2) cin = mE[s2][threadIdx.x] + mP[s2][threadIdx.x] * cin;
+    R r = 1;
+#pragma unroll
+    for (int k = 0; k < kRowLen; ++k) {
+        if (k < len) {
+            r *= c[k];
+            w[k] += r * cin;
+        }
+    }
+    __syncthreads();   // carry maps read; the backward pass reuses them
+#pragma unroll
+    for (int k = 0; k < kRowLen; ++k) c[k] = (live && k < len) ? f.Cf[a + (size_t)(b0 + k) * nx] : R(0);
+    R x = 0, q = 1;
+#pragma unroll
+    for (int k = kRowLen - 1; k >= 0; --k) {
+        if (k < len) {
+            x = w[k] - c[k] * x;
+            q *= -c[k];
+            w[k] = x;
+        }
+    }
+    mE[sg][threadIdx.x] = x;
+    mP[sg][threadIdx.x] = q;
+    __syncthreads();
+    cin = 0;
+    for (int s2 = kRowSeg - 1; s2 > sg; --s2) cin = mE[s2][threadIdx.x] + mP[s2][threadIdx.x] * cin;
+    r = 1;
+#pragma unroll
+    for (int k = kRowLen - 1; k >= 0; --k) {
+        if (k < len) {
+            r *= -c[k];
+            if (live) W[a + (size_t)(b0 + k) * nx] = (T)(w[k] + r * cin);
+        }
+    }
+}
 
 // Tensor-core tiles: FP64 through DMMA (mma.sync m8n8k4, FP64 accumulate),
 // FP32 through TF32 MMA (mma.sync m16n8k8, operands rounded to TF32 once when
@@ -414,8 +506,9 @@ __global__ void __launch_bounds__(128) fd_gemm_kernel(const FdProb<T> *__restric
                                                       const int *__restrict__ act, const T *__restrict__ rb,
                                                       T *__restrict__ zb)
 {
+    static_assert(STAGE == 1 || STAGE == 3, "stages 1 (W1 = Vx^T R) and 3 (Z = Vx W1)");
     constexpr bool A_KF = STAGE == 1;   // A contiguous along k: staged [a][k]
-    constexpr bool B_KF = STAGE != 4;   // B contiguous along k: staged [b][k]
+    constexpr bool B_KF = true;         // B contiguous along k: staged [b][k]
     constexpr int LKF = 20, LRF = 72;
     constexpr int SA = A_KF ? kTile * LKF : kTK * LRF;
     constexpr int SB = B_KF ? kTile * LKF : kTK * LRF;
@@ -425,7 +518,7 @@ __global__ void __launch_bounds__(128) fd_gemm_kernel(const FdProb<T> *__restric
     if (!act[tl.x]) return;
     const FdProb<T> &f = fps[tl.x];
     const int nx = f.nx, ny = f.ny, m = f.m;
-    const int K = (STAGE == 1 || STAGE == 3) ? nx : ny;
+    const int K = nx;
     const int a0 = tl.y * kTile, b0 = tl.z * kTile;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int g = lane >> 2, t4 = lane & 3;
@@ -451,15 +544,12 @@ __global__ void __launch_bounds__(128) fd_gemm_kernel(const FdProb<T> *__restric
     auto ldA = [&](int a, int k) -> T {
         if (a >= nx || k >= K) return T(0);
         if (STAGE == 1) return f.Vx[(size_t)a * nx + k];          // Vx^T
-        if (STAGE == 3) return f.Vx[(size_t)k * nx + a];          // Vx
-        return f.W1[(size_t)k * nx + a];                          // W1 (stages 2, 4)
+        return f.Vx[(size_t)k * nx + a];                          // Vx (stage 3)
     };
     auto ldB = [&](int k, int b) -> T {
         if (k >= K || b >= ny) return T(0);
         if (STAGE == 1) return r[(size_t)(b + 1) * m + (k + 1)];   // R
-        if (STAGE == 2) return f.Vy[(size_t)b * ny + k];          // Vy
-        if (STAGE == 3) return f.W2[(size_t)b * nx + k];          // W2
-        return f.Vy[(size_t)k * ny + b];                          // Vy^T
+        return f.W1[(size_t)b * nx + k];                          // W1 after the row solves (stage 3)
     };
     // element (row, k) of this thread's i-th fetch, coalesced along the contiguous index
     auto coord = [&](bool kf, int i, int &row, int &k) {
@@ -572,8 +662,7 @@ __global__ void __launch_bounds__(128) fd_gemm_kernel(const FdProb<T> *__restric
                 const int b = b0 + wn + j * 8 + 2 * t4 + (c & 1);
                 if (a >= nx || b >= ny) continue;
                 const T v = acc[i][j][c];
-                if (STAGE == 1 || STAGE == 3) f.W1[(size_t)b * nx + a] = v;
-                else if (STAGE == 2) f.W2[(size_t)b * nx + a] = v / (f.lx[a] + f.ly[b]);
+                if (STAGE == 1) f.W1[(size_t)b * nx + a] = v;
                 else z[(size_t)(b + 1) * m + (a + 1)] = v;
             }
 }
@@ -584,7 +673,7 @@ struct BVec {
     T *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *b = nullptr;
     ApplyParams<T> *prm = nullptr;   // per problem (x, y passed separately)
     FdProb<T> *fd = nullptr;
-    T *W1 = nullptr, *W2 = nullptr;
+    T *W1 = nullptr, *Dv = nullptr, *Cf = nullptr;
     std::vector<T *> basis;          // eigenvectors / eigenvalues per distinct 1-D grid
 };
 
@@ -605,8 +694,10 @@ struct iga_batch {
     std::vector<long long> off;   // count + 1
     long long ntot = 0;
     std::vector<BGroup> groups;
-    int nchunks = 0, ntiles = 0;
+    int nchunks = 0, ntiles = 0, nrows = 0;
     int4 *chunks = nullptr, *tiles = nullptr;
+    int2 *rows = nullptr;
+    std::vector<double *> ycoef;     // y pencils of the distinct 1-D grids
     int *c0 = nullptr, *nc = nullptr;
     long long *d_off = nullptr;
     double *partials = nullptr;
@@ -747,7 +838,7 @@ int batch_apply(iga_batch *B, const T *x, T *y, const int *act, cudaStream_t s, 
         BT_TRY(cudaEventRecord(B->join, aux));
         BT_TRY(cudaStreamWaitEvent(s, B->join, 0));
     }
-    seam_fixup_batch_kernel<T><<<dim3(4, B->count), 256, 0, s>>>(prm, act, B->d_off, x, y);
+    seam_fixup_batch_kernel<T><<<dim3(16, B->count), 256, 0, s>>>(prm, act, B->d_off, x, y);
     BT_TRY(cudaGetLastError());
     return IGA_OK;
 }
@@ -761,9 +852,8 @@ int batch_pc(iga_batch *B, int pc, const T *r, T *z, const int *act, cudaStream_
     } else {
         const FdProb<T> *fd = vecs<T>(B).fd;
         fd_gemm_kernel<T, 1><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
-        fd_gemm_kernel<T, 2><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
+        fd_rows_kernel<T><<<B->nrows, dim3(32, kRowSeg), 0, s>>>(fd, B->rows, act);
         fd_gemm_kernel<T, 3><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
-        fd_gemm_kernel<T, 4><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
     }
     BT_TRY(cudaGetLastError());
     return IGA_OK;
@@ -980,6 +1070,47 @@ int setup_fd(iga_batch *B)
             });
         for (auto &t : th) t.join();
     }
+    // y pencils of the grids (double, shared by both precisions) and, per
+    // problem, the LDL^T factors of lx[a] My + Ky for every x mode a
+    std::vector<std::vector<double>> pencils(grids.size());
+    for (size_t k = 0; k < grids.size(); ++k) {
+        std::vector<double> Kd, Ko, Md, Mo;
+        interior_pencil(grids[k], Kd, Ko, Md, Mo);
+        for (const std::vector<double> *v : {&Kd, &Ko, &Md, &Mo}) pencils[k].insert(pencils[k].end(), v->begin(), v->end());
+        double *d = nullptr;
+        int st;
+        if ((st = bupload(&d, pencils[k]))) return st;
+        B->ycoef.push_back(d);
+    }
+    std::vector<std::vector<double>> hDv(B->count), hCf(B->count);
+    {
+        std::vector<std::thread> th;
+        const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 16u));
+        for (unsigned w = 0; w < nt; ++w)
+            th.emplace_back([&, w]() {
+                for (int i = (int)w; i < B->count; i += (int)nt) {
+                    const Basis &bx_ = bases[bx[i]];
+                    const std::vector<double> &yp = pencils[by[i]];
+                    const int nx = bx_.n, ny = (int)yp.size() / 4;
+                    const double *Kd = yp.data(), *Ko = Kd + ny, *Md = Kd + 2 * ny, *Mo = Kd + 3 * ny;
+                    hDv[i].assign((size_t)nx * ny, 0.0);
+                    hCf[i].assign((size_t)nx * ny, 0.0);
+                    for (int a = 0; a < nx; ++a) {
+                        const double lam = bx_.lam[a];
+                        double cprev = 0.0, eprev = 0.0;
+                        for (int b = 0; b < ny; ++b) {
+                            const double den = lam * Md[b] + Kd[b] - eprev * cprev;
+                            const double e = b + 1 < ny ? lam * Mo[b] + Ko[b] : 0.0;
+                            hDv[i][(size_t)b * nx + a] = 1.0 / den;
+                            hCf[i][(size_t)b * nx + a] = e / den;
+                            cprev = e / den;
+                            eprev = e;
+                        }
+                    }
+                }
+            });
+        for (auto &t : th) t.join();
+    }
     auto upload_prec = [&](auto tag) -> int {
         using T = decltype(tag);
         BVec<T> &v = vecs<T>(B);
@@ -995,23 +1126,29 @@ int setup_fd(iga_batch *B)
         size_t wtot = 0;
         for (int i = 0; i < B->count; ++i) wtot += (size_t)(B->plans[i]->m - 2) * (B->plans[i]->n - 2);
         int st;
-        if ((st = bmalloc(&v.W1, wtot)) || (st = bmalloc(&v.W2, wtot))) return st;
+        if ((st = bmalloc(&v.W1, wtot)) || (st = bmalloc(&v.Dv, wtot)) || (st = bmalloc(&v.Cf, wtot))) return st;
+        std::vector<T> stage;
         size_t wo = 0;
         for (int i = 0; i < B->count; ++i) {
             const iga_plan *pl = B->plans[i];
             FdProb<T> &f = fp[i];
             f.Vx = V[bx[i]];
             f.lx = L[bx[i]];
-            f.Vy = V[by[i]];
-            f.ly = L[by[i]];
+            f.yc = B->ycoef[by[i]];
             f.W1 = v.W1 + wo;
-            f.W2 = v.W2 + wo;
+            f.Dv = v.Dv + wo;
+            f.Cf = v.Cf + wo;
             f.off = B->off[i];
             f.m = pl->m;
             f.n = pl->n;
             f.nx = pl->m - 2;
             f.ny = pl->n - 2;
-            wo += (size_t)f.nx * f.ny;
+            const size_t nn = (size_t)f.nx * f.ny;
+            stage.assign(hDv[i].begin(), hDv[i].end());
+            BT_TRY(cudaMemcpy(v.Dv + wo, stage.data(), sizeof(T) * nn, cudaMemcpyHostToDevice));
+            stage.assign(hCf[i].begin(), hCf[i].end());
+            BT_TRY(cudaMemcpy(v.Cf + wo, stage.data(), sizeof(T) * nn, cudaMemcpyHostToDevice));
+            wo += nn;
         }
         return bupload(&v.fd, fp);
     };
@@ -1031,6 +1168,16 @@ int setup_fd(iga_batch *B)
     for (auto &t : tl) tiles.push_back(t.second);
     if (tiles.empty()) tiles.push_back(make_int4(0, 0, 0, 0));   // never active: nx or ny is 0
     B->ntiles = (int)tl.size();
+    // row-solve blocks: (problem, first x mode) for every 32 modes
+    std::vector<int2> rows;
+    for (int i = 0; i < B->count; ++i) {
+        const int nx = B->plans[i]->m - 2, ny = B->plans[i]->n - 2;
+        if (nx <= 0 || ny <= 0) continue;
+        for (int a0 = 0; a0 < nx; a0 += 32) rows.push_back(make_int2(i, a0));
+    }
+    B->nrows = (int)rows.size();
+    if (rows.empty()) rows.push_back(make_int2(0, 0));
+    if ((st = bupload(&B->rows, rows))) return st;
     if ((st = bupload(&B->tiles, tiles))) return st;
     B->fd_ready = true;
     return IGA_OK;
@@ -1091,14 +1238,14 @@ int setup_items(iga_batch *B, int pi)
 void free_vecs_common(BVec<double> &v)
 {
     for (void *p : {(void *)v.x, (void *)v.r, (void *)v.z, (void *)v.p, (void *)v.q, (void *)v.b, (void *)v.prm,
-                    (void *)v.fd, (void *)v.W1, (void *)v.W2})
+                    (void *)v.fd, (void *)v.W1, (void *)v.Dv, (void *)v.Cf})
         if (p) cudaFree(p);
     for (double *p : v.basis) cudaFree(p);
 }
 void free_vecs_common(BVec<float> &v)
 {
     for (void *p : {(void *)v.x, (void *)v.r, (void *)v.z, (void *)v.p, (void *)v.q, (void *)v.b, (void *)v.prm,
-                    (void *)v.fd, (void *)v.W1, (void *)v.W2})
+                    (void *)v.fd, (void *)v.W1, (void *)v.Dv, (void *)v.Cf})
         if (p) cudaFree(p);
     for (float *p : v.basis) cudaFree(p);
 }
@@ -1127,6 +1274,11 @@ int create_batch(const iga_mesh_desc *meshes, int count, int precision, int devi
     for (int i = 0; i < count; ++i) {
         if (meshes[i].nElemX + meshes[i].p < 3 || meshes[i].nElemY + meshes[i].q < 3) {
             set_error("iga_batch_create: every patch needs an interior control point in each direction");
+            return fail(IGA_ERR_UNSUPPORTED);
+        }
+        if (meshes[i].nElemY + meshes[i].q - 2 > kRowSeg * kRowLen) {
+            set_error("iga_batch_create: problem " + std::to_string(i) + " has more than " +
+                      std::to_string(kRowSeg * kRowLen) + " free control points in y (batches hold small patches)");
             return fail(IGA_ERR_UNSUPPORTED);
         }
         if (meshes[i].kappa) {
@@ -1295,7 +1447,8 @@ int iga_batch_destroy(iga_batch *B)
     for (BGroup &G : B->groups)
         for (int pi = 0; pi < 2; ++pi)
             if (G.items[pi]) cudaFree(G.items[pi]);
-    for (void *p : {(void *)B->chunks, (void *)B->tiles, (void *)B->c0, (void *)B->nc, (void *)B->d_off,
+    for (double *p : B->ycoef) cudaFree(p);
+    for (void *p : {(void *)B->chunks, (void *)B->tiles, (void *)B->rows, (void *)B->c0, (void *)B->nc, (void *)B->d_off,
                     (void *)B->partials, (void *)B->counters, (void *)B->sc, (void *)B->cfg, (void *)B->act,
                     (void *)B->act64, (void *)B->ones})
         if (p) cudaFree(p);

@@ -183,20 +183,33 @@ int warps_for(int P, int prec, int geom)
 }
 
 // Rows per strip: the candidate whose CTA count fills the SMs best, with a
-// small penalty on short strips (more seam traffic).
-static int rows_for(int nex, int ney, int W, int nsm)
+// small penalty on short strips (more seam traffic). A MIXED plan launches
+// its FP64 and FP32 operators with different warps per CTA (Ws) on the same
+// strips: each precision's cost is taken relative to its own best and the
+// candidate with the smallest sum wins.
+static double strip_cost(int NSX, int ney, int TY, int W, int nsm)
+{
+    const int NSY = (ney + TY - 1) / TY;
+    const long long ctas = (long long)NSX * ((NSY + W - 1) / W);
+    const long long waves = (ctas + nsm - 1) / nsm;
+    const double work = (double)waves * W * (TY + 2.0);   // per-SM time in strip-row units
+    return work * (1.0 + 0.5 * 3.0 / TY);
+}
+
+static int rows_for(int nex, int ney, const std::vector<int> &Ws, int nsm)
 {
     const int NSX = (nex + kSW - 1) / kSW;
+    static const int cands[] = {64, 48, 32, 24, 16};
+    std::vector<double> best_w(Ws.size(), 1e300);
+    for (size_t k = 0; k < Ws.size(); ++k)
+        for (int TY : cands) best_w[k] = std::min(best_w[k], strip_cost(NSX, ney, TY, Ws[k], nsm));
     int best = 64;
     double best_cost = 1e300;
-    for (int TY : {64, 48, 32, 24, 16}) {
-        const int NSY = (ney + TY - 1) / TY;
-        const long long ctas = (long long)NSX * ((NSY + W - 1) / W);
-        const long long waves = (ctas + nsm - 1) / nsm;
-        const double work = (double)waves * W * (TY + 2.0);   // per-SM time in strip-row units
-        const double cost = work * (1.0 + 0.5 * 3.0 / TY);
-        if (cost < best_cost - 1e-9) {
-            best_cost = cost;
+    for (int TY : cands) {
+        double c = 0.0;
+        for (size_t k = 0; k < Ws.size(); ++k) c += strip_cost(NSX, ney, TY, Ws[k], nsm) / best_w[k];
+        if (c < best_cost - 1e-9) {
+            best_cost = c;
             best = TY;
         }
     }
@@ -465,9 +478,10 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     pl->bc = opts.bc;
     pl->device = opts.device;
     pl->patch = P;
-    const int Wmin = std::min(opts.precision == IGA_FP32 ? 16 : warps_for(P.p, IGA_FP64, opts.geometry),
-                              opts.precision == IGA_FP64 ? 16 : warps_for(P.p, IGA_FP32, opts.geometry));
-    const int TY = opts.rows_per_strip > 0 ? opts.rows_per_strip : rows_for(P.nex, P.ney, Wmin, nsm);
+    std::vector<int> Ws;
+    if (opts.precision != IGA_FP32) Ws.push_back(warps_for(P.p, IGA_FP64, opts.geometry));
+    if (opts.precision != IGA_FP64) Ws.push_back(warps_for(P.p, IGA_FP32, opts.geometry));
+    const int TY = opts.rows_per_strip > 0 ? opts.rows_per_strip : rows_for(P.nex, P.ney, Ws, nsm);
     if (TY < P.p || TY > 1024) {
         delete pl;
         set_error("rows_per_strip must be in [p, 1024]");
