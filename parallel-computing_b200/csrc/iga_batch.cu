@@ -33,6 +33,7 @@
 #include "iga_fem.hpp"
 #include "iga_plan.hpp"
 #include "iga_tune.hpp"
+#include "iga_umma.cuh"
 
 namespace iga {
 
@@ -370,6 +371,7 @@ __global__ void __launch_bounds__(kBT) bk_cond(const int *__restrict__ act, int 
 template <typename T>
 struct FdProb {
     const T *Vx, *lx;      // x eigenvectors (column-major, ld nx) and eigenvalues
+    const T *VxT;          // the transpose of Vx (column-major), for the tcgen05 tiles
     const T *Dv, *Cf;      // LDL^T factors of the y systems: 1 / pivot, upper off-diagonal; [b][a], ld nx
     const double *yc;      // free y nodes' pencil Kd | Ko | Md | Mo (ny each)
     T *W1;                 // nx * ny work matrix
@@ -667,6 +669,163 @@ __global__ void __launch_bounds__(128) fd_gemm_kernel(const FdProb<T> *__restric
             }
 }
 
+// FP32 preconditioner tiles on the 5th-generation tensor cores (tcgen05,
+// kind::tf32): C[a + b ldc] = sum_k A[a lda + k] B[b ldb + k] for a 128 x 64
+// output tile of one problem, the FP32 accumulator in TMEM.
+//   stage 1: A rows = Vx columns (Vx^T), B rows = R^T (r + m + 1, ld m), C = W1
+//   stage 3: A rows = VxT columns (Vx),   B rows = W1^T (ld nx),        C = z + m + 1 (ld m)
+// All 128 threads stage 32-wide K slices (rounded to TF32) into two shared
+// memory buffers in the no-swizzle K-major layout; thread 0 issues four
+// 128 x 64 x 8 MMAs per slice and commits them to the buffer's mbarrier,
+// which the threads wait on (bounded) before refilling that buffer. The
+// epilogue reads the accumulator with tcgen05.ld (warp w: rows 32w .. 32w+31).
+constexpr int kUM = 128, kUN = 64, kUK = 32;
+constexpr int kALbo = (kUM / 8) * 128 + 16;   // K-chunk stride of an A buffer (+16 B: conflict-free stores)
+constexpr int kBLbo = (kUN / 8) * 128 + 16;
+constexpr int kAStage = 8 * kALbo, kBStage = 8 * kBLbo;   // 8 chunks of 4 values = 32 k
+constexpr int kUmmaSmem = 2 * (kAStage + kBStage) + 64;
+
+template <int STAGE>
+__global__ void __launch_bounds__(128) fd_umma_kernel(const FdProb<float> *__restrict__ fps,
+                                                      const int4 *__restrict__ tiles, const int *__restrict__ act,
+                                                      const float *__restrict__ rb, float *__restrict__ zb,
+                                                      int *__restrict__ err)
+{
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + 2 * (kAStage + kBStage));
+    uint32_t *tbase = reinterpret_cast<uint32_t *>(bars + 2);
+    const int4 tl = tiles[blockIdx.x];
+    if (!act[tl.x]) return;
+    const FdProb<float> &f = fps[tl.x];
+    const int nx = f.nx, ny = f.ny, m = f.m, K = nx;
+    const int a0 = tl.y * kUM, b0 = tl.z * kUN;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const float *A, *Bm;
+    float *C;
+    int lda, ldb, ldc;
+    if (STAGE == 1) {
+        A = f.Vx; lda = nx; Bm = rb + f.off + m + 1; ldb = m; C = f.W1; ldc = nx;
+    } else {
+        A = f.VxT; lda = nx; Bm = f.W1; ldb = nx; C = zb + f.off + m + 1; ldc = m;
+    }
+    if (STAGE == 1 && tl.y == 0 && tl.z == 0) {   // boundary ring: identity rows of K_fem
+        const float *r = rb + f.off;
+        float *z = zb + f.off;
+        const int n = f.n, nb = 2 * m + 2 * (n - 2);
+        for (int u = tid; u < nb; u += 128) {
+            int idx;
+            if (u < m) idx = u;
+            else if (u < 2 * m) idx = (n - 1) * m + (u - m);
+            else {
+                const int v = u - 2 * m;
+                idx = (1 + v / 2) * m + ((v & 1) ? (m - 1) : 0);
+            }
+            z[idx] = r[idx];
+        }
+    }
+    if (warp == 0) {
+        umma::alloc(tbase, kUN);
+        umma::relinquish();
+    }
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tbase;
+
+    // thread (warp, lane) moves k = lane of the slice for rows warp + 4 i
+    float ra[kUM / 4], rv[kUN / 4];
+    auto fetch = [&](int k0) {
+        const int k = k0 + lane;
+        const bool kin = k < K;
+#pragma unroll
+        for (int i = 0; i < kUM / 4; ++i) {
+            const int a = a0 + warp + 4 * i;
+            ra[i] = (kin && a < nx) ? A[(size_t)a * lda + k] : 0.0f;
+        }
+#pragma unroll
+        for (int i = 0; i < kUN / 4; ++i) {
+            const int b = b0 + warp + 4 * i;
+            rv[i] = (kin && b < ny) ? Bm[(size_t)b * ldb + k] : 0.0f;
+        }
+    };
+    auto stash = [&](int buf) {
+        unsigned char *Ab = sm + buf * kAStage, *Bb = sm + 2 * kAStage + buf * kBStage;
+        const int ch = lane >> 2, w4 = (lane & 3) * 4;
+#pragma unroll
+        for (int i = 0; i < kUM / 4; ++i) {
+            const int r = warp + 4 * i;
+            *reinterpret_cast<float *>(Ab + ch * kALbo + (r >> 3) * 128 + (r & 7) * 16 + w4) = to_operand(ra[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < kUN / 4; ++i) {
+            const int r = warp + 4 * i;
+            *reinterpret_cast<float *>(Bb + ch * kBLbo + (r >> 3) * 128 + (r & 7) * 16 + w4) = to_operand(rv[i]);
+        }
+    };
+    constexpr uint32_t IDESC = umma::idesc_tf32<kUM, kUN>();
+    const int nk = (K + kUK - 1) / kUK;
+    fetch(0);
+    stash(0);
+    fence_proxy_async_smem();
+    __syncthreads();
+    bool failed = false;
+    int last = -1;   // last slice whose MMAs were issued
+    for (int kt = 0; kt < nk; ++kt) {
+        const int buf = kt & 1;
+        if (tid == 0) {
+            umma::fence_after_sync();
+            const unsigned char *Ab = sm + buf * kAStage, *Bb = sm + 2 * kAStage + buf * kBStage;
+#pragma unroll
+            for (int j = 0; j < kUK / 8; ++j)
+                umma::mma_tf32(tmem, umma::smem_desc(Ab + 2 * j * kALbo, kALbo, 128),
+                               umma::smem_desc(Bb + 2 * j * kBLbo, kBLbo, 128), IDESC, (kt > 0 || j > 0) ? 1u : 0u);
+            umma::commit(&bars[buf]);
+        }
+        last = kt;
+        if (kt + 1 < nk) {
+            fetch((kt + 1) * kUK);
+            bool ok = true;
+            if (kt >= 1) ok = mbar_wait_bounded(&bars[(kt - 1) & 1], ((kt - 1) >> 1) & 1);   // buffer reused
+            failed = __syncthreads_or(!ok);
+            if (failed) break;
+            stash((kt + 1) & 1);
+            fence_proxy_async_smem();
+        }
+        __syncthreads();
+    }
+    // all MMAs done: the last commit tracks every earlier MMA of thread 0
+    const bool ok = mbar_wait_bounded(&bars[last & 1], (last >> 1) & 1);
+    failed = __syncthreads_or(failed || !ok);
+    if (failed) {
+        if (tid == 0) atomicExch(err, 8 /* IGA_ERR_TIMEOUT */);
+        mbar_wait_bounded(&bars[last & 1], (last >> 1) & 1);
+    } else {
+        umma::fence_after_sync();
+        const int a = a0 + 32 * warp + lane;
+#pragma unroll
+        for (int c0 = 0; c0 < kUN; c0 += 16) {
+            float v[16];
+            umma::ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+            umma::wait_ld();
+            if (a < nx) {
+#pragma unroll
+                for (int c = 0; c < 16; ++c) {
+                    const int b = b0 + c0 + c;
+                    if (b < ny) C[a + (size_t)b * ldc] = v[c];
+                }
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::dealloc(tmem, kUN);
+}
+
 // ------------------------------------------------------------ host state
 template <typename T>
 struct BVec {
@@ -694,8 +853,9 @@ struct iga_batch {
     std::vector<long long> off;   // count + 1
     long long ntot = 0;
     std::vector<BGroup> groups;
-    int nchunks = 0, ntiles = 0, nrows = 0;
-    int4 *chunks = nullptr, *tiles = nullptr;
+    int nchunks = 0, ntiles = 0, nrows = 0, ntiles_tc = 0;
+    int4 *chunks = nullptr, *tiles = nullptr, *tiles_tc = nullptr;
+    int *d_err = nullptr;   // device error flag of the tcgen05 tiles (bounded waits)
     int2 *rows = nullptr;
     std::vector<double *> ycoef;     // y pencils of the distinct 1-D grids
     int *c0 = nullptr, *nc = nullptr;
@@ -851,9 +1011,15 @@ int batch_pc(iga_batch *B, int pc, const T *r, T *z, const int *act, cudaStream_
         bk_copy<T><<<B->nchunks, kBT, 0, s>>>(d, act, r, z);
     } else {
         const FdProb<T> *fd = vecs<T>(B).fd;
-        fd_gemm_kernel<T, 1><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
-        fd_rows_kernel<T><<<B->nrows, dim3(32, kRowSeg), 0, s>>>(fd, B->rows, act);
-        fd_gemm_kernel<T, 3><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
+        if constexpr (sizeof(T) == 4) {   // TF32 tiles on tcgen05
+            fd_umma_kernel<1><<<B->ntiles_tc, 128, kUmmaSmem, s>>>(fd, B->tiles_tc, act, r, z, B->d_err);
+            fd_rows_kernel<T><<<B->nrows, dim3(32, kRowSeg), 0, s>>>(fd, B->rows, act);
+            fd_umma_kernel<3><<<B->ntiles_tc, 128, kUmmaSmem, s>>>(fd, B->tiles_tc, act, r, z, B->d_err);
+        } else {                          // FP64 tiles on DMMA
+            fd_gemm_kernel<T, 1><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
+            fd_rows_kernel<T><<<B->nrows, dim3(32, kRowSeg), 0, s>>>(fd, B->rows, act);
+            fd_gemm_kernel<T, 3><<<B->ntiles, 128, 0, s>>>(fd, B->tiles, act, r, z);
+        }
     }
     BT_TRY(cudaGetLastError());
     return IGA_OK;
@@ -1114,13 +1280,18 @@ int setup_fd(iga_batch *B)
     auto upload_prec = [&](auto tag) -> int {
         using T = decltype(tag);
         BVec<T> &v = vecs<T>(B);
-        std::vector<T *> V(bases.size()), L(bases.size());
+        std::vector<T *> V(bases.size()), L(bases.size()), VT(bases.size());
         for (size_t k = 0; k < bases.size(); ++k) {
+            const int nb = bases[k].n;
             std::vector<T> hv(bases[k].V.begin(), bases[k].V.end()), hl(bases[k].lam.begin(), bases[k].lam.end());
+            std::vector<T> ht((size_t)nb * nb);
+            for (int i = 0; i < nb; ++i)
+                for (int j = 0; j < nb; ++j) ht[(size_t)j * nb + i] = (T)bases[k].V[(size_t)i * nb + j];
             int st;
-            if ((st = bupload(&V[k], hv)) || (st = bupload(&L[k], hl))) return st;
+            if ((st = bupload(&V[k], hv)) || (st = bupload(&L[k], hl)) || (st = bupload(&VT[k], ht))) return st;
             v.basis.push_back(V[k]);
             v.basis.push_back(L[k]);
+            v.basis.push_back(VT[k]);
         }
         std::vector<FdProb<T>> fp(B->count);
         size_t wtot = 0;
@@ -1133,6 +1304,7 @@ int setup_fd(iga_batch *B)
             const iga_plan *pl = B->plans[i];
             FdProb<T> &f = fp[i];
             f.Vx = V[bx[i]];
+            f.VxT = VT[bx[i]];
             f.lx = L[bx[i]];
             f.yc = B->ycoef[by[i]];
             f.W1 = v.W1 + wo;
@@ -1178,6 +1350,24 @@ int setup_fd(iga_batch *B)
     B->nrows = (int)rows.size();
     if (rows.empty()) rows.push_back(make_int2(0, 0));
     if ((st = bupload(&B->rows, rows))) return st;
+    // 128 x 64 tiles of the tcgen05 path (FP32)
+    if (B->precision == IGA_MIXED) {
+        std::vector<std::pair<int, int4>> tt;
+        for (int i = 0; i < B->count; ++i) {
+            const int nx = B->plans[i]->m - 2, ny = B->plans[i]->n - 2;
+            if (nx <= 0 || ny <= 0) continue;
+            for (int a = 0; a < (nx + kUM - 1) / kUM; ++a)
+                for (int b = 0; b < (ny + kUN - 1) / kUN; ++b) tt.push_back({nx, make_int4(i, a, b, 0)});
+        }
+        std::stable_sort(tt.begin(), tt.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+        std::vector<int4> tc;
+        for (auto &t : tt) tc.push_back(t.second);
+        B->ntiles_tc = (int)tc.size();
+        if (tc.empty()) tc.push_back(make_int4(0, 0, 0, 0));
+        if ((st = bupload(&B->tiles_tc, tc))) return st;
+        BT_TRY(cudaFuncSetAttribute(fd_umma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kUmmaSmem));
+        BT_TRY(cudaFuncSetAttribute(fd_umma_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kUmmaSmem));
+    }
     if ((st = bupload(&B->tiles, tiles))) return st;
     B->fd_ready = true;
     return IGA_OK;
@@ -1341,6 +1531,8 @@ int create_batch(const iga_mesh_desc *meshes, int count, int precision, int devi
     if ((st = bupload(&B->chunks, ch)) || (st = bupload(&B->c0, c0)) || (st = bupload(&B->nc, nc)) ||
         (st = bupload(&B->d_off, B->off)))
         return fail(st);
+    if ((st = bmalloc(&B->d_err, 1))) return fail(st);
+    BT_TRY(cudaMemset(B->d_err, 0, sizeof(int)));
     if ((st = bmalloc(&B->partials, (size_t)B->nchunks * 4)) || (st = bmalloc(&B->counters, count)) ||
         (st = bmalloc(&B->sc, count)) || (st = bmalloc(&B->cfg, 1)) || (st = bmalloc(&B->act, count)) ||
         (st = bmalloc(&B->act64, count)))
@@ -1448,7 +1640,7 @@ int iga_batch_destroy(iga_batch *B)
         for (int pi = 0; pi < 2; ++pi)
             if (G.items[pi]) cudaFree(G.items[pi]);
     for (double *p : B->ycoef) cudaFree(p);
-    for (void *p : {(void *)B->chunks, (void *)B->tiles, (void *)B->rows, (void *)B->c0, (void *)B->nc, (void *)B->d_off,
+    for (void *p : {(void *)B->chunks, (void *)B->tiles, (void *)B->tiles_tc, (void *)B->d_err, (void *)B->rows, (void *)B->c0, (void *)B->nc, (void *)B->d_off,
                     (void *)B->partials, (void *)B->counters, (void *)B->sc, (void *)B->cfg, (void *)B->act,
                     (void *)B->act64, (void *)B->ones})
         if (p) cudaFree(p);
@@ -1601,6 +1793,13 @@ int iga_batch_solve(iga_batch *B, const double *b, double *x, const iga_solve_op
     BT_TRY(cudaStreamSynchronize(s));
     cudaEventDestroy(ev);
     if (st) return st;
+    int herr = 0;
+    BT_TRY(cudaMemcpy(&herr, B->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) {
+        BT_TRY(cudaMemset(B->d_err, 0, sizeof(int)));
+        set_error("iga_batch_solve: a bounded device wait gave up (tensor-core preconditioner tiles)");
+        return IGA_ERR_TIMEOUT;
+    }
     iga_batch_stats S{};
     int result = IGA_OK;
     for (int i = 0; i < B->count; ++i) {
