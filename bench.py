@@ -411,6 +411,24 @@ def our_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.profile_batch_pc:
+        shapes = ib.batch_problems(256, seed=2)
+        batch = ib.Batch([ib.unit_square(p, a, c) for p, a, c in shapes], precision=ib.MIXED,
+                         tune_file=ib.TUNE_FILE)
+        v = torch.from_numpy(splitmix_uniform(SEED, -1.0, 1.0, batch.ntot)).cuda()
+        w = torch.empty_like(v)
+        v32, w32 = v.float(), torch.empty_like(v, dtype=torch.float32)
+        for _ in range(3):
+            batch.pc_apply(v, w)
+            batch.pc_apply(v32, w32, precision=ib.FP32)
+            batch.apply(v, w)
+            batch.apply(v32, w32, precision=ib.FP32)
+        torch.cuda.synchronize()
+        batch.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
     if args.batch_only:
         res = time_batch(ib, torch, torch.cuda.current_stream(), barrier, max_over_ranks)
         if rank == 0:
@@ -568,6 +586,9 @@ def main():
     ap.add_argument("--skip-solve", action="store_true", help="skip the time-to-1e-10 solves")
     ap.add_argument("--batch-only", action="store_true",
                     help="time only the 256-problem batched solves (prints their JSON object)")
+    ap.add_argument("--profile-batch-pc", action="store_true",
+                    help="run the batched preconditioner and operator of the 256-problem batch a few times "
+                         "outside any graph (a target for ncu; prints nothing else)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
