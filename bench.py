@@ -275,6 +275,17 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
     # noise, J = |u - u_obs|^2 / 2; forward solve + adjoint solve + dJ/dkappa.
     out["adjoint_p3_512"] = time_adjoint(ib, torch, stream, barrier, max_over_ranks)
     out["batched_256"] = time_batch(ib, torch, stream, barrier, max_over_ranks)
+    # spectra (Lanczos on the PCG coefficients): kappa(K) grows like h^-2, the
+    # FEM-preconditioned kappa(M^-1 K) stays bounded
+    spectra = {}
+    for ne in (64, 256, 1024):
+        ps = ib.Plan(ib.unit_square(3, ne))
+        lo, hi, k = ps.spectrum(pc=ib.PC_NONE, steps=600)
+        plo, phi, pk = ps.spectrum(pc=ib.PC_FEM_EXACT, steps=200)
+        spectra[f"p3_{ne}x{ne}"] = {"kappa_K": hi / lo, "lanczos_steps_K": k, "kappa_fem_pc": phi / plo,
+                                     "lambda_fem_pc": [plo, phi], "lanczos_steps_pc": pk}
+        ps.close()
+    out["spectra"] = spectra
     # reference preconditioner, p=2 64x64 (the CPU-runnable configuration), for
     # f = 2 pi^2 sin sin and for the reference's own load x(1-x)y(1-y)
     m2 = ib.unit_square(2, 64)

@@ -105,6 +105,18 @@ int iga_adjoint_grad(iga_plan *plan, const double *u_dev, const double *lambda_d
  * abscissae of the IGA knot vector. */
 int iga_fem_nodes(const iga_plan *plan, double *gx, double *gy);
 
+/* Extreme eigenvalues of the SPD operator K (pc = IGA_PC_NONE) or of the
+ * preconditioned M^-1 K (pc = IGA_PC_FEM_EXACT or IGA_PC_FEM_CG) on the free
+ * control points, from `steps` Lanczos steps: the coefficients of a standard
+ * PCG (FP64, device) on a seeded random right-hand side form the Lanczos
+ * matrix, whose extreme eigenvalues are returned (host). steps_done (may be
+ * NULL) receives the steps taken (fewer when the Krylov space is exhausted).
+ * The reference studies the same extremes with SLEPc's Lanczos SVD
+ * (eigenvalue_problem/driver.cpp:252-411); condition numbers are
+ * lam_max / lam_min. */
+int iga_spectrum_estimate(iga_plan *plan, int pc, int steps, uint64_t seed, double *lam_min, double *lam_max,
+                          int *steps_done);
+
 #ifdef __cplusplus
 }
 #endif

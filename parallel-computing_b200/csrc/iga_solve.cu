@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <random>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -1544,6 +1545,82 @@ int iga_solve(iga_plan *pl, const double *b, double *x, const iga_solve_opts *o_
     stt.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (stats) *stats = stt;
     return result;
+}
+
+int iga_spectrum_estimate(iga_plan *pl, int pc, int steps, uint64_t seed, double *lam_min, double *lam_max,
+                          int *steps_done)
+{
+    if (!pl || !lam_min || !lam_max || steps < 1) return IGA_ERR_ARG;
+    if (pc != IGA_PC_NONE && pc != IGA_PC_FEM_CG && pc != IGA_PC_FEM_EXACT) return IGA_ERR_ARG;
+    if (!pl->op64.ready) {
+        set_error("iga_spectrum_estimate needs the FP64 operator");
+        return IGA_ERR_ARG;
+    }
+    SolverState *S;
+    int st;
+    if ((st = ensure_state(pl, &S))) return st;
+    SOLVE_TRY(cudaSetDevice(pl->device));
+    if ((st = alloc_prec(S->d, pl, *S))) return st;
+    PrecState<double> &ps = S->d;
+    const long long N = pl->nfunc;
+    const cudaStream_t s = S->stream;
+    iga_solve_opts o;
+    iga_solve_opts_default(&o);
+    o.pc = pc;
+    o.pc_rtol = 1e-13;
+    // seeded random start vector, zero on the boundary ring (the Krylov space
+    // stays on the free control points: identity rows and identity PC rows)
+    std::vector<double> h((size_t)N);
+    std::mt19937_64 gen(seed);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    for (int j = 0; j < pl->n; ++j)
+        for (int i = 0; i < pl->m; ++i)
+            h[(size_t)j * pl->m + i] = (i == 0 || j == 0 || i == pl->m - 1 || j == pl->n - 1) ? 0.0 : nd(gen);
+    SOLVE_TRY(cudaMemcpyAsync(ps.r, h.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    zero_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.x, N);
+    int64_t pcits = 0;
+    if ((st = pc_apply(ps, pl, S, o, ps.r, ps.z, o.pc_rtol, pcits))) return st;
+    dot_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, N, &S->s->rz, S->partials, S->counter);
+    pcg_p_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.z, N, S->s, 1);
+    SOLVE_TRY(cudaMemsetAsync(&S->s->breakdown, 0, sizeof(int), s));
+    if ((st = sync_scalars(S))) return st;
+    const double rr0 = S->h->rz;
+    std::vector<double> alpha, beta;
+    for (int k = 0; k < steps; ++k) {
+        const double rz_old = S->h->rz;
+        if ((st = iga_apply_internal_sb(pl, IGA_FP64, ps.p, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY))) return st;
+        pcg_pq_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.q, N, S->s, S->partials, S->counter);
+        pcg_xr_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.x, ps.r, ps.p, ps.q, N, S->s, S->partials,
+                                                             S->counter);
+        if ((st = pc_apply(ps, pl, S, o, ps.r, ps.z, o.pc_rtol, pcits))) return st;
+        dot_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, N, &S->s->rz, S->partials, S->counter);
+        if ((st = sync_scalars(S))) return st;
+        if (S->h->breakdown || !(S->h->alpha > 0.0)) break;
+        alpha.push_back(S->h->alpha);
+        const double rz_new = S->h->rz;
+        if (!(rz_new > 1e-28 * rr0)) break;   // the Krylov space is exhausted
+        beta.push_back(rz_new / rz_old);
+        S->h->beta = beta.back();
+        SOLVE_TRY(cudaMemcpyAsync(&S->s->beta, &S->h->beta, sizeof(double), cudaMemcpyHostToDevice, s));
+        pcg_p_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.z, N, S->s, 0);
+    }
+    const int K = (int)alpha.size();
+    if (K < 1) {
+        set_error("iga_spectrum_estimate: no Lanczos step completed");
+        return IGA_ERR_BREAKDOWN;
+    }
+    // Lanczos matrix of the PCG coefficients: T_kk = 1/a_k + b_{k-1}/a_{k-1},
+    // T_k,k+1 = sqrt(b_k) / a_k (M^-1 K in the M-inner product)
+    std::vector<double> Td(K), To(K, 0.0), Md(K, 1.0), Mo(K, 0.0), lam(K), V((size_t)K * K);
+    for (int k = 0; k < K; ++k) {
+        Td[k] = 1.0 / alpha[k] + (k > 0 ? beta[k - 1] / alpha[k - 1] : 0.0);
+        if (k + 1 < K) To[k] = -std::sqrt(beta[k]) / alpha[k];
+    }
+    pencil_eig(K, Td.data(), To.data(), Md.data(), Mo.data(), lam.data(), V.data());
+    *lam_min = lam[0];
+    *lam_max = lam[K - 1];
+    if (steps_done) *steps_done = K;
+    return IGA_OK;
 }
 
 }  // extern "C"

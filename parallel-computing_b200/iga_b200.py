@@ -129,6 +129,9 @@ SIGNATURES = [
     ("iga_batch_autotune", ctypes.c_int, [VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p]),
     ("iga_tune_lookup", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    ("iga_spectrum_estimate", ctypes.c_int, [VP, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+                                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_int)]),
     ("iga_part_open", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(VP)]),
     ("iga_part_close", ctypes.c_int, [VP]),
     ("iga_part_get_info", ctypes.c_int, [VP, ctypes.POINTER(PartInfo)]),
@@ -539,6 +542,13 @@ class Plan:
     def adjoint_grad(self, u, lam, g, stream=None):
         _check(_lib().iga_adjoint_grad(self.h, _ptr(u), _ptr(lam), _ptr(g), _stream(stream)), "iga_adjoint_grad")
         return g
+
+    def spectrum(self, pc=PC_FEM_EXACT, steps=200, seed=7):
+        """(lam_min, lam_max, steps) of K (pc=PC_NONE) or M^-1 K on the free control points (Lanczos)."""
+        lo, hi, k = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _check(_lib().iga_spectrum_estimate(self.h, pc, steps, seed, ctypes.byref(lo), ctypes.byref(hi),
+                                            ctypes.byref(k)), "iga_spectrum_estimate")
+        return lo.value, hi.value, k.value
 
     def fem_nodes(self):
         gx = np.empty(self.mesh["nex"] + self.mesh["p"])
