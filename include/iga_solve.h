@@ -32,9 +32,15 @@ enum {
     IGA_PC_FEM_EXACT = 2  /* the same FEM matrix inverted exactly (tensor-product fast diagonalisation) */
 };
 
+enum {
+    IGA_MIXED_PC = 3   /* solve precision: FP64 flexible PCG (FP64 operator and vectors) with the
+                          preconditioner evaluated in FP32 (TF32 tensor-core GEMMs) */
+};
+
 typedef struct {
     int precision;     /* IGA_FP64: FP64 PCG. IGA_MIXED: FP32 PCG sweeps (FP32 operator and
-                          preconditioner) wrapped in FP64 iterative refinement. */
+                          preconditioner) wrapped in FP64 iterative refinement. IGA_MIXED_PC:
+                          FP64 PCG, FP32 preconditioner (needs only the FP64 operator). */
     int pc;            /* IGA_PC_* */
     double rtol;       /* target relative true residual (FP64) */
     int max_it;        /* outer PCG iterations per solve / per FP32 sweep */
@@ -59,7 +65,7 @@ void iga_solve_opts_default(iga_solve_opts *opts);
 
 /* Solve K x = b on the device (b, x: nfunc doubles, caller-owned). The plan
  * must hold the FP64 operator; IGA_MIXED needs a plan created with
- * precision IGA_MIXED (both operators). */
+ * precision IGA_MIXED (both operators); IGA_MIXED_PC runs on either. */
 int iga_solve(iga_plan *plan, const double *b_dev, double *x_dev, const iga_solve_opts *opts,
               iga_solve_stats *stats, void *stream);
 

@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/iga_solve.h"
@@ -25,12 +26,12 @@
 
 namespace iga {
 
-constexpr int kRedBlocks = 296;   // fixed grid of every reduction kernel (2 x 148 SMs)
+constexpr int kRedBlocks = 592;   // fixed grid of every reduction kernel (4 x 148 SMs)
 constexpr int kThreads = 256;
 constexpr int kChunk = 16;        // inner CG iterations per captured graph
 
 struct DevScalars {
-    double alpha, beta, rz, rr, rr0, tol2, bb;      // outer PCG
+    double alpha, beta, rz, rzo, rr, rr0, tol2, bb; // outer PCG (rzo = r_new . z_old)
     double ialpha, ibeta, irz, irr, itol2;          // inner FEM-CG
     int done, breakdown, idone, iiters, ibreak, imax;
     int it, maxit;                                  // outer PCG in a device-side loop
@@ -271,25 +272,87 @@ __global__ void icg_p_kernel(InnerCG<T> a)
 }
 
 // ------------------------------------------------------------ outer PCG vector kernels
+// Elementwise loops move 16 bytes per access (4 floats / 2 doubles) when every
+// array of the kernel starts on a 16-byte boundary; the last N % VN entries
+// (or all of them, for unaligned arrays) take scalar accesses. The thread that
+// handles an entry depends only on N and the grid, so the reductions stay
+// deterministic.
+template <typename T>
+struct alignas(16) Pk {
+    static constexpr int n = 16 / sizeof(T);
+    T v[n];
+};
+
+template <typename T>
+__device__ __forceinline__ Pk<T> ldp(const T *a, long long i)
+{
+    return *reinterpret_cast<const Pk<T> *>(a + i);
+}
+
+template <typename T>
+__device__ __forceinline__ void stp(T *a, long long i, const Pk<T> &v)
+{
+    *reinterpret_cast<Pk<T> *>(a + i) = v;
+}
+
+__device__ __forceinline__ bool al16(const void *a) { return ((uintptr_t)a & 15u) == 0; }
+
+// Calls f(i, c) for the first entry i and count c of every pack this thread
+// owns, then f(i, 1) for its scalar tail entries.
+template <typename T, typename F>
+__device__ __forceinline__ void vloop(long long N, bool vec, F &&f)
+{
+    constexpr int VN = Pk<T>::n;
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x, st = (long long)gridDim.x * blockDim.x;
+    const long long nv = vec ? N / VN : 0;
+    for (long long k = g; k < nv; k += st) f(k * VN, VN);
+    for (long long i = nv * VN + g; i < N; i += st) f(i, 1);
+}
+
+// Loads c entries (a pack or one scalar) starting at i.
+template <typename T>
+__device__ __forceinline__ Pk<T> ldc(const T *a, long long i, int c)
+{
+    if (c > 1) return ldp(a, i);
+    Pk<T> v;
+    v.v[0] = a[i];
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ void stc(T *a, long long i, int c, const Pk<T> &v)
+{
+    if (c > 1) stp(a, i, v);
+    else a[i] = v.v[0];
+}
+
 template <typename T>
 __global__ void dot_kernel(const T *__restrict__ a, const T *__restrict__ b, long long N, double *out, double *partials,
                            unsigned *counter)
 {
     double v[1] = {0.0};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
-        v[0] += (double)a[t] * (double)b[t];
+    vloop<T>(N, al16(a) && al16(b), [&](long long i, int c) {
+        const Pk<T> x = ldc(a, i, c), y = ldc(b, i, c);
+#pragma unroll
+        for (int k = 0; k < Pk<T>::n; ++k)
+            if (k < c) v[0] += (double)x.v[k] * (double)y.v[k];
+    });
     double tot[1];
     if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) *out = tot[0];
 }
 
-// alpha = rz / (p.q) from the device scalars, x += alpha p, r -= alpha q, rr = r.r
+// alpha = rz / (p.q) from the device scalars
 template <typename T>
 __global__ void pcg_pq_kernel(const T *__restrict__ p, const T *__restrict__ q, long long N, DevScalars *s,
                               double *partials, unsigned *counter)
 {
     double v[1] = {0.0};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
-        v[0] += (double)p[t] * (double)q[t];
+    vloop<T>(N, al16(p) && al16(q), [&](long long i, int c) {
+        const Pk<T> a = ldc(p, i, c), b = ldc(q, i, c);
+#pragma unroll
+        for (int k = 0; k < Pk<T>::n; ++k)
+            if (k < c) v[0] += (double)a.v[k] * (double)b.v[k];
+    });
     double tot[1];
     if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) {
         if (!(tot[0] > 0.0)) {
@@ -301,40 +364,56 @@ __global__ void pcg_pq_kernel(const T *__restrict__ p, const T *__restrict__ q, 
     }
 }
 
+// x += alpha p, r -= alpha q; rr = r.r and rzo = r.z with the previous
+// preconditioned residual z (the flexible beta's correction term, taken here
+// so that z need not be kept). Returns the totals to the last block.
 template <typename T>
-__global__ void pcg_xr_kernel(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p, const T *__restrict__ q,
-                              long long N, DevScalars *s, double *partials, unsigned *counter)
+__device__ __forceinline__ bool xr_update(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p,
+                                          const T *__restrict__ q, const T *__restrict__ z, long long N,
+                                          const DevScalars *s, double *partials, unsigned *counter, double (&tot)[2])
 {
     const T al = (T)s->alpha;
-    double v[1] = {0.0};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
-        x[t] += al * p[t];
-        const T rv = r[t] - al * q[t];
-        r[t] = rv;
-        v[0] += (double)rv * (double)rv;
+    double v[2] = {0.0, 0.0};
+    vloop<T>(N, al16(x) && al16(r) && al16(p) && al16(q) && al16(z), [&](long long i, int c) {
+        Pk<T> xv = ldc(x, i, c), rv = ldc(r, i, c);
+        const Pk<T> pv = ldc(p, i, c), qv = ldc(q, i, c), zv = ldc(z, i, c);
+#pragma unroll
+        for (int k = 0; k < Pk<T>::n; ++k) {
+            if (k < c) {
+                xv.v[k] += al * pv.v[k];
+                rv.v[k] -= al * qv.v[k];
+                v[0] += (double)rv.v[k] * (double)rv.v[k];
+                v[1] += (double)rv.v[k] * (double)zv.v[k];
+            }
+        }
+        stc(x, i, c, xv);
+        stc(r, i, c, rv);
+    });
+    return reduce_last<2>(v, partials, counter, tot);
+}
+
+template <typename T>
+__global__ void pcg_xr_kernel(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p, const T *__restrict__ q,
+                              const T *__restrict__ z, long long N, DevScalars *s, double *partials, unsigned *counter)
+{
+    double tot[2];
+    if (xr_update(x, r, p, q, z, N, s, partials, counter, tot) && threadIdx.x == 0) {
+        s->rr = tot[0];
+        s->rzo = tot[1];
     }
-    double tot[1];
-    if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) s->rr = tot[0];
 }
 
 // Same update inside the device-side loop: counts the iteration and sets the
 // loop's condition (continue while rr > tol2, it < maxit, no breakdown, finite).
 template <typename T>
 __global__ void pcg_xr_cond_kernel(T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p,
-                                   const T *__restrict__ q, long long N, DevScalars *s, double *partials,
-                                   unsigned *counter, cudaGraphConditionalHandle h)
+                                   const T *__restrict__ q, const T *__restrict__ z, long long N, DevScalars *s,
+                                   double *partials, unsigned *counter, cudaGraphConditionalHandle h)
 {
-    const T al = (T)s->alpha;
-    double v[1] = {0.0};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
-        x[t] += al * p[t];
-        const T rv = r[t] - al * q[t];
-        r[t] = rv;
-        v[0] += (double)rv * (double)rv;
-    }
-    double tot[1];
-    if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) {
+    double tot[2];
+    if (xr_update(x, r, p, q, z, N, s, partials, counter, tot) && threadIdx.x == 0) {
         s->rr = tot[0];
+        s->rzo = tot[1];
         s->it += 1;
         const bool go = tot[0] > s->tol2 && s->it < s->maxit && !s->breakdown && tot[0] == tot[0];
         cudaGraphSetConditional(h, go ? 1u : 0u);
@@ -349,19 +428,22 @@ __global__ void loop_init_kernel(DevScalars *s, double tol2, int maxit)
     s->breakdown = 0;
 }
 
-// Flexible (Polak-Ribiere) beta = r.(z - z_old) / rz_old; rz = r.z.
+// Flexible (Polak-Ribiere) beta = r.(z - z_old) / rz_old with r.z_old = rzo
+// from the update kernel; rz = r.z.
 template <typename T>
-__global__ void pcg_beta_kernel(const T *__restrict__ r, const T *__restrict__ z, const T *__restrict__ zo, long long N,
-                                DevScalars *s, double *partials, unsigned *counter)
+__global__ void pcg_beta_kernel(const T *__restrict__ r, const T *__restrict__ z, long long N, DevScalars *s,
+                                double *partials, unsigned *counter)
 {
-    double v[2] = {0.0, 0.0};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
-        v[0] += (double)r[t] * (double)z[t];
-        v[1] += (double)r[t] * (double)zo[t];
-    }
-    double tot[2];
-    if (reduce_last<2>(v, partials, counter, tot) && threadIdx.x == 0) {
-        s->beta = (tot[0] - tot[1]) / s->rz;
+    double v[1] = {0.0};
+    vloop<T>(N, al16(r) && al16(z), [&](long long i, int c) {
+        const Pk<T> a = ldc(r, i, c), b = ldc(z, i, c);
+#pragma unroll
+        for (int k = 0; k < Pk<T>::n; ++k)
+            if (k < c) v[0] += (double)a.v[k] * (double)b.v[k];
+    });
+    double tot[1];
+    if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) {
+        s->beta = (tot[0] - s->rzo) / s->rz;
         s->rz = tot[0];
     }
 }
@@ -370,8 +452,17 @@ template <typename T>
 __global__ void pcg_p_kernel(T *__restrict__ p, const T *__restrict__ z, long long N, const DevScalars *s, int first)
 {
     const T be = first ? T(0) : (T)s->beta;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
-        p[t] = first ? z[t] : z[t] + be * p[t];   // the first direction never reads stale p
+    vloop<T>(N, al16(p) && al16(z), [&](long long i, int c) {
+        const Pk<T> zv = ldc(z, i, c);
+        if (first) {   // the first direction never reads stale p
+            stc(p, i, c, zv);
+            return;
+        }
+        Pk<T> pv = ldc(p, i, c);
+#pragma unroll
+        for (int k = 0; k < Pk<T>::n; ++k) pv.v[k] = zv.v[k] + be * pv.v[k];
+        stc(p, i, c, pv);
+    });
 }
 
 // r = b - Ax (FP64), rr = r.r, bb = b.b
@@ -379,12 +470,19 @@ __global__ void residual_kernel(const double *__restrict__ b, const double *__re
                                 long long N, DevScalars *s, double *partials, unsigned *counter)
 {
     double v[2] = {0.0, 0.0};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
-        const double rv = b[t] - Ax[t];
-        r[t] = rv;
-        v[0] += rv * rv;
-        v[1] += b[t] * b[t];
-    }
+    vloop<double>(N, al16(b) && al16(Ax) && al16(r), [&](long long i, int c) {
+        const Pk<double> bv = ldc(b, i, c), av = ldc(Ax, i, c);
+        Pk<double> rv;
+#pragma unroll
+        for (int k = 0; k < Pk<double>::n; ++k) {
+            rv.v[k] = bv.v[k] - av.v[k];
+            if (k < c) {
+                v[0] += rv.v[k] * rv.v[k];
+                v[1] += bv.v[k] * bv.v[k];
+            }
+        }
+        stc(r, i, c, rv);
+    });
     double tot[2];
     if (reduce_last<2>(v, partials, counter, tot) && threadIdx.x == 0) {
         s->rr = tot[0];
@@ -398,11 +496,16 @@ __global__ void sub_kernel(const T *__restrict__ b, const T *__restrict__ q, T *
                            DevScalars *s, double *partials, unsigned *counter)
 {
     double v[1] = {0.0};
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x) {
-        const T rv = b[t] - q[t];
-        r[t] = rv;
-        v[0] += (double)rv * (double)rv;
-    }
+    vloop<T>(N, al16(b) && al16(q) && al16(r), [&](long long i, int c) {
+        const Pk<T> bv = ldc(b, i, c), qv = ldc(q, i, c);
+        Pk<T> rv;
+#pragma unroll
+        for (int k = 0; k < Pk<T>::n; ++k) {
+            rv.v[k] = bv.v[k] - qv.v[k];
+            if (k < c) v[0] += (double)rv.v[k] * (double)rv.v[k];
+        }
+        stc(r, i, c, rv);
+    });
     double tot[1];
     if (reduce_last<1>(v, partials, counter, tot) && threadIdx.x == 0) s->rr = tot[0];
 }
@@ -410,15 +513,16 @@ __global__ void sub_kernel(const T *__restrict__ b, const T *__restrict__ q, T *
 template <typename T>
 __global__ void copy_kernel(T *__restrict__ dst, const T *__restrict__ src, long long N)
 {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
-        dst[t] = src[t];
+    vloop<T>(N, al16(dst) && al16(src), [&](long long i, int c) { stc(dst, i, c, ldc(src, i, c)); });
 }
 
 template <typename T>
 __global__ void zero_kernel(T *__restrict__ dst, long long N)
 {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
-        dst[t] = 0;
+    Pk<T> zv;
+#pragma unroll
+    for (int k = 0; k < Pk<T>::n; ++k) zv.v[k] = T(0);
+    vloop<T>(N, al16(dst), [&](long long i, int c) { stc(dst, i, c, zv); });
 }
 
 // FP32 sweep right-hand side r32 = r64 / scale.
@@ -434,6 +538,30 @@ __global__ void refine_update_kernel(double *__restrict__ x, const float *__rest
 {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
         x[t] += scale * (double)d[t];
+}
+
+// Scale of an FP64 vector carried through an FP32 preconditioner: the input
+// is divided by ||r|| (rr = r.r of the current residual) on the way down and
+// the output multiplied by it on the way up, so FP32's exponent range holds
+// any residual size. 1 when rr is zero or not finite.
+__device__ __forceinline__ double pc_scale(const DevScalars *s)
+{
+    const double rr = s->rr;
+    return (rr > 0.0 && rr < 1e300) ? sqrt(rr) : 1.0;
+}
+
+__global__ void to_fp32_kernel(const double *__restrict__ r, float *__restrict__ r32, long long N, const DevScalars *s)
+{
+    const double inv = 1.0 / pc_scale(s);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        r32[t] = (float)(r[t] * inv);
+}
+
+__global__ void from_fp32_kernel(const float *__restrict__ z32, double *__restrict__ z, long long N, const DevScalars *s)
+{
+    const double sc = pc_scale(s);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
+        z[t] = sc * (double)z32[t];
 }
 
 // ------------------------------------------------------------ exact FEM inverse (fast diagonalisation)
@@ -608,21 +736,26 @@ __global__ void tri_bwd_fix(T *__restrict__ W, const T *__restrict__ C, int nx, 
 // Interior block of r (m x n grid, x fastest) into a zero-padded nxp x nyp
 // column-major matrix (rows = x), and back: GEMM-friendly leading dimensions.
 // Launched on a 2-D grid (blockIdx.y strides over the columns b) so no index
-// division is needed.
-template <typename T>
-__global__ void fd_gather_kernel(const T *__restrict__ r, T *__restrict__ U, int m, int nx, int ny, int nxp, int nyp)
+// division is needed. With sc (FP64 vectors, FP32 transform) the gather
+// divides by pc_scale and the scatter multiplies by it.
+template <typename T, typename V>
+__global__ void fd_gather_kernel(const V *__restrict__ r, T *__restrict__ U, int m, int nx, int ny, int nxp, int nyp,
+                                 const DevScalars *sc)
 {
+    const double inv = sc ? 1.0 / pc_scale(sc) : 1.0;
     for (int b = blockIdx.y; b < nyp; b += gridDim.y)
         for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nxp; a += gridDim.x * blockDim.x)
-            U[(size_t)b * nxp + a] = (a < nx && b < ny) ? r[(size_t)(b + 1) * m + (a + 1)] : T(0);
+            U[(size_t)b * nxp + a] = (a < nx && b < ny) ? (T)((double)r[(size_t)(b + 1) * m + (a + 1)] * inv) : T(0);
 }
 
-template <typename T>
-__global__ void fd_scatter_kernel(const T *__restrict__ Z, T *__restrict__ z, int m, int nx, int ny, int nxp)
+template <typename T, typename V>
+__global__ void fd_scatter_kernel(const T *__restrict__ Z, V *__restrict__ z, int m, int nx, int ny, int nxp,
+                                  const DevScalars *sc)
 {
+    const double f = sc ? pc_scale(sc) : 1.0;
     for (int b = blockIdx.y; b < ny; b += gridDim.y)
         for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nx; a += gridDim.x * blockDim.x)
-            z[(size_t)(b + 1) * m + (a + 1)] = Z[(size_t)b * nxp + a];
+            z[(size_t)(b + 1) * m + (a + 1)] = (V)(f * (double)Z[(size_t)b * nxp + a]);
 }
 
 static dim3 grid2d(int nrows, int ncols)
@@ -686,7 +819,8 @@ struct PrecState {
     bool ready = false;
     T *kd = nullptr, *ko = nullptr, *md = nullptr, *mo = nullptr;
     T *ld = nullptr, *lo = nullptr, *nd = nullptr, *no = nullptr;
-    T *x = nullptr, *r = nullptr, *z = nullptr, *zo = nullptr, *p = nullptr, *q = nullptr, *b = nullptr;
+    T *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr, *b = nullptr;
+    T *tz = nullptr;   // FP32 state: the preconditioner's output inside an FP64 (IGA_MIXED_PC) solve
     T *sc = nullptr;   // kappa-scaled preconditioner input
     T *iz = nullptr, *ir = nullptr, *ip = nullptr, *iq = nullptr;
     cudaGraphExec_t chunk = nullptr;
@@ -699,7 +833,7 @@ struct PrecState {
     // device-side PCG loop: a CUDA graph whose conditional WHILE node runs one
     // iteration per pass (built for one preconditioner / kappa-scaling choice)
     cudaGraphExec_t loop = nullptr;
-    int loop_pc = -1, loop_scaled = -1;
+    int loop_pc = -1, loop_scaled = -1, loop_prec = -1;
     bool loop_failed = false;   // the loop graph could not be instantiated: host-driven loop
     FemCoef<T> coef() const
     {
@@ -817,7 +951,7 @@ static int alloc_prec(PrecState<T> &ps, const iga_plan *pl, const SolverState &S
     if ((st = up(&ps.kd, kd)) || (st = up(&ps.ko, ko)) || (st = up(&ps.md, md)) || (st = up(&ps.mo, mo)) ||
         (st = up(&ps.ld, ld)) || (st = up(&ps.lo, lo)) || (st = up(&ps.nd, nd)) || (st = up(&ps.no, no)))
         return st;
-    for (T **v : {&ps.x, &ps.r, &ps.z, &ps.zo, &ps.p, &ps.q, &ps.b, &ps.sc, &ps.iz, &ps.ir, &ps.ip, &ps.iq})
+    for (T **v : {&ps.x, &ps.r, &ps.z, &ps.tz, &ps.p, &ps.q, &ps.b, &ps.sc, &ps.iz, &ps.ir, &ps.ip, &ps.iq})
         SOLVE_TRY(cudaMalloc((void **)v, sizeof(T) * N));
     ps.ready = true;
     return IGA_OK;
@@ -853,7 +987,7 @@ static int ensure_state(iga_plan *pl, SolverState **out)
 template <typename T>
 static void free_prec(PrecState<T> &ps)
 {
-    T *bufs[] = {ps.kd, ps.ko, ps.md, ps.mo, ps.ld, ps.lo, ps.nd, ps.no, ps.x, ps.r, ps.z, ps.zo, ps.p,
+    T *bufs[] = {ps.kd, ps.ko, ps.md, ps.mo, ps.ld, ps.lo, ps.nd, ps.no, ps.x, ps.r, ps.z, ps.tz, ps.p,
                  ps.q, ps.b, ps.sc, ps.iz, ps.ir, ps.ip, ps.iq, ps.Vx, ps.lx, ps.W1, ps.W2, ps.Dv, ps.Cf};
     for (T *v : bufs)
         if (v) cudaFree(v);
@@ -1066,18 +1200,20 @@ static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperati
 // lx[a] My + Ky: W = Vx^T R, row a of W solved along y, Z = Vx W. Two GEMMs
 // and three recurrence passes (the fast diagonalisation in both directions
 // would take four GEMMs).
-template <typename T>
-static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const T *r, T *z)
+// V is the vectors' type; an FP32 transform of FP64 vectors (T = float,
+// V = double) passes sc, the device scalars whose rr scales the data.
+template <typename T, typename V>
+static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const V *r, V *z, const DevScalars *sc)
 {
     const int m = pl->m, n = pl->n, nx = m - 2, ny = n - 2;
-    boundary_copy_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(z, r, m, n);
+    boundary_copy_kernel<V><<<kRedBlocks, kThreads, 0, S->stream>>>(z, r, m, n);
     if (nx <= 0 || ny <= 0) return IGA_OK;
     const int nxp = ps.nxp, nyp = ps.nyp;
     const int nseg = (ny + kSeg - 1) / kSeg;
     const int tb = (int)std::min<long long>(((long long)nx * nseg + kThreads - 1) / kThreads, 8 * 148);
     const int ta = (int)std::min<long long>(((long long)nx * 32 + kThreads - 1) / kThreads, 8 * 148);
     cublasSetStream(S->blas, S->stream);
-    fd_gather_kernel<T><<<grid2d(nxp, nyp), 256, 0, S->stream>>>(r, ps.W2, m, nx, ny, nxp, nyp);
+    fd_gather_kernel<T, V><<<grid2d(nxp, nyp), 256, 0, S->stream>>>(r, ps.W2, m, nx, ny, nxp, nyp, sc);
     cublasStatus_t e = gemm(S->blas, CUBLAS_OP_T, CUBLAS_OP_N, nxp, nyp, nxp, ps.Vx, nxp, ps.W2, nxp, ps.W1, nxp);
     if (e == CUBLAS_STATUS_SUCCESS) {
         tri_fwd_local<T><<<tb, kThreads, 0, S->stream>>>(ps.W1, ps.Dv, ps.lx, ps.ycoef, nx, ny, nxp, nseg, ps.seg_end,
@@ -1093,7 +1229,7 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
         set_error("cuBLAS GEMM failed in the FEM preconditioner");
         return IGA_ERR_CUDA;
     }
-    fd_scatter_kernel<T><<<grid2d(nx, ny), 256, 0, S->stream>>>(ps.W2, z, m, nx, ny, nxp);
+    fd_scatter_kernel<T, V><<<grid2d(nx, ny), 256, 0, S->stream>>>(ps.W2, z, m, nx, ny, nxp, sc);
     return IGA_OK;
 }
 
@@ -1118,6 +1254,35 @@ static int update_kscale(const iga_plan *pl, SolverState *S)
     return IGA_OK;
 }
 
+// z = M^-1 r for FP64 vectors with the preconditioner evaluated in FP32
+// (IGA_MIXED_PC): the input divided by ||r|| into FP32 (inside the
+// transform's gather for the exact inverse), the FP32 preconditioner, the
+// output multiplied back into FP64. The outer flexible PCG absorbs the FP32
+// (TF32 GEMM) rounding of the preconditioner.
+static int pc_apply_fp32(const iga_plan *pl, SolverState *S, const iga_solve_opts &o, const double *r, double *z,
+                         double pc_rtol, int64_t &pc_iters)
+{
+    const long long N = pl->nfunc;
+    PrecState<float> &f = S->f;
+    int st;
+    const double *rin = r;
+    if (pl->kappa_dev) {
+        if ((st = update_kscale(pl, S))) return st;
+        mul_kernel<double><<<kRedBlocks, kThreads, 0, S->stream>>>(S->d.sc, r, S->ks64, N);
+        rin = S->d.sc;
+    }
+    if (o.pc == IGA_PC_FEM_EXACT) {
+        if ((st = fd_upload(f, pl, S))) return st;
+        if ((st = fd_apply<float, double>(f, pl, S, rin, z, S->s))) return st;
+    } else {
+        to_fp32_kernel<<<kRedBlocks, kThreads, 0, S->stream>>>(rin, f.sc, N, S->s);
+        if ((st = pc_apply_core<float>(f, pl, S, o, f.sc, f.tz, pc_rtol, pc_iters))) return st;
+        from_fp32_kernel<<<kRedBlocks, kThreads, 0, S->stream>>>(f.tz, z, N, S->s);
+    }
+    if (pl->kappa_dev) mul_kernel<double><<<kRedBlocks, kThreads, 0, S->stream>>>(z, z, S->ks64, N);
+    return IGA_OK;
+}
+
 // z = M^-1 r for the configured preconditioner; with a coefficient kappa,
 // z = S M^-1 (S r) with the local scaling S.
 template <typename T>
@@ -1125,6 +1290,9 @@ static int pc_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
                     double pc_rtol, int64_t &pc_iters)
 {
     const long long N = pl->nfunc;
+    if constexpr (std::is_same<T, double>::value) {
+        if (o.precision == IGA_MIXED_PC && o.pc != IGA_PC_NONE) return pc_apply_fp32(pl, S, o, r, z, pc_rtol, pc_iters);
+    }
     if (o.pc == IGA_PC_NONE || !pl->kappa_dev) return pc_apply_core(ps, pl, S, o, r, z, pc_rtol, pc_iters);
     int st;
     if ((st = update_kscale(pl, S))) return st;
@@ -1147,7 +1315,7 @@ static int pc_apply_core(PrecState<T> &ps, const iga_plan *pl, SolverState *S, c
     int st;
     if (o.pc == IGA_PC_FEM_EXACT) {
         if ((st = fd_upload(ps, pl, S))) return st;
-        return fd_apply(ps, pl, S, r, z);
+        return fd_apply<T, T>(ps, pl, S, r, z, nullptr);
     }
     if ((st = inner_chunk_graph(ps, pl, S))) return st;
     InnerCG<T> a = inner_of(ps, pl, S);
@@ -1204,28 +1372,28 @@ static int pcg(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_solve_o
     for (int it = 0; it < o.max_it; ++it) {
         if ((st = iga_apply_internal_sb(pl, prec, ps.p, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY))) return st;
         pcg_pq_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.q, N, S->s, S->partials, S->counter);
-        pcg_xr_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(x, ps.r, ps.p, ps.q, N, S->s, S->partials, S->counter);
+        pcg_xr_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(x, ps.r, ps.p, ps.q, ps.z, N, S->s, S->partials,
+                                                         S->counter);
         ++its;
         if ((st = sync_scalars(S))) return st;
         if (S->h->breakdown) return IGA_ERR_BREAKDOWN;
         if (!std::isfinite(S->h->rr)) return IGA_ERR_NONFINITE;
         if (std::sqrt(S->h->rr) <= rtol * bnorm) return IGA_OK;
-        std::swap(ps.z, ps.zo);
         if ((st = pc_apply(ps, pl, S, o, ps.r, ps.z, pc_rtol, pc_iters))) return st;
-        pcg_beta_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, ps.zo, N, S->s, S->partials, S->counter);
+        pcg_beta_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, N, S->s, S->partials, S->counter);
         pcg_p_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.z, N, S->s, 0);
     }
     return IGA_ERR_NOT_CONVERGED;
 }
 
 // Builds the device-side loop for the current preconditioner choice: body =
-// q = K p; alpha; x += alpha p, r -= alpha q (+ loop condition); z_old = z;
+// q = K p; alpha; x += alpha p, r -= alpha q, r.z_old (+ loop condition);
 // z = M^-1 r; beta; p = z + beta p, on the fixed buffers of ps.
 template <typename T>
 static int build_loop(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_solve_opts &o, int prec)
 {
     const int scaled = pl->kappa_dev ? 1 : 0;
-    if (ps.loop_pc == o.pc && ps.loop_scaled == scaled && (ps.loop || ps.loop_failed))
+    if (ps.loop_pc == o.pc && ps.loop_scaled == scaled && ps.loop_prec == o.precision && (ps.loop || ps.loop_failed))
         return ps.loop ? IGA_OK : IGA_ERR_UNSUPPORTED;
     if (ps.loop) {
         cudaGraphExecDestroy(ps.loop);
@@ -1250,13 +1418,12 @@ static int build_loop(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_
     int st = iga_apply_internal_sb(pl, prec, ps.p, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY);
     if (!st) {
         pcg_pq_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.q, N, S->s, S->partials, S->counter);
-        pcg_xr_cond_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.x, ps.r, ps.p, ps.q, N, S->s, S->partials, S->counter,
-                                                             h);
-        copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.zo, ps.z, N);
+        pcg_xr_cond_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.x, ps.r, ps.p, ps.q, ps.z, N, S->s, S->partials,
+                                                             S->counter, h);
         st = pc_apply(ps, pl, S, o, ps.r, ps.z, o.pc_rtol, dummy);
     }
     if (!st) {
-        pcg_beta_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, ps.zo, N, S->s, S->partials, S->counter);
+        pcg_beta_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, N, S->s, S->partials, S->counter);
         pcg_p_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.z, N, S->s, 0);
     }
     cudaGraph_t captured = body;
@@ -1278,6 +1445,7 @@ static int build_loop(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_
         ps.loop = nullptr;
         ps.loop_pc = o.pc;
         ps.loop_scaled = scaled;
+        ps.loop_prec = o.precision;
         ps.loop_failed = true;
         return IGA_ERR_UNSUPPORTED;
     }
@@ -1285,6 +1453,7 @@ static int build_loop(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_
     ps.loop_failed = false;
     ps.loop_pc = o.pc;
     ps.loop_scaled = scaled;
+    ps.loop_prec = o.precision;
     return IGA_OK;
 }
 
@@ -1297,7 +1466,11 @@ static int pcg_graph(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_s
     const cudaStream_t s = S->stream;
     int st;
     if ((st = update_kscale(pl, S))) return st;
-    if (o.pc == IGA_PC_FEM_EXACT && (st = fd_upload(ps, pl, S))) return st;
+    if (o.pc == IGA_PC_FEM_EXACT) {   // device set-up before any capture
+        if (std::is_same<T, double>::value && o.precision == IGA_MIXED_PC) st = fd_upload(S->f, pl, S);
+        else st = fd_upload(ps, pl, S);
+        if (st) return st;
+    }
     if (b != ps.b) copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.b, b, N);
     if (x != ps.x) copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.x, x, N);
     if ((st = iga_apply_internal_sb(pl, prec, ps.x, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY))) return st;
@@ -1460,6 +1633,10 @@ int iga_solve(iga_plan *pl, const double *b, double *x, const iga_solve_opts *o_
         set_error("iga_solve needs the FP64 operator (plan precision IGA_FP64 or IGA_MIXED)");
         return IGA_ERR_ARG;
     }
+    if (o.precision != IGA_FP64 && o.precision != IGA_MIXED && o.precision != IGA_MIXED_PC) {
+        set_error("iga_solve precision is IGA_FP64, IGA_MIXED or IGA_MIXED_PC");
+        return IGA_ERR_ARG;
+    }
     if (o.precision == IGA_MIXED && !pl->op32.ready) {
         set_error("IGA_MIXED solves need a plan created with precision IGA_MIXED");
         return IGA_ERR_ARG;
@@ -1491,8 +1668,9 @@ int iga_solve(iga_plan *pl, const double *b, double *x, const iga_solve_opts *o_
     const double bnorm = std::sqrt(S->h->bb);
     double rel = bnorm > 0 ? std::sqrt(S->h->rr) / bnorm : 0.0;
     int result = IGA_OK;
-    if (o.precision == IGA_FP64) {
+    if (o.precision != IGA_MIXED) {
         if ((st = alloc_prec(S->d, pl, *S))) return st;
+        if (o.precision == IGA_MIXED_PC && o.pc != IGA_PC_NONE && (st = alloc_prec(S->f, pl, *S))) return st;
         // Restart from the true residual until it meets rtol (recurrence drift).
         for (int restart = 0; restart < 4 && rel > o.rtol; ++restart) {
             st = o.pc == IGA_PC_FEM_CG
@@ -1590,7 +1768,7 @@ int iga_spectrum_estimate(iga_plan *pl, int pc, int steps, uint64_t seed, double
         const double rz_old = S->h->rz;
         if ((st = iga_apply_internal_sb(pl, IGA_FP64, ps.p, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY))) return st;
         pcg_pq_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.q, N, S->s, S->partials, S->counter);
-        pcg_xr_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.x, ps.r, ps.p, ps.q, N, S->s, S->partials,
+        pcg_xr_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.x, ps.r, ps.p, ps.q, ps.z, N, S->s, S->partials,
                                                              S->counter);
         if ((st = pc_apply(ps, pl, S, o, ps.r, ps.z, o.pc_rtol, pcits))) return st;
         dot_kernel<double><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, N, &S->s->rz, S->partials, S->counter);

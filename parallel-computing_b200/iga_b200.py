@@ -23,6 +23,7 @@ VP = ctypes.c_void_p
 
 IGA_OK = 0
 FP64, FP32, MIXED = 0, 1, 2
+MIXED_PC = 3   # solve precision: FP64 PCG with the preconditioner in FP32
 GEOM_PRECOMPUTED, GEOM_ON_THE_FLY = 0, 1
 SIGN_REFERENCE, SIGN_SPD = -1, 1
 BC_REFERENCE, BC_IDENTITY, BC_NONE = 0, 1, 2

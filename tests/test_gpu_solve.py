@@ -129,6 +129,34 @@ def test_mixed_precision_refinement(torch_cuda, ib, orc, pc):
     assert np.linalg.norm(r) / np.linalg.norm(b) < 2e-10
 
 
+@pytest.mark.parametrize("pc,kappa", [(1, False), (2, False), (2, True)])
+def test_fp64_pcg_with_fp32_preconditioner(torch_cuda, ib, orc, pc, kappa):
+    """IGA_MIXED_PC: FP64 flexible PCG whose preconditioner runs in FP32 reaches the
+    FP64 tolerance on an FP64-only plan and agrees with the FP64 solve."""
+    torch = torch_cuda
+    mesh = distorted(ib.unit_square(3, 40, 33))
+    plan = ib.Plan(mesh)
+    if kappa:
+        nq = 40 * 33 * 16
+        k = 1.0 + 0.5 * splitmix_uniform(5, -1, 1, nq)
+        plan.set_kappa(torch.from_numpy(k).cuda())
+    b = splitmix_normal(2, plan.nfunc)
+    b[boundary_mask(43, 36)] = 0.0
+    bd = torch.from_numpy(b).cuda()
+    x64, xpc = torch.zeros_like(bd), torch.zeros_like(bd)
+    s64 = plan.solve(bd, x64, pc=pc, rtol=1e-10, pc_rtol=1e-6)
+    spc = plan.solve(bd, xpc, pc=pc, rtol=1e-10, pc_rtol=1e-6, precision=ib.MIXED_PC)
+    assert s64.status == 0 and spc.status == 0 and spc.relres <= 1e-10 and spc.sweeps == 0
+    assert spc.iterations <= 2 * s64.iterations + 5
+    assert rel(xpc.cpu().numpy(), x64.cpu().numpy()) < 1e-7
+    if not kappa:
+        r = b - orc.apply_mf(mesh, xpc.cpu().numpy(), sign=1.0, bc=1)
+        assert np.linalg.norm(r) / np.linalg.norm(b) < 2e-10
+    # an unknown solve precision is an argument error
+    with pytest.raises(ib.IgaError):
+        plan.solve(bd, xpc, precision=7)
+
+
 def test_solver_failure_modes(torch_cuda, ib):
     torch = torch_cuda
     plan = ib.Plan(ib.unit_square(2, 16))
