@@ -34,6 +34,7 @@ struct DevScalars {
     double alpha, beta, rz, rzo, rr, rr0, tol2, bb; // outer PCG (rzo = r_new . z_old)
     double ialpha, ibeta, irz, irr, itol2;          // inner FEM-CG
     int done, breakdown, idone, iiters, ibreak, imax;
+    int err;                                        // a bounded wait in a kernel gave up
     int it, maxit;                                  // outer PCG in a device-side loop
 };
 
@@ -566,201 +567,189 @@ __global__ void from_fp32_kernel(const float *__restrict__ z32, double *__restri
 
 // ------------------------------------------------------------ exact FEM inverse (fast diagonalisation)
 // ---- tridiagonal solves along y of the x-diagonalised FEM system
-// For every x mode a < nx: (lx[a] My + Ky) t = w, w = row a of W (column-major,
-// element (a, b) at a + b ld), in place. The LDL^T factors are precomputed per
-// mode (Dv = 1 / pivot, C = the upper factor's off-diagonal), so
-//   forward  y_b = Dv_b w_b + beta_b y_{b-1},  beta_b = -e_{b-1} Dv_b,
-//   backward x_b = y_b + gamma_b x_{b+1},      gamma_b = -C_b,
-// with e_b = lx[a] Mo_b + Ko_b (yc = Kd | Ko | Md | Mo of the free y nodes).
-// Each first-order recurrence is solved in
-// segments of kSeg rows in parallel: a local pass (zero carry-in) that also
-// records the segment's end value and coefficient product, a sequential pass
-// over the few segments for the carries, and a fix-up pass adding the carry
-// times the running coefficient product. nx * segments threads per pass.
-constexpr int kSeg = 16;
+// For every x mode a < nx: (lx[a] My + Ky) t = w, w = column a of the nyp x nxp
+// matrix Wt (y contiguous: element (b, a) at b + a nyp), in place. The LDL^T
+// factors are precomputed per mode in the same layout: Lf_b = e_{b-1} / d_{b-1}
+// (the unit lower factor's subdiagonal, Lf_0 = 0) and Dv_b = 1 / d_b, so
+//   forward  u_b = w_b - Lf_b u_{b-1},       v_b = Dv_b u_b,
+//   backward x_b = v_b - Lf_{b+1} x_{b+1}    (no term past the last free row).
+// One warp per mode: lane l owns rows [l s, l s + s) with s odd, so that the
+// lanes' shared-memory accesses fall in distinct banks. Each recurrence is
+// composed per lane into an affine map c -> E + P c, the maps are combined by
+// a warp shuffle scan, and each lane then runs its rows from its carry-in.
+// Arithmetic in T. STAGED: the mode's column and factors are brought into
+// shared memory by the bulk-copy engine and the result is written back with
+// 16-byte stores; else (columns too long for shared memory) the kernel works
+// on them in place.
+constexpr int kTriMaxWarps = 16;
 
-// The segment's rows b0 .. b0 + len - 1 of column a: loads first (a full
-// segment issues all of them before the dependent chain starts).
-template <typename T, int NV>
-__device__ __forceinline__ void seg_load(const T *const (&src)[NV], size_t a, int b0, int len, int ld,
-                                         double (&v)[NV][kSeg])
+// inclusive scan of affine maps over lanes, lane order (forward) or reverse lane order
+template <typename R>
+__device__ __forceinline__ void affine_scan(R &E, R &P, int lane, bool reverse)
 {
 #pragma unroll
-    for (int k = 0; k < kSeg; ++k)
-#pragma unroll
-        for (int j = 0; j < NV; ++j) v[j][k] = k < len ? (double)src[j][a + (size_t)(b0 + k) * ld] : 0.0;
-}
-
-// forward local pass: y (zero carry-in) into W; segment end value and product
-template <typename T>
-__global__ void tri_fwd_local(T *__restrict__ W, const T *__restrict__ Dv, const T *__restrict__ lx,
-                              const double *__restrict__ yc, int nx, int ny, int ld, int nseg,
-                              double *__restrict__ end, double *__restrict__ prod)
-{
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nx * nseg;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(t % nx), sg = (int)(t / nx);
-        const double lam = (double)lx[a];
-        const int b0 = sg * kSeg, len = min(ny - b0, kSeg);
-        double v[2][kSeg];
-        const T *src[2] = {W, Dv};
-        seg_load<T, 2>(src, a, b0, len, ld, v);
-        double y = 0.0, pr = 1.0;
-#pragma unroll
-        for (int k = 0; k < kSeg; ++k) {
-            if (k < len) {
-                const int b = b0 + k;
-                const double beta = b == 0 ? 0.0 : -(lam * yc[3 * ny + b - 1] + yc[ny + b - 1]) * v[1][k];
-                y = v[1][k] * v[0][k] + beta * y;
-                pr *= beta;
-                W[a + (size_t)b * ld] = (T)y;
-            }
-        }
-        end[t] = y;
-        prod[t] = pr;
-    }
-}
-
-// carries: cin[a, s] = the recurrence's value entering segment s (forward or,
-// with reverse = 1, backward over the segments). Segment s maps a carry-in c
-// to its carry-out end_s + prod_s c; one warp per mode a composes these affine
-// maps: each lane folds a run of consecutive segments, a warp shuffle scan
-// combines the runs, and each lane then walks its run with its carry-in.
-__global__ void tri_carry(const double *__restrict__ end, const double *__restrict__ prod, double *__restrict__ cin,
-                          int nx, int nseg, int reverse)
-{
-    const int lane = threadIdx.x & 31;
-    const int per = (nseg + 31) / 32;   // segments per lane
-    for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < nx;
-         w += ((long long)gridDim.x * blockDim.x) >> 5) {
-        const int a = (int)w;
-        // this lane's run, in recurrence order: k = lane * per .. lane * per + per - 1
-        double E = 0.0, Pm = 1.0;   // composed map of the run: c -> E + Pm c
-        for (int j = 0; j < per; ++j) {
-            const int k = lane * per + j;
-            if (k < nseg) {
-                const int sg = reverse ? nseg - 1 - k : k;
-                const double e = end[a + (size_t)sg * nx], p = prod[a + (size_t)sg * nx];
-                E = e + p * E;
-                Pm = p * Pm;
-            }
-        }
-        // exclusive scan over lanes of the composed maps (earlier lanes apply first)
-        double sE = E, sP = Pm;
-        for (int o = 1; o < 32; o <<= 1) {
-            const double pe = __shfl_up_sync(0xffffffffu, sE, o), pp = __shfl_up_sync(0xffffffffu, sP, o);
-            if (lane >= o) {
-                sE = sE + sP * pe;
-                sP = sP * pp;
-            }
-        }
-        double c = __shfl_up_sync(0xffffffffu, sE, 1);   // value entering this lane's run
-        if (lane == 0) c = 0.0;
-        for (int j = 0; j < per; ++j) {
-            const int k = lane * per + j;
-            if (k < nseg) {
-                const int sg = reverse ? nseg - 1 - k : k;
-                cin[a + (size_t)sg * nx] = c;
-                c = end[a + (size_t)sg * nx] + prod[a + (size_t)sg * nx] * c;
-            }
+    for (int o = 1; o < 32; o <<= 1) {
+        const R pe = reverse ? __shfl_down_sync(0xffffffffu, E, o) : __shfl_up_sync(0xffffffffu, E, o);
+        const R pp = reverse ? __shfl_down_sync(0xffffffffu, P, o) : __shfl_up_sync(0xffffffffu, P, o);
+        if (reverse ? lane + o < 32 : lane >= o) {
+            E = E + P * pe;
+            P = P * pp;
         }
     }
 }
 
-// forward fix-up, then the backward local pass over the same segment
-template <typename T>
-__global__ void tri_fwd_fix_bwd_local(T *__restrict__ W, const T *__restrict__ Dv, const T *__restrict__ C,
-                                      const T *__restrict__ lx, const double *__restrict__ yc, int nx, int ny, int ld,
-                                      int nseg, const double *__restrict__ cin, double *__restrict__ end,
-                                      double *__restrict__ prod)
+template <typename T, bool STAGED>
+__global__ void __launch_bounds__(kTriMaxWarps * 32)
+fd_tri_kernel(T *__restrict__ W, const T *__restrict__ Lf, const T *__restrict__ Dv, int nx, int ny, int nyp, int seg,
+              DevScalars *sc)
 {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nx * nseg;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(t % nx), sg = (int)(t / nx);
-        const double lam = (double)lx[a];
-        const int b0 = sg * kSeg, len = min(ny - b0, kSeg);
-        double v[3][kSeg];
-        const T *src[3] = {W, Dv, C};
-        seg_load<T, 3>(src, a, b0, len, ld, v);
-        const double c0 = cin[t];
-        double r = 1.0;
-#pragma unroll
-        for (int k = 0; k < kSeg; ++k) {
-            if (k < len) {
-                const int b = b0 + k;
-                const double beta = b == 0 ? 0.0 : -(lam * yc[3 * ny + b - 1] + yc[ny + b - 1]) * v[1][k];
-                r *= beta;
-                v[0][k] += r * c0;
+    extern __shared__ __align__(16) unsigned char tri_smem[];
+    __shared__ uint64_t bar[kTriMaxWarps];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    T *wb = nullptr, *lb = nullptr, *db = nullptr;
+    if constexpr (STAGED) {
+        wb = reinterpret_cast<T *>(tri_smem) + (size_t)wid * 3 * nyp;
+        lb = wb + nyp;
+        db = lb + nyp;
+        if (lane == 0) mbar_init(&bar[wid], 1);
+        fence_mbar_init();
+        __syncwarp();
+    }
+    uint32_t phase = 0;
+    const int b0 = lane * seg, b1 = min(b0 + seg, ny);
+    for (int a = blockIdx.x * nw + wid; a < nx; a += gridDim.x * nw) {
+        T *wg = W + (size_t)a * nyp;
+        const T *lg = Lf + (size_t)a * nyp, *dg = Dv + (size_t)a * nyp;
+        T *wp;
+        const T *lp, *dp;
+        if constexpr (STAGED) {
+            if (lane == 0) {
+                const uint32_t bytes = (uint32_t)nyp * (uint32_t)sizeof(T);
+                mbar_arrive_expect_tx(&bar[wid], 3u * bytes);
+                bulk_g2s(wb, wg, bytes, &bar[wid]);
+                bulk_g2s(lb, lg, bytes, &bar[wid]);
+                bulk_g2s(db, dg, bytes, &bar[wid]);
             }
-        }
-        double x = 0.0, q = 1.0;
-#pragma unroll
-        for (int k = kSeg - 1; k >= 0; --k) {
-            if (k < len) {
-                const double gamma = -v[2][k];
-                x = v[0][k] + gamma * x;
-                q *= gamma;
-                W[a + (size_t)(b0 + k) * ld] = (T)x;
+            if (!mbar_wait_bounded(&bar[wid], phase)) {
+                if (lane == 0) sc->err = 1;
+                mbar_wait_bounded(&bar[wid], phase);   // let the copies land before leaving
+                return;
             }
+            phase ^= 1u;
+            wp = wb;
+            lp = lb;
+            dp = db;
+        } else {
+            wp = wg;
+            lp = lg;
+            dp = dg;
         }
-        end[t] = x;
-        prod[t] = q;
+        // forward: this lane's map, the scan, then its rows from the carry-in
+        T E = 0, P = 1;
+#pragma unroll 4
+        for (int b = b0; b < b1; ++b) {
+            const T l = lp[b];
+            E = wp[b] - l * E;
+            P = -l * P;
+        }
+        affine_scan(E, P, lane, false);
+        T u = __shfl_up_sync(0xffffffffu, E, 1);
+        if (lane == 0) u = 0;
+#pragma unroll 4
+        for (int b = b0; b < b1; ++b) {
+            u = wp[b] - lp[b] * u;
+            wp[b] = u * dp[b];
+        }
+        __syncwarp();
+        // backward over the same rows, lanes in reverse order
+        E = 0;
+        P = 1;
+#pragma unroll 4
+        for (int b = b1 - 1; b >= b0; --b) {
+            const T l = b + 1 < ny ? lp[b + 1] : T(0);
+            E = wp[b] - l * E;
+            P = -l * P;
+        }
+        affine_scan(E, P, lane, true);
+        T x = __shfl_down_sync(0xffffffffu, E, 1);
+        if (lane == 31) x = 0;
+#pragma unroll 4
+        for (int b = b1 - 1; b >= b0; --b) {
+            const T l = b + 1 < ny ? lp[b + 1] : T(0);
+            x = wp[b] - l * x;
+            wp[b] = x;
+        }
+        if constexpr (STAGED) {
+            __syncwarp();
+            const int nv = (int)((size_t)nyp * sizeof(T) / 16);
+            const uint4 *src = reinterpret_cast<const uint4 *>(wb);
+            uint4 *dst = reinterpret_cast<uint4 *>(wg);
+            for (int i = lane; i < nv; i += 32) dst[i] = src[i];
+            fence_proxy_async_smem();   // order these generic accesses before the next bulk copy
+            __syncwarp();
+        }
     }
 }
 
-// backward fix-up
-template <typename T>
-__global__ void tri_bwd_fix(T *__restrict__ W, const T *__restrict__ C, int nx, int ny, int ld, int nseg,
-                            const double *__restrict__ cin)
+// Launch shape of fd_tri_kernel for columns of nyp entries of T: warps per
+// CTA of the staged kernel (0 when a column and its factors do not fit in
+// shared memory) and its dynamic shared memory.
+static int tri_warps(int nyp, size_t esz, size_t &smem)
 {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)nx * nseg;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int a = (int)(t % nx), sg = (int)(t / nx);
-        const double c0 = cin[t];
-        if (c0 == 0.0) continue;
-        const int b0 = sg * kSeg, len = min(ny - b0, kSeg);
-        double v[2][kSeg];
-        const T *src[2] = {W, C};
-        seg_load<T, 2>(src, a, b0, len, ld, v);
-        double r = 1.0;
-#pragma unroll
-        for (int k = kSeg - 1; k >= 0; --k) {
-            if (k < len) {
-                r *= -v[1][k];
-                W[a + (size_t)(b0 + k) * ld] = (T)(v[0][k] + r * c0);
-            }
-        }
-    }
+    const size_t per_warp = 3 * (size_t)nyp * esz, cap = 226 * 1024;   // leaves room for the static barriers
+    const int w = (int)std::min<size_t>(kTriMaxWarps, cap / per_warp);
+    smem = (size_t)w * per_warp;
+    return w;
 }
 
 // Interior block of r (m x n grid, x fastest) into a zero-padded nxp x nyp
 // column-major matrix (rows = x), and back: GEMM-friendly leading dimensions.
-// Launched on a 2-D grid (blockIdx.y strides over the columns b) so no index
-// division is needed. With sc (FP64 vectors, FP32 transform) the gather
-// divides by pc_scale and the scatter multiplies by it.
+// Each thread moves 16 bytes of the padded matrix (nxp is a multiple of 64);
+// blockIdx.y strides over the columns b, so no index division is needed. With
+// sc (FP64 vectors, FP32 transform) the gather divides by pc_scale and the
+// scatter multiplies by it.
 template <typename T, typename V>
 __global__ void fd_gather_kernel(const V *__restrict__ r, T *__restrict__ U, int m, int nx, int ny, int nxp, int nyp,
                                  const DevScalars *sc)
 {
+    constexpr int VN = Pk<T>::n;
     const double inv = sc ? 1.0 / pc_scale(sc) : 1.0;
+    const int nv = nxp / VN;
     for (int b = blockIdx.y; b < nyp; b += gridDim.y)
-        for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nxp; a += gridDim.x * blockDim.x)
-            U[(size_t)b * nxp + a] = (a < nx && b < ny) ? (T)((double)r[(size_t)(b + 1) * m + (a + 1)] * inv) : T(0);
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += gridDim.x * blockDim.x) {
+            Pk<T> o;
+#pragma unroll
+            for (int c = 0; c < VN; ++c) {
+                const int a = k * VN + c;
+                o.v[c] = (a < nx && b < ny) ? (T)((double)r[(size_t)(b + 1) * m + (a + 1)] * inv) : T(0);
+            }
+            stp(U, (long long)b * nxp + (long long)k * VN, o);
+        }
 }
 
 template <typename T, typename V>
 __global__ void fd_scatter_kernel(const T *__restrict__ Z, V *__restrict__ z, int m, int nx, int ny, int nxp,
                                   const DevScalars *sc)
 {
+    constexpr int VN = Pk<T>::n;
     const double f = sc ? pc_scale(sc) : 1.0;
+    const int nv = (nx + VN - 1) / VN;
     for (int b = blockIdx.y; b < ny; b += gridDim.y)
-        for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < nx; a += gridDim.x * blockDim.x)
-            z[(size_t)(b + 1) * m + (a + 1)] = (V)(f * (double)Z[(size_t)b * nxp + a]);
+        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += gridDim.x * blockDim.x) {
+            const Pk<T> zv = ldp(Z, (long long)b * nxp + (long long)k * VN);
+#pragma unroll
+            for (int c = 0; c < VN; ++c) {
+                const int a = k * VN + c;
+                if (a < nx) z[(size_t)(b + 1) * m + (a + 1)] = (V)(f * (double)zv.v[c]);
+            }
+        }
 }
 
-static dim3 grid2d(int nrows, int ncols)
+// 2-D launch of the gather / scatter: 128-thread blocks over the 16-byte
+// groups of a column, one block row per column (at most 65535).
+static dim3 grid2d(int ngroups, int ncols)
 {
-    return dim3((unsigned)std::max(1, std::min((nrows + 255) / 256, 8)), (unsigned)std::max(1, std::min(ncols, 1024)));
+    return dim3((unsigned)std::max(1, (ngroups + 127) / 128), (unsigned)std::max(1, std::min(ncols, 65535)));
 }
 
 // z = r on the boundary ring (identity rows of K_fem).
@@ -826,10 +815,11 @@ struct PrecState {
     cudaGraphExec_t chunk = nullptr;
     // exact FEM inverse: x eigenvectors (column-major), eigenvalues, two work
     // matrices, and the LDL^T factors of the y systems of every x mode
-    T *Vx = nullptr, *lx = nullptr, *W1 = nullptr, *W2 = nullptr, *Dv = nullptr, *Cf = nullptr;
-    double *ycoef = nullptr;                             // y pencil: Kd | Ko | Md | Mo
-    double *seg_end = nullptr, *seg_prod = nullptr, *seg_cin = nullptr;
+    T *Vx = nullptr, *lx = nullptr, *W1 = nullptr, *W2 = nullptr, *Dv = nullptr;
+    T *Lf = nullptr;   // LDL^T unit lower factor's subdiagonal per x mode (layout of Dv)
     int nxp = 0, nyp = 0;   // transform sizes padded to multiples of 64
+    int tri_w = 0;          // warps per CTA of the staged tridiagonal kernel (0: in place)
+    size_t tri_smem = 0;
     // device-side PCG loop: a CUDA graph whose conditional WHILE node runs one
     // iteration per pass (built for one preconditioner / kappa-scaling choice)
     cudaGraphExec_t loop = nullptr;
@@ -851,7 +841,7 @@ struct SolverState {
     void *blas_ws = nullptr;   // fixed cuBLAS workspace (no allocation inside graph capture)
     bool fd_host = false;
     std::vector<double> lamx, Vx;             // host x eigenpairs (built once)
-    std::vector<double> Dv, Cf;               // host LDL^T factors of the y systems, [b][a]
+    std::vector<double> Dv, Lf;               // host LDL^T factors of the y systems, [a][b]
     double *ks64 = nullptr;                   // kappa scaling of the preconditioner
     float *ks32 = nullptr;
     int kappa_version = 0;
@@ -988,11 +978,8 @@ template <typename T>
 static void free_prec(PrecState<T> &ps)
 {
     T *bufs[] = {ps.kd, ps.ko, ps.md, ps.mo, ps.ld, ps.lo, ps.nd, ps.no, ps.x, ps.r, ps.z, ps.tz, ps.p,
-                 ps.q, ps.b, ps.sc, ps.iz, ps.ir, ps.ip, ps.iq, ps.Vx, ps.lx, ps.W1, ps.W2, ps.Dv, ps.Cf};
+                 ps.q, ps.b, ps.sc, ps.iz, ps.ir, ps.ip, ps.iq, ps.Vx, ps.lx, ps.W1, ps.W2, ps.Dv, ps.Lf};
     for (T *v : bufs)
-        if (v) cudaFree(v);
-    double *dbufs[] = {ps.ycoef, ps.seg_end, ps.seg_prod, ps.seg_cin};
-    for (double *v : dbufs)
         if (v) cudaFree(v);
     if (ps.chunk) cudaGraphExecDestroy(ps.chunk);
     if (ps.loop) cudaGraphExecDestroy(ps.loop);
@@ -1090,15 +1077,15 @@ static int fd_setup(PrecState<double> &, const iga_plan *pl, SolverState *S)
     interior_pencil(S->gy, Kd, Ko, Md, Mo);
     const int ny = (int)Kd.size();
     S->Dv.assign((size_t)nx * ny, 0.0);
-    S->Cf.assign((size_t)nx * ny, 0.0);
+    S->Lf.assign((size_t)nx * ny, 0.0);
     for (int a = 0; a < nx; ++a) {
         const double lam = S->lamx[a];
-        double cprev = 0.0, eprev = 0.0;
+        double cprev = 0.0, eprev = 0.0;   // e_{b-1} / d_{b-1} and e_{b-1}
         for (int b = 0; b < ny; ++b) {
             const double den = lam * Md[b] + Kd[b] - eprev * cprev;
             const double e = b + 1 < ny ? lam * Mo[b] + Ko[b] : 0.0;
-            S->Dv[(size_t)b * nx + a] = 1.0 / den;
-            S->Cf[(size_t)b * nx + a] = e / den;
+            S->Dv[(size_t)a * ny + b] = 1.0 / den;
+            S->Lf[(size_t)a * ny + b] = cprev;
             cprev = e / den;
             eprev = e;
         }
@@ -1133,32 +1120,23 @@ static int fd_upload(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
         SOLVE_TRY(cudaMemcpy(*dst, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
         return IGA_OK;
     };
-    // y factors padded like W: element (a, b) at a + b nxp
+    // y factors in the layout of Wt: element (b, a) at b + a nyp
     auto up_fac = [&](T **dst, const std::vector<double> &F) -> int {
         std::vector<T> h((size_t)nxp * nyp, T(0));
-        for (int b = 0; b < ny; ++b)
-            for (int a = 0; a < nx; ++a) h[(size_t)b * nxp + a] = (T)F[(size_t)b * nx + a];
+        for (int a = 0; a < nx; ++a)
+            for (int b = 0; b < ny; ++b) h[(size_t)a * nyp + b] = (T)F[(size_t)a * ny + b];
         SOLVE_TRY(cudaMalloc((void **)dst, sizeof(T) * h.size()));
         SOLVE_TRY(cudaMemcpy(*dst, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
         return IGA_OK;
     };
     int st;
     if ((st = up_mat(&ps.Vx, S->Vx, nx, nxp)) || (st = up_vec(&ps.lx, S->lamx, nxp)) || (st = up_fac(&ps.Dv, S->Dv)) ||
-        (st = up_fac(&ps.Cf, S->Cf)))
+        (st = up_fac(&ps.Lf, S->Lf)))
         return st;
-    {
-        std::vector<double> Kd, Ko, Md, Mo;
-        interior_pencil(S->gy, Kd, Ko, Md, Mo);
-        std::vector<double> yc;
-        const std::vector<double> *parts[] = {&Kd, &Ko, &Md, &Mo};
-        for (const std::vector<double> *v : parts) yc.insert(yc.end(), v->begin(), v->end());
-        SOLVE_TRY(cudaMalloc((void **)&ps.ycoef, sizeof(double) * yc.size()));
-        SOLVE_TRY(cudaMemcpy(ps.ycoef, yc.data(), sizeof(double) * yc.size(), cudaMemcpyHostToDevice));
-        const size_t nseg = (size_t)(ny + kSeg - 1) / kSeg;
-        SOLVE_TRY(cudaMalloc((void **)&ps.seg_end, sizeof(double) * nx * nseg));
-        SOLVE_TRY(cudaMalloc((void **)&ps.seg_prod, sizeof(double) * nx * nseg));
-        SOLVE_TRY(cudaMalloc((void **)&ps.seg_cin, sizeof(double) * nx * nseg));
-    }
+    ps.tri_w = tri_warps(nyp, sizeof(T), ps.tri_smem);
+    if (ps.tri_w)
+        SOLVE_TRY(cudaFuncSetAttribute(fd_tri_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ps.tri_smem));
     SOLVE_TRY(cudaMalloc((void **)&ps.W1, sizeof(T) * (size_t)nxp * nyp));
     SOLVE_TRY(cudaMalloc((void **)&ps.W2, sizeof(T) * (size_t)nxp * nyp));
     if (!S->blas) {
@@ -1197,9 +1175,10 @@ static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperati
 // zero-padded to multiples of 64 so the GEMMs run with aligned leading
 // dimensions). With Kx V = Mx V diag(lx) (V Mx-orthonormal), K_fem =
 // Kx (x) My + Mx (x) Ky becomes, mode by mode in x, the tridiagonal y system
-// lx[a] My + Ky: W = Vx^T R, row a of W solved along y, Z = Vx W. Two GEMMs
-// and three recurrence passes (the fast diagonalisation in both directions
-// would take four GEMMs).
+// lx[a] My + Ky: Wt = R^T Vx (so that each mode's y values are contiguous),
+// column a of Wt solved along y, Z = Vx Wt^T. Two GEMMs and one pass of
+// tridiagonal solves (the fast diagonalisation in both directions would take
+// four GEMMs).
 // V is the vectors' type; an FP32 transform of FP64 vectors (T = float,
 // V = double) passes sc, the device scalars whose rr scales the data.
 template <typename T, typename V>
@@ -1209,27 +1188,27 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
     boundary_copy_kernel<V><<<kRedBlocks, kThreads, 0, S->stream>>>(z, r, m, n);
     if (nx <= 0 || ny <= 0) return IGA_OK;
     const int nxp = ps.nxp, nyp = ps.nyp;
-    const int nseg = (ny + kSeg - 1) / kSeg;
-    const int tb = (int)std::min<long long>(((long long)nx * nseg + kThreads - 1) / kThreads, 8 * 148);
-    const int ta = (int)std::min<long long>(((long long)nx * 32 + kThreads - 1) / kThreads, 8 * 148);
+    int seg = (ny + 31) / 32;
+    seg |= 1;   // odd: conflict-free shared-memory rows
     cublasSetStream(S->blas, S->stream);
-    fd_gather_kernel<T, V><<<grid2d(nxp, nyp), 256, 0, S->stream>>>(r, ps.W2, m, nx, ny, nxp, nyp, sc);
-    cublasStatus_t e = gemm(S->blas, CUBLAS_OP_T, CUBLAS_OP_N, nxp, nyp, nxp, ps.Vx, nxp, ps.W2, nxp, ps.W1, nxp);
+    constexpr int VN = Pk<T>::n;
+    fd_gather_kernel<T, V><<<grid2d(nxp / VN, nyp), 128, 0, S->stream>>>(r, ps.W2, m, nx, ny, nxp, nyp, sc);
+    cublasStatus_t e = gemm(S->blas, CUBLAS_OP_T, CUBLAS_OP_N, nyp, nxp, nxp, ps.W2, nxp, ps.Vx, nxp, ps.W1, nyp);
     if (e == CUBLAS_STATUS_SUCCESS) {
-        tri_fwd_local<T><<<tb, kThreads, 0, S->stream>>>(ps.W1, ps.Dv, ps.lx, ps.ycoef, nx, ny, nxp, nseg, ps.seg_end,
-                                                         ps.seg_prod);
-        tri_carry<<<ta, kThreads, 0, S->stream>>>(ps.seg_end, ps.seg_prod, ps.seg_cin, nx, nseg, 0);
-        tri_fwd_fix_bwd_local<T><<<tb, kThreads, 0, S->stream>>>(ps.W1, ps.Dv, ps.Cf, ps.lx, ps.ycoef, nx, ny, nxp,
-                                                                 nseg, ps.seg_cin, ps.seg_end, ps.seg_prod);
-        tri_carry<<<ta, kThreads, 0, S->stream>>>(ps.seg_end, ps.seg_prod, ps.seg_cin, nx, nseg, 1);
-        tri_bwd_fix<T><<<tb, kThreads, 0, S->stream>>>(ps.W1, ps.Cf, nx, ny, nxp, nseg, ps.seg_cin);
-        e = gemm(S->blas, CUBLAS_OP_N, CUBLAS_OP_N, nxp, nyp, nxp, ps.Vx, nxp, ps.W1, nxp, ps.W2, nxp);
+        if (ps.tri_w) {
+            const int grid = std::min((nx + ps.tri_w - 1) / ps.tri_w, 148);
+            fd_tri_kernel<T, true><<<grid, ps.tri_w * 32, ps.tri_smem, S->stream>>>(ps.W1, ps.Lf, ps.Dv, nx, ny, nyp,
+                                                                                 seg, S->s);
+        } else {
+            fd_tri_kernel<T, false><<<(nx + 7) / 8, 256, 0, S->stream>>>(ps.W1, ps.Lf, ps.Dv, nx, ny, nyp, seg, S->s);
+        }
+        e = gemm(S->blas, CUBLAS_OP_N, CUBLAS_OP_T, nxp, nyp, nxp, ps.Vx, nxp, ps.W1, nyp, ps.W2, nxp);
     }
     if (e != CUBLAS_STATUS_SUCCESS) {
         set_error("cuBLAS GEMM failed in the FEM preconditioner");
         return IGA_ERR_CUDA;
     }
-    fd_scatter_kernel<T, V><<<grid2d(nx, ny), 256, 0, S->stream>>>(ps.W2, z, m, nx, ny, nxp, sc);
+    fd_scatter_kernel<T, V><<<grid2d((nx + VN - 1) / VN, ny), 128, 0, S->stream>>>(ps.W2, z, m, nx, ny, nxp, sc);
     return IGA_OK;
 }
 
@@ -1653,6 +1632,7 @@ int iga_solve(iga_plan *pl, const double *b, double *x, const iga_solve_opts *o_
     SOLVE_TRY(cudaStreamWaitEvent(S->stream, ev, 0));
     const long long N = pl->nfunc;
     iga_solve_stats stt{};
+    SOLVE_TRY(cudaMemsetAsync(&S->s->err, 0, sizeof(int), S->stream));
     if (!o.x0_nonzero) zero_kernel<double><<<kRedBlocks, kThreads, 0, S->stream>>>(x, N);
     if ((st = true_residual(pl, S, b, x))) return st;
     if (!std::isfinite(S->h->bb) || !std::isfinite(S->h->rr)) {
@@ -1718,6 +1698,10 @@ int iga_solve(iga_plan *pl, const double *b, double *x, const iga_solve_opts *o_
     SOLVE_TRY(cudaStreamSynchronize(S->stream));
     cudaEventDestroy(ev);
     stt.relres = rel;
+    if (S->h->err) {   // host copy current as of the last true residual
+        set_error("a bounded device wait gave up in the preconditioner");
+        result = IGA_ERR_TIMEOUT;
+    }
     if (result == IGA_OK && !(rel <= o.rtol)) result = IGA_ERR_NOT_CONVERGED;
     stt.status = result;
     stt.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -14,6 +14,15 @@ a forward update sends owned values to the peers that hold them as ghosts, a
 reverse update sends ghost contributions back, and each owner adds them peer
 by peer in ascending rank order (a fixed summation order: bitwise
 reproducible across runs).
+
+The Krylov loop over those ranks (DistPCG) is the reference's KSPSolve across
+MPI ranks (matrix_free/iteration_number_fempc_mf.cpp:193-233 and the
+no-preconditioner driver beside it): flexible PCG on the owned entries, one
+MatMult and two all-reductions per iteration ([p.q], then [r.r, r.z, r.z_old]
+in one call). The preconditioner is either none or BlockFemPC, each rank's
+exact FEM inverse on its own block (a block-Jacobi preconditioner that needs
+no communication); the reference's inner CG on the distributed FEM matrix is
+not reproduced across ranks.
 """
 import numpy as np
 
@@ -137,3 +146,123 @@ def emulate_partitioned_matmult(parts, x_global, local_apply=None):
             y_owned.index_add_(0, torch.as_tensor(send_idx[q], device=dev), contrib)
         y_global[p.owned_offset:p.owned_offset + p.nowned] = y_owned
     return y_global
+
+
+def pcg_solve(matmult, pc, allreduce, b, x, rtol=1e-10, max_it=10000):
+    """Flexible (Polak-Ribiere) PCG on K x = b from x = 0 over vectors that may
+    be one rank's owned entries. matmult(v, out) computes out = K v (all ranks
+    together); pc(r, out) applies the preconditioner (None: identity);
+    allreduce(t) sums a small FP64 tensor over the ranks in place. Stops when
+    ||r|| <= rtol ||b|| (recurrence residual). Returns (iterations, ||r|| / ||b||)."""
+    import torch
+    x.zero_()
+    r = b.clone()
+    z = torch.empty_like(b)
+    q = torch.empty_like(b)
+
+    def precond(v, out):
+        if pc is None:
+            out.copy_(v)
+        else:
+            pc(v, out)
+    precond(r, z)
+    d = torch.stack([torch.dot(b, b), torch.dot(r, r), torch.dot(r, z)])
+    allreduce(d)
+    bb, rr, rz = (float(v) for v in d)
+    bnorm = bb ** 0.5
+    if bnorm == 0.0:
+        return 0, 0.0
+    p = z.clone()
+    it = 0
+    while rr ** 0.5 > rtol * bnorm and it < max_it:
+        matmult(p, q)
+        d = torch.dot(p, q).reshape(1)
+        allreduce(d)
+        pq = float(d[0])
+        if not pq > 0.0:
+            raise FloatingPointError("PCG breakdown: p.Kp <= 0")
+        alpha = rz / pq
+        x.add_(p, alpha=alpha)
+        r.add_(q, alpha=-alpha)
+        rzo = torch.dot(r, z)
+        precond(r, z)
+        d = torch.stack([torch.dot(r, r), torch.dot(r, z), rzo])
+        allreduce(d)
+        rr, rz_new, rzo = (float(v) for v in d)
+        it += 1
+        beta = (rz_new - rzo) / rz
+        rz = rz_new
+        p.mul_(beta).add_(z)
+    return it, rr ** 0.5 / bnorm
+
+
+class BlockFemPC:
+    """z_owned = [Kf^-1 (r_owned placed in the part's block, zero elsewhere)]_owned:
+    Kf is the FEM matrix of the part's sub-patch (identity rows on the block's
+    outer ring), inverted exactly by the device's fast-diagonalisation
+    preconditioner (iga_pc_apply with IGA_PC_FEM_EXACT on a plan of the
+    sub-patch). The owned entries of an interior part lie inside its block, so
+    every rank applies a principal submatrix of an SPD inverse: the global
+    preconditioner is block diagonal and SPD. local_solve(r_block, z_block)
+    replaces the device solve (the host tests use a CPU stand-in)."""
+
+    def __init__(self, part, device, local_solve=None):
+        import torch
+        nl = part.nowned + part.nghost
+        pos = np.empty(nl, dtype=np.int64)
+        pos[part.block_to_local] = np.arange(nl)
+        self.pos = torch.as_tensor(pos[:part.nowned], device=device)
+        self.rb = torch.zeros(nl, dtype=torch.float64, device=device)
+        self.zb = torch.empty_like(self.rb)
+        self.plan = None
+        if local_solve is None:
+            import iga_b200 as ib
+            dev = torch.device(device)
+            self.plan = ib.Plan(part.mesh(), device=dev.index or 0)
+            plan = self.plan
+            local_solve = lambda rb, zb: plan.pc_apply(rb, zb, pc=ib.PC_FEM_EXACT)  # noqa: E731
+        self.local_solve = local_solve
+
+    def __call__(self, r_owned, z_owned):
+        self.rb.zero_()
+        self.rb[self.pos] = r_owned
+        self.local_solve(self.rb, self.zb)
+        z_owned.copy_(self.zb[self.pos])
+
+
+class DistPCG:
+    """Flexible PCG on K x = b over the ranks of a partitioned mesh: op is a
+    DistPartOperator whose part was built with sign SPD and bc IDENTITY (so K
+    is SPD with identity Dirichlet rows; b must be zero on them); pc is None
+    or a callable on owned vectors (BlockFemPC)."""
+
+    def __init__(self, op, pc=None):
+        self.op, self.pc = op, pc
+
+    def solve(self, b_owned, x_owned, rtol=1e-10, max_it=10000):
+        dist = self.op.dist
+
+        def allreduce(t):
+            dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return pcg_solve(self.op.matmult, self.pc, allreduce, b_owned, x_owned, rtol, max_it)
+
+
+def emulate_partitioned_pcg(parts, b_global, pcs=None, local_apply=None, rtol=1e-10, max_it=10000):
+    """DistPCG with every part in one process (one GPU, or the CPU): the same
+    operator, preconditioner and loop on the concatenated owned vectors
+    (partition numbering). pcs: None or one preconditioner per part. Returns
+    (x_global, iterations, relres)."""
+    import torch
+    off = [p.owned_offset for p in parts] + [parts[-1].owned_offset + parts[-1].nowned]
+
+    def matmult(v, out):
+        out.copy_(emulate_partitioned_matmult(parts, v, local_apply=local_apply))
+
+    pc = None
+    if pcs is not None:
+        def pc(v, out):
+            for k, f in enumerate(pcs):
+                f(v[off[k]:off[k + 1]], out[off[k]:off[k + 1]])
+    x = torch.zeros_like(b_global)
+    its, rel = pcg_solve(matmult, pc, lambda t: None, b_global, x, rtol, max_it)
+    return x, its, rel

@@ -197,6 +197,31 @@ def test_preconditioner_inverts_fem_matrix(torch_cuda, ib, pc, prec, tol):
     assert float((y - r).norm() / r.norm()) < tol
 
 
+@pytest.mark.parametrize("ney", [9700, 19400, 95])
+def test_exact_pc_long_columns(torch_cuda, ib, ney):
+    """Tall meshes: the y tridiagonal solves of the exact inverse run on columns of
+    ney + 1 free rows, past the shared-memory staging limits (9642 FP64 / 19285 FP32
+    entries) where the kernel works in place, and just below a lane-segment edge.
+    FP64: K_fem z = r. FP32: z close to the FP64 z (a residual check means nothing
+    in FP32 here: the y systems' condition numbers reach ney^2)."""
+    torch = torch_cuda
+    mesh = ib.unit_square(2, 9, ney)
+    plan = ib.Plan(mesh, precision=ib.MIXED)
+    m, n = 11, ney + 2
+    r = torch.from_numpy(splitmix_uniform(9, -1, 1, plan.nfunc)).cuda()
+    r[torch.from_numpy(boundary_mask(m, n)).cuda()] = 0
+    z = torch.empty_like(r)
+    plan.pc_apply(r, z, pc=ib.PC_FEM_EXACT, precision=ib.FP64)
+    y = torch.empty_like(r)
+    plan.fem_apply(z, y, precision=ib.FP64)
+    r32 = r.float()
+    z32 = torch.empty_like(r32)
+    plan.pc_apply(r32, z32, pc=ib.PC_FEM_EXACT, precision=ib.FP32)
+    torch.cuda.synchronize()
+    assert float((y - r).norm() / r.norm()) < 1e-9
+    assert float((z32.double() - z).norm() / z.norm()) < 1e-2
+
+
 @pytest.mark.parametrize("p,ne", [(2, 16), (3, 40), (4, 24), (3, 510), (3, 512), (5, 20)])
 def test_exact_pc_solve_matches_inner_cg_solve(torch_cuda, ib, orc, p, ne):
     torch = torch_cuda

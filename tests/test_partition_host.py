@@ -11,7 +11,8 @@ import socket
 import numpy as np
 import pytest
 
-from iga_testlib import PARTITIONS, load_binding, partition_numbering, read_info, splitmix_uniform, unit_square_mesh
+from iga_testlib import (PARTITIONS, load_binding, partition_numbering, read_info, splitmix_uniform, unit_square_mesh,
+                         write_partition_files)
 
 CASES = ["p3_9x7_2", "p2_10x12_3", "p4_8x11_2"]
 
@@ -145,7 +146,7 @@ def _gloo_rank(rank, world, port, name, out_dir):
 
 
 @pytest.mark.parametrize("name", ["p3_9x7_2", "p2_10x12_3"])
-def test_gloo_ranks_match_reference(name, tmp_path):
+def test_gloo_ranks_match_reference(ib, name, tmp_path):
     """One process per part over gloo: forward ghost update, local element
     loop, reverse add; the assembled owned rows equal the reference's
     partitioned MatMult."""
@@ -200,3 +201,171 @@ def test_test_writer_reproduces_reference_files(orc, name, tmp_path):
     for f in sorted(os.listdir(d)):
         if f.endswith(".txt"):
             assert filecmp.cmp(os.path.join(d, f), os.path.join(tmp_path, f), shallow=False), f
+
+
+def local_oracle_spd(orc, part, sub, x_local):
+    """The part's SPD MatMult with identity Dirichlet rows on the CPU: the
+    local form of K (sign +1) with Dirichlet columns dropped, owned Dirichlet
+    rows y = x, ghost Dirichlet rows 0 (the owner supplies the identity)."""
+    xb = x_local[part.block_to_local].copy()
+    xb[part.local_id[part.block_to_local] < 0] = 0.0
+    yb = orc.apply_mf(sub, xb, sign=1.0, bc=2)
+    y = np.empty_like(x_local)
+    y[part.block_to_local] = yb
+    dirl = part.local_id < 0
+    y[dirl] = 0.0
+    own = np.nonzero(dirl[:part.nowned])[0]
+    y[own] = x_local[own]
+    return y
+
+
+def net_lengths(sub):
+    """Mean polyline lengths of the control net's rows (x) and columns (y)."""
+    m, n = sub["nex"] + sub["p"], sub["ney"] + sub["q"]
+    cp = sub["CP"].reshape(n, m, 2)
+    lx = np.linalg.norm(np.diff(cp, axis=1), axis=2).sum(axis=1).mean()
+    ly = np.linalg.norm(np.diff(cp, axis=0), axis=2).sum(axis=0).mean()
+    return lx, ly
+
+
+def block_fem_solver(orc, sub):
+    """CPU stand-in of the device's exact FEM inverse on a sub-patch: the
+    dense FEM matrix of the sub-patch's FEM grid (identity boundary rows)."""
+    lx, ly = net_lengths(sub)
+    gx = orc.fem_nodes(sub["p"], sub["nex"], lx)
+    gy = orc.fem_nodes(sub["q"], sub["ney"], ly)
+    import scipy.linalg
+    import torch
+    nb = len(gx) * len(gy)
+    lu = scipy.linalg.lu_factor(np.stack([orc.fem_matvec(gx, gy, e) for e in np.eye(nb)], axis=1))
+    return lambda rb, zb: zb.copy_(torch.from_numpy(scipy.linalg.lu_solve(lu, rb.numpy())))
+
+
+def serial_solution(orc, name, seed=21):
+    """b (natural numbering, zero on the boundary) and the oracle's FP64 PCG
+    solution of the SPD system, both in the partition numbering."""
+    d, p, q, nex, ney, P = case_info(name)
+    mesh = unit_square_mesh(orc, p, q, nex, ney)
+    m, n = nex + p, ney + q
+    b = splitmix_uniform(seed, -1.0, 1.0, m * n)
+    mask = np.zeros((n, m), bool)
+    mask[0, :] = mask[-1, :] = mask[:, 0] = mask[:, -1] = True
+    b[mask.ravel()] = 0.0
+    x, it, rr = orc.pcg(mesh, b, rtol=1e-13, maxit=2000)
+    new = partition_numbering(p, q, nex, ney, P)
+    bp, xp = np.empty_like(b), np.empty_like(x)
+    bp[new], xp[new] = b, x
+    return bp, xp
+
+
+def _gloo_pcg_rank(rank, world, port, name, pc, out_dir):
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from iga_testlib import Oracle
+        import iga_b200 as ib
+        from iga_dist import BlockFemPC, DistPartOperator, DistPCG
+        orc = Oracle()
+        d = os.path.join(PARTITIONS, name)
+        part = ib.Part(os.path.join(d, "info.txt"), ib.partition_filename(os.path.join(d, "part"), rank), rank)
+        sub = part.mesh()
+        op = DistPartOperator(part, dist, "cpu",
+                              local_apply=lambda xl, yl: yl.copy_(torch.from_numpy(
+                                  local_oracle_spd(orc, part, sub, xl.numpy()))))
+        prec = BlockFemPC(part, "cpu", local_solve=block_fem_solver(orc, sub)) if pc else None
+        bp = np.load(os.path.join(out_dir, "b.npy"))
+        b_owned = torch.from_numpy(bp[part.owned_offset:part.owned_offset + part.nowned].copy())
+        x_owned = torch.empty_like(b_owned)
+        its, rel = DistPCG(op, prec).solve(b_owned, x_owned, rtol=1e-11)
+        np.save(os.path.join(out_dir, f"x{rank}.npy"), x_owned.numpy())
+        np.save(os.path.join(out_dir, f"its{rank}.npy"), np.array([its, rel]))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("name,pc", [("p3_9x7_2", False), ("p3_9x7_2", True), ("p4_8x11_2", True)])
+def test_gloo_distributed_pcg_matches_serial_solve(ib, orc, name, pc, tmp_path):
+    """The multi-rank Krylov loop (one process per part, gloo): ghost updates,
+    local element loops, two all-reductions per iteration, optional block FEM
+    preconditioner; the assembled solution equals the serial FP64 solve and
+    every rank agrees on the iteration count."""
+    import torch.multiprocessing as mp
+    d, p, q, nex, ney, P = case_info(name)
+    world = P * P
+    bp, xp = serial_solution(orc, name)
+    np.save(os.path.join(tmp_path, "b.npy"), bp)
+    mp.start_processes(_gloo_pcg_rank, args=(world, _free_port(), name, pc, str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    x = np.concatenate([np.load(os.path.join(tmp_path, f"x{r}.npy")) for r in range(world)])
+    its = [np.load(os.path.join(tmp_path, f"its{r}.npy")) for r in range(world)]
+    assert len({int(i[0]) for i in its}) == 1 and its[0][1] <= 1e-11
+    assert np.linalg.norm(x - xp) / np.linalg.norm(xp) < 1e-9
+
+
+def owned_inside_blocks(parts, nfx, nfy):
+    """Every owned entry lies off its block's outer ring unless it is on the
+    global boundary (so each block preconditioner is an SPD principal block)."""
+    for pt in parts:
+        i = pt.info
+        pos = np.empty(pt.nowned + pt.nghost, dtype=np.int64)
+        pos[pt.block_to_local] = np.arange(len(pos))
+        bi, bj = pos[:pt.nowned] % i.block_m, pos[:pt.nowned] // i.block_m
+        ring = (bi == 0) | (bj == 0) | (bi == i.block_m - 1) | (bj == i.block_n - 1)
+        gi, gj = i.elem_x0 + bi, i.elem_y0 + bj
+        glob = (gi == 0) | (gj == 0) | (gi == nfx - 1) | (gj == nfy - 1)
+        if np.any(ring & ~glob):
+            return False
+    return True
+
+
+def emulated_solves(orc, parts, bp):
+    import torch
+    from iga_dist import BlockFemPC, emulate_partitioned_pcg
+    subs = [pt.mesh() for pt in parts]
+
+    def apply(part, xl, yl):
+        yl.copy_(torch.from_numpy(local_oracle_spd(orc, part, subs[part.rank], xl.numpy())))
+    x0, it0, _ = emulate_partitioned_pcg(parts, torch.from_numpy(bp), local_apply=apply, rtol=1e-11)
+    pcs = [BlockFemPC(pt, "cpu", local_solve=block_fem_solver(orc, sub)) for pt, sub in zip(parts, subs)]
+    x1, it1, _ = emulate_partitioned_pcg(parts, torch.from_numpy(bp), pcs=pcs, local_apply=apply, rtol=1e-11)
+    return x0.numpy(), it0, x1.numpy(), it1
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_emulated_pcg_matches_serial_solve(ib, orc, name):
+    """All parts in one process, the same loop, with and without the block
+    FEM preconditioner: the serial FP64 solution."""
+    d, p, q, nex, ney, P = case_info(name)
+    parts = open_parts(ib, name)
+    assert owned_inside_blocks(parts, nex + p, ney + q)
+    bp, xp = serial_solution(orc, name)
+    x0, it0, x1, it1 = emulated_solves(orc, parts, bp)
+    for x in (x0, x1):
+        assert np.linalg.norm(x - xp) / np.linalg.norm(xp) < 1e-9
+
+
+def test_emulated_pcg_block_pc_reduces_iterations(ib, orc, tmp_path):
+    """p = 2, 64 x 64 elements on 2 x 2 parts (files written by the test
+    restatement of the reference preprocessor): the block FEM preconditioner
+    roughly halves the iteration count of the unpreconditioned loop."""
+    p, ne, P = 2, 64, 2
+    mesh = unit_square_mesh(orc, p, p, ne, ne)
+    write_partition_files(mesh, P, str(tmp_path))
+    parts = [ib.Part(os.path.join(tmp_path, "info.txt"), ib.partition_filename(os.path.join(tmp_path, "part"), r), r)
+             for r in range(P * P)]
+    m = ne + p
+    assert owned_inside_blocks(parts, m, m)
+    b = splitmix_uniform(21, -1.0, 1.0, m * m)
+    mask = np.zeros((m, m), bool)
+    mask[0, :] = mask[-1, :] = mask[:, 0] = mask[:, -1] = True
+    b[mask.ravel()] = 0.0
+    new = partition_numbering(p, p, ne, ne, P)
+    bp = np.empty_like(b)
+    bp[new] = b
+    x0, it0, x1, it1 = emulated_solves(orc, parts, bp)
+    assert np.linalg.norm(x1 - x0) / np.linalg.norm(x0) < 1e-9
+    assert it1 < 0.6 * it0
