@@ -220,8 +220,10 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
     stream = torch.cuda.current_stream()
     # FP32 sweeps to 1e-3 (the library default): shallow sweeps restart the
     # Krylov space before FP32 rounding slows it down
+    # fp64_pcg_fp32_pc: FP64 PCG whose preconditioner runs in FP32 (IGA_MIXED_PC)
     for name, kw in (("fp64", dict(pc=ib.PC_FEM_EXACT)),
-                     ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED, sweep_rtol=1e-3))):
+                     ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED, sweep_rtol=1e-3)),
+                     ("fp64_pcg_fp32_pc", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED_PC))):
         x = torch.zeros_like(b)
         plan.solve(b, x, **kw)   # warm-up: eigen-decomposition, cuBLAS, allocations
         times, st = [], None
@@ -248,7 +250,8 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
     ann = {"problem": "quarter annulus r in [1,2] (NURBS, p=4), 1024x1024, u = sin(pi r) sin(2 theta), rtol 1e-10"}
     # FP32 sweeps to 1e-2 (measured fastest here: five shallow sweeps)
     for name, kw in (("fp64", dict(pc=ib.PC_FEM_EXACT)),
-                     ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED, sweep_rtol=1e-2))):
+                     ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED, sweep_rtol=1e-2)),
+                     ("fp64_pcg_fp32_pc", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED_PC))):
         x = torch.zeros_like(ba)
         pa.solve(ba, x, **kw)
         times = []
@@ -393,7 +396,7 @@ def time_adjoint(ib, torch, stream, barrier, max_over_ranks):
     plan.close()
     torch.cuda.empty_cache()
     return {"problem": "p=3 512x512, kappa = exp(GRF), J = |u - u_obs|^2 / 2",
-            "seconds_forward_adjoint_gradient": t, "J": float(J), "quadrature_points": int(kappa.numel()),
+            "seconds_forward_adjoint_gradient": t, "J": float(J.detach()), "quadrature_points": int(kappa.numel()),
             "fd_directional_rel_err": errs}
 
 
