@@ -108,17 +108,30 @@ __host__ __device__ constexpr int apply_max_threads()
                           : (P <= 2 ? (GEOM ? 384 : 512) : P == 3 ? (GEOM ? 320 : 384) : 256);
 }
 
-// One CTA: column strip gx, strips gyb*W .. gyb*W+W-1 of that column (one per warp).
+// Whether a lane keeps its x-direction tables in registers (16 values at
+// p = 3) or reads them from shared memory: registers except where they are
+// the scarcer resource (FP64 on-the-fly geometry, FP64 p >= 4). In registers
+// they save 32 shared loads per element row of a p=3 FP64 strip (12 instead
+// of 13 warps per SM: 1.12x faster), and the warps of a CTA need not share a
+// column strip.
+template <int P, typename T, int GEOM>
+__host__ __device__ constexpr bool apply_txreg()
+{
+    return sizeof(T) == 4 || (GEOM == 0 && P <= 3);
+}
+
+// One warp: strip (gx, gy). With tables in shared memory the CTA's warps
+// share the column strip gx (the CTA copies its tables once).
 template <int P, typename T, int GEOM, int NST>
 __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__restrict__ x, T *__restrict__ y, const int gx,
-                                           const int gyb)
+                                           const int gy)
 {
     using S = ApplyShape<P, T>;
     constexpr int NB = S::NB, NQ = S::NQ, QH = S::QH;
+    constexpr bool TXREG = apply_txreg<P, T, GEOM>();
     const StripGrid &g = a.g;
     const int lane = threadIdx.x, w = threadIdx.y, W = blockDim.y;
     const int c = lane >> 1, h = lane & 1;
-    const int gy = gyb * W + w;
 
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
@@ -136,12 +149,12 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     T *yr = reinterpret_cast<T *>(smem + off) + (size_t)w * S::XR * S::TYW;     // y tables of upcoming rows
     uint64_t *wbar = bars + w * NST;
 
-    {   // x tables of this column strip, shared by the CTA's warps
+    if constexpr (!TXREG) {   // x tables of this column strip, shared by the CTA's warps
         const T *src = a.tabX + (size_t)gx * S::TABX;
         for (int i = threadIdx.y * 32 + lane; i < S::TABX; i += 32 * W) tabXs[i] = src[i];
+        __syncthreads();
     }
-    __syncthreads();
-    if (gy >= g.NSY) return;
+    if (gx >= g.NSX || gy >= g.NSY) return;
     const int ex0 = kSW * gx, ey0 = g.TY * gy;
     const int nsteps = min(g.TY, g.ney - ey0);
     if (nsteps <= 0) return;
@@ -182,20 +195,18 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     constexpr int D = S::XR - 1;
     for (int k = 0; k < D; ++k) fetch_row(k);
 
-    // This lane's x-direction tables: tabXs[kind][j][il][lane]; held in
-    // registers (16 values at p = 3) except where registers are the scarcer
-    // resource (FP64 on-the-fly geometry, FP64 p >= 4), where they are read
-    // from shared memory. In registers they save 32 shared loads per element
-    // row of a p=3 FP64 strip (12 instead of 13 warps per SM: 1.12x faster).
-    constexpr bool TXREG = sizeof(T) == 4 || (GEOM == 0 && P <= 3);
+    // This lane's x-direction tables, [kind][j][il][lane] per column strip
+    // (apply_txreg: registers, loaded straight from global memory; else the
+    // CTA's shared copy).
     T txr[TXREG ? 2 : 1][TXREG ? QH : 1][TXREG ? NB : 1];
     if constexpr (TXREG) {
+        const T *src = a.tabX + (size_t)gx * S::TABX;
 #pragma unroll
         for (int kind = 0; kind < 2; ++kind)
 #pragma unroll
             for (int j = 0; j < QH; ++j)
 #pragma unroll
-                for (int il = 0; il < NB; ++il) txr[kind][j][il] = tabXs[((kind * QH + j) * NB + il) * 32 + lane];
+                for (int il = 0; il < NB; ++il) txr[kind][j][il] = src[((kind * QH + j) * NB + il) * 32 + lane];
     }
     auto tx = [&](int kind, int j, int il) -> T {
         if constexpr (TXREG) return txr[kind][j][il];
@@ -451,10 +462,21 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     cp_async_wait<0>();
 }
 
+// Strips to warps: with tables in registers any warp takes any strip, warp
+// k of the 1-D grid strip k in column-major order (gx outer), so the grid
+// covers NSX * NSY strips with no partly idle CTAs; with shared tables the
+// CTA is one column strip gx = blockIdx.x and its warps take consecutive
+// strips of it.
 template <int P, typename T, int GEOM, int NST>
 __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kernel(ApplyParams<T> a)
 {
-    apply_tile<P, T, GEOM, NST>(a, a.x, a.y, blockIdx.x, blockIdx.y);
+    if constexpr (apply_txreg<P, T, GEOM>()) {
+        const int sid = blockIdx.x * blockDim.y + threadIdx.y;
+        const int gx = sid / a.g.NSY;
+        apply_tile<P, T, GEOM, NST>(a, a.x, a.y, gx, sid - gx * a.g.NSY);
+    } else {
+        apply_tile<P, T, GEOM, NST>(a, a.x, a.y, blockIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+    }
 }
 
 // Many independent patches in one launch: CTA b runs work item items[b] =
@@ -469,7 +491,7 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, 0>(), 1)
     const int4 it = items[blockIdx.x];
     if (!active[it.x]) return;
     const long long o = offs[it.x];
-    apply_tile<P, T, 0, NST>(params[it.x], xb + o, yb + o, it.y, it.z);
+    apply_tile<P, T, 0, NST>(params[it.x], xb + o, yb + o, it.y, it.z * blockDim.y + threadIdx.y);
 }
 
 // Sums the frames of the strips covering each seam control point, strip

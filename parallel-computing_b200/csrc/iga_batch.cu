@@ -1390,7 +1390,7 @@ int setup_params(iga_batch *B)
         a.wq = (const T *)op.wq;
         a.kappa = nullptr;
         a.frame = (T *)op.frame;
-        a.g = pl->grid;
+        a.g = op.grid;
         a.sign = T(1);
         a.bc = IGA_BC_IDENTITY;
         a.err = pl->d_err;
@@ -1411,7 +1411,7 @@ int setup_items(iga_batch *B, int pi)
         for (int i = 0; i < B->count; ++i) {
             const iga_plan *pl = B->plans[i];
             if (pl->p != G.P) continue;
-            const StripGrid &g = pl->grid;
+            const StripGrid &g = (pi ? pl->op32 : pl->op64).grid;
             for (int gyb = 0; gyb < (g.NSY + W - 1) / W; ++gyb)
                 for (int gx = 0; gx < g.NSX; ++gx) items.push_back(make_int4(i, gx, gyb, 0));
         }
@@ -1675,7 +1675,8 @@ int iga_batch_shape(const iga_batch *B, int i, int precision, int *rows, int *wa
 {
     if (!B || i < 0 || i >= B->count || !rows || !warps) return IGA_ERR_ARG;
     const int pi = prec_index(precision);
-    *rows = B->plans[i]->grid.TY;
+    const iga_plan *pl = B->plans[i];
+    *rows = (pi ? pl->op32 : pl->op64).grid.TY;
     *warps = 0;
     for (const BGroup &G : B->groups)
         if (G.P == B->plans[i]->p) *warps = G.W[pi];

@@ -184,22 +184,28 @@ int warps_for(int P, int prec, int geom)
 
 // Rows per strip: the candidate whose CTA count fills the SMs best, with a
 // small penalty on short strips (more seam traffic). A MIXED plan launches
-// its FP64 and FP32 operators with different warps per CTA (Ws) on the same
+// its FP64 and FP32 operators with different warps per CTA on the same
 // strips: each precision's cost is taken relative to its own best and the
-// candidate with the smallest sum wins.
-static double strip_cost(int NSX, int ney, int TY, int W, int nsm)
+// candidate with the smallest sum wins. flat: the kernel deals strips to warps
+// one by one (apply_txreg), else a CTA covers W strips of one column.
+struct WarpShape {
+    int W;
+    bool flat;
+};
+
+static double strip_cost(int NSX, int ney, int TY, WarpShape ws, int nsm)
 {
-    const int NSY = (ney + TY - 1) / TY;
-    const long long ctas = (long long)NSX * ((NSY + W - 1) / W);
+    const int NSY = (ney + TY - 1) / TY, W = ws.W;
+    const long long ctas = ws.flat ? ((long long)NSX * NSY + W - 1) / W : (long long)NSX * ((NSY + W - 1) / W);
     const long long waves = (ctas + nsm - 1) / nsm;
     const double work = (double)waves * W * (TY + 2.0);   // per-SM time in strip-row units
     return work * (1.0 + 0.5 * 3.0 / TY);
 }
 
-static int rows_for(int nex, int ney, const std::vector<int> &Ws, int nsm)
+static int rows_for(int nex, int ney, const std::vector<WarpShape> &Ws, int nsm)
 {
     const int NSX = (nex + kSW - 1) / kSW;
-    static const int cands[] = {64, 48, 32, 24, 16};
+    static const int cands[] = {64, 56, 48, 40, 32, 28, 24, 20, 16};
     std::vector<double> best_w(Ws.size(), 1e300);
     for (size_t k = 0; k < Ws.size(); ++k)
         for (int TY : cands) best_w[k] = std::min(best_w[k], strip_cost(NSX, ney, TY, Ws[k], nsm));
@@ -216,6 +222,11 @@ static int rows_for(int nex, int ney, const std::vector<int> &Ws, int nsm)
     return best;
 }
 
+static bool apply_flat(int P, int prec, int geom)
+{
+    return prec == IGA_FP32 || (geom == IGA_GEOM_PRECOMPUTED && P <= 3);
+}
+
 }  // namespace iga
 
 using namespace iga;
@@ -225,7 +236,7 @@ template <typename T>
 static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const Tables1D &tx, const Tables1D &ty)
 {
     const int p = P.p, NB = p + 1, NQ = p + 1, NQ2 = NQ * NQ;
-    const StripGrid &g = pl->grid;
+    const StripGrid &g = op.grid;
     // x tables regrouped per column strip: [gx][kind][j][il][lane], lane = 2c + h
     // holding element column 16 gx + c at quadrature column qx = h QH + j.
     const int QH = (NQ + 1) / 2;
@@ -293,7 +304,7 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
     a.wq = (const T *)op.wq;
     a.kappa = (const T *)op.kappa;
     a.frame = (T *)op.frame;
-    a.g = pl->grid;
+    a.g = op.grid;
     a.sign = (T)sign;
     a.bc = bc;
     a.err = pl->d_err;
@@ -305,9 +316,11 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
         IGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         attr_set = true;
     }
-    dim3 grid(pl->grid.NSX, (pl->grid.NSY + W - 1) / W), block(32, W);
+    const StripGrid &g = op.grid;
+    const long long nstrips = (long long)g.NSX * g.NSY;
+    dim3 grid = apply_txreg<P, T, GEOM>() ? dim3((unsigned)((nstrips + W - 1) / W)) : dim3(g.NSX, (g.NSY + W - 1) / W);
+    dim3 block(32, W);
     kern<<<grid, block, smem, s>>>(a);
-    const StripGrid &g = pl->grid;
     const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
     if (nseam > 0) {
         const int blocks = (int)std::min<long long>((nseam + 255) / 256, 4 * 148);
@@ -478,25 +491,38 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     pl->bc = opts.bc;
     pl->device = opts.device;
     pl->patch = P;
-    std::vector<int> Ws;
-    if (opts.precision != IGA_FP32) Ws.push_back(warps_for(P.p, IGA_FP64, opts.geometry));
-    if (opts.precision != IGA_FP64) Ws.push_back(warps_for(P.p, IGA_FP32, opts.geometry));
-    const int TY = opts.rows_per_strip > 0 ? opts.rows_per_strip : rows_for(P.nex, P.ney, Ws, nsm);
-    if (TY < P.p || TY > 1024) {
-        delete pl;
-        set_error("rows_per_strip must be in [p, 1024]");
-        return IGA_ERR_ARG;
-    }
-    StripGrid &g = pl->grid;
-    g.m = P.m;
-    g.n = P.n;
-    g.nex = P.nex;
-    g.ney = P.ney;
-    g.TY = TY;
-    g.NSX = (P.nex + kSW - 1) / kSW;
-    g.NSY = (P.ney + TY - 1) / TY;
-    g.P = P.p;
-    g.FS = frame_size(P.p, TY);
+    // Rows per strip, per operator: a MIXED plan's FP64 and FP32 operators
+    // have their own G layouts, so each gets the strip height that fills the
+    // SMs best with its own warps per CTA (or the caller's rows_per_strip).
+    auto rows_of = [&](int prec) {
+        if (opts.rows_per_strip > 0) return opts.rows_per_strip;
+        return rows_for(P.nex, P.ney, {{warps_for(P.p, prec, opts.geometry), apply_flat(P.p, prec, opts.geometry)}},
+                        nsm);
+    };
+    auto make_grid = [&](int TY) {
+        StripGrid g;
+        g.m = P.m;
+        g.n = P.n;
+        g.nex = P.nex;
+        g.ney = P.ney;
+        g.TY = TY;
+        g.NSX = (P.nex + kSW - 1) / kSW;
+        g.NSY = (P.ney + TY - 1) / TY;
+        g.P = P.p;
+        g.FS = frame_size(P.p, TY);
+        return g;
+    };
+    const int TY64 = opts.precision != IGA_FP32 ? rows_of(IGA_FP64) : 0;
+    const int TY32 = opts.precision != IGA_FP64 ? rows_of(IGA_FP32) : 0;
+    for (int TY : {TY64, TY32})
+        if (TY != 0 && (TY < P.p || TY > 1024)) {
+            delete pl;
+            set_error("rows_per_strip must be in [p, 1024]");
+            return IGA_ERR_ARG;
+        }
+    if (TY64) pl->op64.grid = make_grid(TY64);
+    if (TY32) pl->op32.grid = make_grid(TY32);
+    pl->grid = TY64 ? pl->op64.grid : pl->op32.grid;   // sizes for the operator-independent kernels
 
     int st = IGA_OK;
     auto fail = [&](int code) {
@@ -602,10 +628,10 @@ int iga_plan_set_kappa(iga_plan *pl, const double *kappa, void *stream)
         if (pl->geometry == IGA_GEOM_PRECOMPUTED) {
             if (k == 0)
                 geom_setup_kernel<double><<<1184, 256, 0, s>>>((double *)op.G, pl->tabX64, pl->tabY64, pl->CP, pl->qw,
-                                                              pl->kappa_dev, pl->grid, pl->d_err);
+                                                              pl->kappa_dev, op.grid, pl->d_err);
             else
                 geom_setup_kernel<float><<<1184, 256, 0, s>>>((float *)op.G, pl->tabX64, pl->tabY64, pl->CP, pl->qw,
-                                                             pl->kappa_dev, pl->grid, pl->d_err);
+                                                             pl->kappa_dev, op.grid, pl->d_err);
         } else {
             const size_t es = k == 0 ? sizeof(double) : sizeof(float);
             if (!op.kappa) IGA_CUDA_TRY(cudaMalloc(&op.kappa, nq * es));

@@ -14,6 +14,7 @@ namespace iga {
 struct OperatorData {
     bool ready = false;
     int warps = 8;
+    StripGrid grid;         // strips of this operator (a MIXED plan's two operators may differ in TY)
     void *tabX = nullptr;   // [NSX][2][NQ][NB][32]
     void *tabY = nullptr;   // [ney][2][NQ][NB]
     void *G = nullptr;      // precomputed geometry (may be null)
