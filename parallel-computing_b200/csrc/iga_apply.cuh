@@ -479,19 +479,24 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kern
     }
 }
 
-// Many independent patches in one launch: CTA b runs work item items[b] =
-// (problem, column strip, block of W strips) with that problem's parameters,
-// or nothing when the problem is marked inactive (converged).
+// Many independent patches in one launch, with that problem's parameters
+// per work item, or nothing when the problem is marked inactive (converged)
+// or the item is padding (problem -1). Tables in registers (apply_txreg):
+// warp k of the grid runs strip items[k] = (problem, column strip, strip
+// row), so the warps of a CTA may take strips of different problems and
+// columns; else CTA b runs items[b] = (problem, column strip, block of W
+// strips of that column).
 template <int P, typename T, int NST>
 __global__ void __launch_bounds__(apply_max_threads<P, T, 0>(), 1)
     apply_batch_kernel(const ApplyParams<T> *__restrict__ params, const int4 *__restrict__ items,
                        const int *__restrict__ active, const long long *__restrict__ offs, const T *__restrict__ xb,
                        T *__restrict__ yb)
 {
-    const int4 it = items[blockIdx.x];
-    if (!active[it.x]) return;
+    constexpr bool flat = apply_txreg<P, T, 0>();
+    const int4 it = items[flat ? blockIdx.x * blockDim.y + threadIdx.y : blockIdx.x];
+    if (it.x < 0 || !active[it.x]) return;   // uniform over the CTA unless flat (no CTA barrier then)
     const long long o = offs[it.x];
-    apply_tile<P, T, 0, NST>(params[it.x], xb + o, yb + o, it.y, it.z * blockDim.y + threadIdx.y);
+    apply_tile<P, T, 0, NST>(params[it.x], xb + o, yb + o, it.y, flat ? it.z : it.z * blockDim.y + threadIdx.y);
 }
 
 // Sums the frames of the strips covering each seam control point, strip

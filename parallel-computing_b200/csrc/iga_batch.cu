@@ -1407,15 +1407,24 @@ int setup_items(iga_batch *B, int pi)
             G.items[pi] = nullptr;
         }
         const int W = G.W[pi];
+        // the kernels' apply_txreg: FP32, or FP64 up to p = 3 (precomputed G)
+        const bool flat = pi == 1 || G.P <= 3;
         std::vector<int4> items;
         for (int i = 0; i < B->count; ++i) {
             const iga_plan *pl = B->plans[i];
             if (pl->p != G.P) continue;
             const StripGrid &g = (pi ? pl->op32 : pl->op64).grid;
-            for (int gyb = 0; gyb < (g.NSY + W - 1) / W; ++gyb)
-                for (int gx = 0; gx < g.NSX; ++gx) items.push_back(make_int4(i, gx, gyb, 0));
+            if (flat) {   // one item per strip (warp)
+                for (int gx = 0; gx < g.NSX; ++gx)
+                    for (int gy = 0; gy < g.NSY; ++gy) items.push_back(make_int4(i, gx, gy, 0));
+            } else {      // one item per CTA: W strips of a column
+                for (int gyb = 0; gyb < (g.NSY + W - 1) / W; ++gyb)
+                    for (int gx = 0; gx < g.NSX; ++gx) items.push_back(make_int4(i, gx, gyb, 0));
+            }
         }
-        G.nitems[pi] = (int)items.size();
+        if (flat)
+            while (items.size() % W) items.push_back(make_int4(-1, 0, 0, 0));   // whole CTAs
+        G.nitems[pi] = (int)(flat ? items.size() / W : items.size());         // CTAs
         int st;
         if ((st = bupload(&G.items[pi], items))) return st;
         const int prec = pi ? IGA_FP32 : IGA_FP64;
