@@ -443,6 +443,23 @@ def our_arm(args):
             dist.destroy_process_group()
         return
 
+    if args.profile_pc:
+        # the exact FEM preconditioner of the p=3 patch (FP32 and FP64) and the
+        # FP32 operator, a few applies outside any graph
+        plan = ib.Plan(ib.unit_square(P, args.ne, args.ne), precision=ib.MIXED)
+        r = torch.from_numpy(splitmix_uniform(SEED, -1.0, 1.0, plan.nfunc)).cuda()
+        z = torch.empty_like(r)
+        r32, z32 = r.float(), torch.empty_like(r, dtype=torch.float32)
+        for _ in range(3):
+            plan.pc_apply(r32, z32, pc=ib.PC_FEM_EXACT, precision=ib.FP32)
+            plan.pc_apply(r, z, pc=ib.PC_FEM_EXACT, precision=ib.FP64)
+            plan.apply(r32, z32, precision=ib.FP32)
+        torch.cuda.synchronize()
+        plan.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
     if args.batch_only:
         res = time_batch(ib, torch, torch.cuda.current_stream(), barrier, max_over_ranks)
         if rank == 0:
@@ -600,6 +617,9 @@ def main():
     ap.add_argument("--skip-solve", action="store_true", help="skip the time-to-1e-10 solves")
     ap.add_argument("--batch-only", action="store_true",
                     help="time only the 256-problem batched solves (prints their JSON object)")
+    ap.add_argument("--profile-pc", action="store_true",
+                    help="run the exact FEM preconditioner (FP32, FP64) and the FP32 operator of the p=3 patch "
+                         "(--ne) a few times outside any graph (a target for ncu; prints nothing else)")
     ap.add_argument("--profile-batch-pc", action="store_true",
                     help="run the batched preconditioner and operator of the 256-problem batch a few times "
                          "outside any graph (a target for ncu; prints nothing else)")
