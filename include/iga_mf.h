@@ -42,7 +42,7 @@ typedef struct iga_plan iga_plan;
 enum {
     IGA_OK = 0,
     IGA_ERR_ARG = 1,            /* invalid argument or mesh */
-    IGA_ERR_UNSUPPORTED = 2,    /* valid input this build does not handle */
+    IGA_ERR_UNSUPPORTED = 2,    /* valid input this library does not handle */
     IGA_ERR_CUDA = 3,           /* a CUDA runtime call failed */
     IGA_ERR_NOMEM = 4,          /* device allocation failed */
     IGA_ERR_NOT_CONVERGED = 5,  /* Krylov solve hit max_it */
@@ -63,7 +63,7 @@ enum { IGA_F_REFERENCE = 0, IGA_F_SINSIN = 1, IGA_F_ANNULUS = 2 }; /* load funct
 /* One single-patch tensor-product mesh, in the reference's arrays (all HOST
  * pointers, read during iga_plan_create only). Optional arrays may be NULL. */
 typedef struct {
-    int p, q;             /* degrees; this build requires p == q, 1 <= p <= 5 */
+    int p, q;             /* degrees; this library requires p == q, 1 <= p <= 5 */
     int nElemX, nElemY;
     const double *CP;     /* 2*nfunc, (x,y) interleaved, nfunc = (nElemX+p)*(nElemY+q) */
     const double *weights;/* nfunc NURBS weights or NULL (reference: no weights).

@@ -249,7 +249,7 @@ static bool factor_weights(const double *w, int m, int n, std::vector<double> &a
 std::string build_patch(const MeshDescView &d, Patch &P)
 {
     if (d.p < 1 || d.p > 5) return "p must be in 1..5";
-    if (d.q != d.p) return "this build requires p == q";
+    if (d.q != d.p) return "this library requires p == q";
     if (d.nex < 1 || d.ney < 1) return "nElemX and nElemY must be positive";
     if (!d.CP) return "CP is required";
     P.p = d.p;

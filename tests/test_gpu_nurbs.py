@@ -1,4 +1,4 @@
-"""NURBS geometry: the exact quarter annulus (BASELINE's mixed-precision case).
+"""NURBS geometry: the exact quarter annulus (the mixed-precision configuration).
 
 The reference has no rational geometry, so parity here is against the oracle's
 restatement of the reference element algorithm extended with control-point
