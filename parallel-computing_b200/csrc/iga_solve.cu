@@ -1437,9 +1437,12 @@ static int build_loop(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_
 }
 
 // Flexible PCG whose iterations run on the device: one graph launch per solve.
+// x_zero: x is known to be zero and b nonzero (a refinement sweep on the
+// normalised residual): r = b without the operator and no host check before
+// the loop.
 template <typename T>
 static int pcg_graph(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_solve_opts &o, const T *b, T *x,
-                     double rtol, double bnorm, int prec, int &its)
+                     double rtol, double bnorm, int prec, int &its, bool x_zero = false)
 {
     const long long N = pl->nfunc;
     const cudaStream_t s = S->stream;
@@ -1452,10 +1455,15 @@ static int pcg_graph(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_s
     }
     if (b != ps.b) copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.b, b, N);
     if (x != ps.x) copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.x, x, N);
-    if ((st = iga_apply_internal_sb(pl, prec, ps.x, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY))) return st;
-    sub_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.b, ps.q, ps.r, N, S->s, S->partials, S->counter);
-    if ((st = sync_scalars(S))) return st;
-    if (std::sqrt(S->h->rr) <= rtol * bnorm) return IGA_OK;
+    if (x_zero) {
+        copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.b, N);
+        dot_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.r, N, &S->s->rr, S->partials, S->counter);
+    } else {
+        if ((st = iga_apply_internal_sb(pl, prec, ps.x, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY))) return st;
+        sub_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.b, ps.q, ps.r, N, S->s, S->partials, S->counter);
+        if ((st = sync_scalars(S))) return st;
+        if (std::sqrt(S->h->rr) <= rtol * bnorm) return IGA_OK;
+    }
     int64_t dummy = 0;
     if ((st = pc_apply(ps, pl, S, o, ps.r, ps.z, o.pc_rtol, dummy))) return st;
     dot_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, N, &S->s->rz, S->partials, S->counter);
@@ -1678,7 +1686,8 @@ int iga_solve(iga_plan *pl, const double *b, double *x, const iga_solve_opts *o_
             st = o.pc == IGA_PC_FEM_CG
                      ? pcg<float>(pl, S, S->f, o, S->f.b, S->f.x, o.sweep_rtol, 1.0, o.pc_rtol, IGA_FP32,
                                   stt.iterations, stt.pc_iterations)
-                     : pcg_graph<float>(pl, S, S->f, o, S->f.b, S->f.x, o.sweep_rtol, 1.0, IGA_FP32, stt.iterations);
+                     : pcg_graph<float>(pl, S, S->f, o, S->f.b, S->f.x, o.sweep_rtol, 1.0, IGA_FP32, stt.iterations,
+                                        true);
             if (st && st != IGA_ERR_NOT_CONVERGED) {
                 result = st;
                 break;
