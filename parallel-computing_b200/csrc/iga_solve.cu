@@ -708,10 +708,33 @@ static int tri_warps(int nyp, size_t esz, size_t &smem)
 // blockIdx.y strides over the columns b, so no index division is needed. With
 // sc (FP64 vectors, FP32 transform) the gather divides by pc_scale and the
 // scatter multiplies by it.
-template <typename T, typename V>
-__global__ void fd_gather_kernel(const V *__restrict__ r, T *__restrict__ U, int m, int nx, int ny, int nxp, int nyp,
-                                 const DevScalars *sc)
+// z = r on the boundary ring of the m x n grid (identity rows of K_fem),
+// ring entries t0, t0 + stride, ...
+template <typename T>
+__device__ __forceinline__ void ring_copy(T *__restrict__ z, const T *__restrict__ r, int m, int n, long long t0,
+                                          long long stride)
 {
+    const long long nb = 2LL * m + 2LL * (n - 2);
+    for (long long t = t0; t < nb; t += stride) {
+        long long idx;
+        if (t < m) idx = t;
+        else if (t < 2LL * m) idx = (long long)(n - 1) * m + (t - m);
+        else {
+            const long long u = t - 2LL * m;
+            const long long j = 1 + u / 2;
+            idx = j * m + ((u % 2) ? (m - 1) : 0);
+        }
+        z[idx] = r[idx];
+    }
+}
+
+// The gather also copies the boundary ring of r into z (one launch fewer).
+template <typename T, typename V>
+__global__ void fd_gather_kernel(const V *__restrict__ r, T *__restrict__ U, V *__restrict__ z, int m, int n, int nx,
+                                 int ny, int nxp, int nyp, const DevScalars *sc)
+{
+    ring_copy(z, r, m, n, ((long long)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x,
+              (long long)gridDim.x * gridDim.y * blockDim.x);
     constexpr int VN = Pk<T>::n;
     const double inv = sc ? 1.0 / pc_scale(sc) : 1.0;
     const int nv = nxp / VN;
@@ -756,18 +779,7 @@ static dim3 grid2d(int ngroups, int ncols)
 template <typename T>
 __global__ void boundary_copy_kernel(T *__restrict__ z, const T *__restrict__ r, int m, int n)
 {
-    const long long nb = 2LL * m + 2LL * (n - 2);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb; t += (long long)gridDim.x * blockDim.x) {
-        long long idx;
-        if (t < m) idx = t;
-        else if (t < 2LL * m) idx = (long long)(n - 1) * m + (t - m);
-        else {
-            const long long u = t - 2LL * m;
-            const long long j = 1 + u / 2;
-            idx = j * m + ((u % 2) ? (m - 1) : 0);
-        }
-        z[idx] = r[idx];
-    }
+    ring_copy(z, r, m, n, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 
 // ------------------------------------------------------------ kappa scaling of the preconditioner
@@ -1185,14 +1197,16 @@ template <typename T, typename V>
 static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const V *r, V *z, const DevScalars *sc)
 {
     const int m = pl->m, n = pl->n, nx = m - 2, ny = n - 2;
-    boundary_copy_kernel<V><<<kRedBlocks, kThreads, 0, S->stream>>>(z, r, m, n);
-    if (nx <= 0 || ny <= 0) return IGA_OK;
+    if (nx <= 0 || ny <= 0) {   // no free nodes: the ring is everything
+        boundary_copy_kernel<V><<<kRedBlocks, kThreads, 0, S->stream>>>(z, r, m, n);
+        return IGA_OK;
+    }
     const int nxp = ps.nxp, nyp = ps.nyp;
     int seg = (ny + 31) / 32;
     seg |= 1;   // odd: conflict-free shared-memory rows
     cublasSetStream(S->blas, S->stream);
     constexpr int VN = Pk<T>::n;
-    fd_gather_kernel<T, V><<<grid2d(nxp / VN, nyp), 128, 0, S->stream>>>(r, ps.W2, m, nx, ny, nxp, nyp, sc);
+    fd_gather_kernel<T, V><<<grid2d(nxp / VN, nyp), 128, 0, S->stream>>>(r, ps.W2, z, m, n, nx, ny, nxp, nyp, sc);
     cublasStatus_t e = gemm(S->blas, CUBLAS_OP_T, CUBLAS_OP_N, nyp, nxp, nxp, ps.W2, nxp, ps.Vx, nxp, ps.W1, nyp);
     if (e == CUBLAS_STATUS_SUCCESS) {
         if (ps.tri_w) {
