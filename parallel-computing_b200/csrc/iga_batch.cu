@@ -372,6 +372,8 @@ template <typename T>
 struct FdProb {
     const T *Vx, *lx;      // x eigenvectors (column-major, ld nx) and eigenvalues
     const T *VxT;          // the transpose of Vx (column-major), for the tcgen05 tiles
+    const T *Vxp, *VxTp;   // FP32: Vx and VxT with columns padded to ldv (a multiple of 4): 16-byte rows
+    int ldv;
     const T *Dv, *Cf;      // LDL^T factors of the y systems: 1 / pivot, upper off-diagonal; [b][a], ld nx
     const double *yc;      // free y nodes' pencil Kd | Ko | Md | Mo (ny each)
     T *W1;                 // nx * ny work matrix
@@ -704,9 +706,9 @@ __global__ void __launch_bounds__(128) fd_umma_kernel(const FdProb<float> *__res
     float *C;
     int lda, ldb, ldc;
     if (STAGE == 1) {
-        A = f.Vx; lda = nx; Bm = rb + f.off + m + 1; ldb = m; C = f.W1; ldc = nx;
+        A = f.Vxp; lda = f.ldv; Bm = rb + f.off + m + 1; ldb = m; C = f.W1; ldc = nx;
     } else {
-        A = f.VxT; lda = nx; Bm = f.W1; ldb = nx; C = zb + f.off + m + 1; ldc = m;
+        A = f.VxTp; lda = f.ldv; Bm = f.W1; ldb = nx; C = zb + f.off + m + 1; ldc = m;
     }
     if (STAGE == 1 && tl.y == 0 && tl.z == 0) {   // boundary ring: identity rows of K_fem
         const float *r = rb + f.off;
@@ -737,15 +739,20 @@ __global__ void __launch_bounds__(128) fd_umma_kernel(const FdProb<float> *__res
     umma::fence_after_sync();
     const uint32_t tmem = *tbase;
 
-    // thread (warp, lane) moves k = lane of the slice for rows warp + 4 i
-    float ra[kUM / 4], rv[kUN / 4];
+    // A (rows padded to lda, a multiple of 4, zero past K): thread t moves the
+    // 16-byte K chunk t % 8 of rows t / 8 + 16 i; B: thread (warp, lane) moves
+    // k = lane of rows warp + 4 i
+    float4 ra[kUM / 16];
+    float rv[kUN / 4];
     auto fetch = [&](int k0) {
         const int k = k0 + lane;
         const bool kin = k < K;
+        const int kc = k0 + 4 * (tid & 7);
 #pragma unroll
-        for (int i = 0; i < kUM / 4; ++i) {
-            const int a = a0 + warp + 4 * i;
-            ra[i] = (kin && a < nx) ? A[(size_t)a * lda + k] : 0.0f;
+        for (int i = 0; i < kUM / 16; ++i) {
+            const int a = a0 + (tid >> 3) + 16 * i;
+            ra[i] = (kc < K && a < nx) ? *reinterpret_cast<const float4 *>(A + (size_t)a * lda + kc)
+                                       : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
         for (int i = 0; i < kUN / 4; ++i) {
@@ -757,9 +764,11 @@ __global__ void __launch_bounds__(128) fd_umma_kernel(const FdProb<float> *__res
         unsigned char *Ab = sm + buf * kAStage, *Bb = sm + 2 * kAStage + buf * kBStage;
         const int ch = lane >> 2, w4 = (lane & 3) * 4;
 #pragma unroll
-        for (int i = 0; i < kUM / 4; ++i) {
-            const int r = warp + 4 * i;
-            *reinterpret_cast<float *>(Ab + ch * kALbo + (r >> 3) * 128 + (r & 7) * 16 + w4) = to_operand(ra[i]);
+        for (int i = 0; i < kUM / 16; ++i) {
+            const int r = (tid >> 3) + 16 * i;
+            const float4 v = make_float4(to_operand(ra[i].x), to_operand(ra[i].y), to_operand(ra[i].z),
+                                         to_operand(ra[i].w));
+            *reinterpret_cast<float4 *>(Ab + (tid & 7) * kALbo + (r >> 3) * 128 + (r & 7) * 16) = v;
         }
 #pragma unroll
         for (int i = 0; i < kUN / 4; ++i) {
@@ -1280,7 +1289,8 @@ int setup_fd(iga_batch *B)
     auto upload_prec = [&](auto tag) -> int {
         using T = decltype(tag);
         BVec<T> &v = vecs<T>(B);
-        std::vector<T *> V(bases.size()), L(bases.size()), VT(bases.size());
+        std::vector<T *> V(bases.size()), L(bases.size()), VT(bases.size()), Vp(bases.size(), nullptr),
+            VTp(bases.size(), nullptr);
         for (size_t k = 0; k < bases.size(); ++k) {
             const int nb = bases[k].n;
             std::vector<T> hv(bases[k].V.begin(), bases[k].V.end()), hl(bases[k].lam.begin(), bases[k].lam.end());
@@ -1292,6 +1302,18 @@ int setup_fd(iga_batch *B)
             v.basis.push_back(V[k]);
             v.basis.push_back(L[k]);
             v.basis.push_back(VT[k]);
+            if (sizeof(T) == 4) {   // padded copies for the tcgen05 tiles' 16-byte operand loads
+                const int ld = (nb + 3) / 4 * 4;
+                std::vector<T> pv((size_t)nb * ld, T(0)), pt((size_t)nb * ld, T(0));
+                for (int i = 0; i < nb; ++i)
+                    for (int j = 0; j < nb; ++j) {
+                        pv[(size_t)i * ld + j] = hv[(size_t)i * nb + j];
+                        pt[(size_t)i * ld + j] = ht[(size_t)i * nb + j];
+                    }
+                if ((st = bupload(&Vp[k], pv)) || (st = bupload(&VTp[k], pt))) return st;
+                v.basis.push_back(Vp[k]);
+                v.basis.push_back(VTp[k]);
+            }
         }
         std::vector<FdProb<T>> fp(B->count);
         size_t wtot = 0;
@@ -1305,6 +1327,9 @@ int setup_fd(iga_batch *B)
             FdProb<T> &f = fp[i];
             f.Vx = V[bx[i]];
             f.VxT = VT[bx[i]];
+            f.Vxp = Vp[bx[i]];
+            f.VxTp = VTp[bx[i]];
+            f.ldv = (bases[bx[i]].n + 3) / 4 * 4;
             f.lx = L[bx[i]];
             f.yc = B->ycoef[by[i]];
             f.W1 = v.W1 + wo;
