@@ -741,50 +741,59 @@ __global__ void __launch_bounds__(128) fd_umma_kernel(const FdProb<float> *__res
 
     // A (rows padded to lda, a multiple of 4, zero past K): thread t moves the
     // 16-byte K chunk t % 8 of rows t / 8 + 16 i; B: thread (warp, lane) moves
-    // k = lane of rows warp + 4 i
-    float4 ra[kUM / 16];
-    float rv[kUN / 4];
-    auto fetch = [&](int k0) {
-        const int k = k0 + lane;
+    // k = lane of rows warp + 4 i. Two register sets: slice kt + 2 is loaded
+    // while slice kt + 1 goes from the other set into shared memory, so a
+    // slice's global loads have a whole iteration to land.
+    struct Regs {
+        float4 a[kUM / 16];
+        float b[kUN / 4];
+    };
+    Regs R0, R1;
+    auto fetch = [&](int kt, Regs &rg) {
+        const int k0 = kt * kUK, k = k0 + lane;
         const bool kin = k < K;
         const int kc = k0 + 4 * (tid & 7);
 #pragma unroll
         for (int i = 0; i < kUM / 16; ++i) {
             const int a = a0 + (tid >> 3) + 16 * i;
-            ra[i] = (kc < K && a < nx) ? *reinterpret_cast<const float4 *>(A + (size_t)a * lda + kc)
-                                       : make_float4(0.f, 0.f, 0.f, 0.f);
+            rg.a[i] = (kc < K && a < nx) ? *reinterpret_cast<const float4 *>(A + (size_t)a * lda + kc)
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
         }
 #pragma unroll
         for (int i = 0; i < kUN / 4; ++i) {
             const int b = b0 + warp + 4 * i;
-            rv[i] = (kin && b < ny) ? Bm[(size_t)b * ldb + k] : 0.0f;
+            rg.b[i] = (kin && b < ny) ? Bm[(size_t)b * ldb + k] : 0.0f;
         }
     };
-    auto stash = [&](int buf) {
+    auto stash = [&](int buf, const Regs &rg) {
         unsigned char *Ab = sm + buf * kAStage, *Bb = sm + 2 * kAStage + buf * kBStage;
         const int ch = lane >> 2, w4 = (lane & 3) * 4;
 #pragma unroll
         for (int i = 0; i < kUM / 16; ++i) {
             const int r = (tid >> 3) + 16 * i;
-            const float4 v = make_float4(to_operand(ra[i].x), to_operand(ra[i].y), to_operand(ra[i].z),
-                                         to_operand(ra[i].w));
+            const float4 v = make_float4(to_operand(rg.a[i].x), to_operand(rg.a[i].y), to_operand(rg.a[i].z),
+                                         to_operand(rg.a[i].w));
             *reinterpret_cast<float4 *>(Ab + (tid & 7) * kALbo + (r >> 3) * 128 + (r & 7) * 16) = v;
         }
 #pragma unroll
         for (int i = 0; i < kUN / 4; ++i) {
             const int r = warp + 4 * i;
-            *reinterpret_cast<float *>(Bb + ch * kBLbo + (r >> 3) * 128 + (r & 7) * 16 + w4) = to_operand(rv[i]);
+            *reinterpret_cast<float *>(Bb + ch * kBLbo + (r >> 3) * 128 + (r & 7) * 16 + w4) = to_operand(rg.b[i]);
         }
     };
     constexpr uint32_t IDESC = umma::idesc_tf32<kUM, kUN>();
     const int nk = (K + kUK - 1) / kUK;
-    fetch(0);
-    stash(0);
+    fetch(0, R0);
+    if (nk > 1) fetch(1, R1);
+    stash(0, R0);
     fence_proxy_async_smem();
     __syncthreads();
     bool failed = false;
     int last = -1;   // last slice whose MMAs were issued
-    for (int kt = 0; kt < nk; ++kt) {
+    // one iteration: MMAs of slice kt; loads of slice kt + 2 into the set that
+    // held slice kt (`cur`); slice kt + 1 from the other set (`nxt`) into the
+    // buffer freed by slice kt - 1
+    auto step = [&](int kt, Regs &cur, Regs &nxt) -> bool {
         const int buf = kt & 1;
         if (tid == 0) {
             umma::fence_after_sync();
@@ -796,16 +805,23 @@ __global__ void __launch_bounds__(128) fd_umma_kernel(const FdProb<float> *__res
             umma::commit(&bars[buf]);
         }
         last = kt;
+        if (kt + 2 < nk) fetch(kt + 2, cur);
         if (kt + 1 < nk) {
-            fetch((kt + 1) * kUK);
             bool ok = true;
             if (kt >= 1) ok = mbar_wait_bounded(&bars[(kt - 1) & 1], ((kt - 1) >> 1) & 1);   // buffer reused
-            failed = __syncthreads_or(!ok);
-            if (failed) break;
-            stash((kt + 1) & 1);
+            if (__syncthreads_or(!ok)) return false;
+            stash((kt + 1) & 1, nxt);
             fence_proxy_async_smem();
         }
         __syncthreads();
+        return true;
+    };
+    for (int kt = 0; kt < nk; ++kt) {
+        const bool ok = (kt & 1) ? step(kt, R1, R0) : step(kt, R0, R1);
+        if (!ok) {
+            failed = true;
+            break;
+        }
     }
     // all MMAs done: the last commit tracks every earlier MMA of thread 0
     const bool ok = mbar_wait_bounded(&bars[last & 1], (last >> 1) & 1);
