@@ -830,8 +830,9 @@ struct PrecState {
     T *Vx = nullptr, *lx = nullptr, *W1 = nullptr, *W2 = nullptr, *Dv = nullptr;
     T *Lf = nullptr;   // LDL^T unit lower factor's subdiagonal per x mode (layout of Dv)
     int nxp = 0, nyp = 0;   // transform sizes padded to multiples of 64
-    int tri_w = 0;          // warps per CTA of the staged tridiagonal kernel (0: in place)
-    size_t tri_smem = 0;
+    int tri_w = 0;          // most warps per CTA of the staged tridiagonal kernel (0: in place)
+    size_t tri_smem = 0;    // its shared memory at tri_w warps
+    int nsm = 148;          // SMs of the plan's device
     // device-side PCG loop: a CUDA graph whose conditional WHILE node runs one
     // iteration per pass (built for one preconditioner / kappa-scaling choice)
     cudaGraphExec_t loop = nullptr;
@@ -1146,6 +1147,7 @@ static int fd_upload(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
         (st = up_fac(&ps.Lf, S->Lf)))
         return st;
     ps.tri_w = tri_warps(nyp, sizeof(T), ps.tri_smem);
+    SOLVE_TRY(cudaDeviceGetAttribute(&ps.nsm, cudaDevAttrMultiProcessorCount, pl->device));
     if (ps.tri_w)
         SOLVE_TRY(cudaFuncSetAttribute(fd_tri_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)ps.tri_smem));
@@ -1210,9 +1212,12 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
     cublasStatus_t e = gemm(S->blas, CUBLAS_OP_T, CUBLAS_OP_N, nyp, nxp, nxp, ps.W2, nxp, ps.Vx, nxp, ps.W1, nyp);
     if (e == CUBLAS_STATUS_SUCCESS) {
         if (ps.tri_w) {
-            const int grid = std::min((nx + ps.tri_w - 1) / ps.tri_w, 148);
-            fd_tri_kernel<T, true><<<grid, ps.tri_w * 32, ps.tri_smem, S->stream>>>(ps.W1, ps.Lf, ps.Dv, nx, ny, nyp,
-                                                                                 seg, S->s);
+            // one mode per warp as long as the modes reach every SM, else the most
+            // warps per CTA that shared memory allows (warps then loop over modes)
+            const int w = std::max(1, std::min(ps.tri_w, (nx + ps.nsm - 1) / ps.nsm));
+            const int grid = std::min((nx + w - 1) / w, ps.nsm);
+            const size_t smem = ps.tri_smem / ps.tri_w * w;
+            fd_tri_kernel<T, true><<<grid, w * 32, smem, S->stream>>>(ps.W1, ps.Lf, ps.Dv, nx, ny, nyp, seg, S->s);
         } else {
             fd_tri_kernel<T, false><<<(nx + 7) / 8, 256, 0, S->stream>>>(ps.W1, ps.Lf, ps.Dv, nx, ny, nyp, seg, S->s);
         }
