@@ -38,7 +38,7 @@ struct ApplyParams {
     T *y;
     const T *G;       // GEOM 0: [strip][TY][NQ][NQ][3][SW]
     const T *tabX;    // [NSX][2][QH][NB][32]  (kind 0: value, 1: d/dxi)
-    const T *tabY;    // [ney][2][NQ][NB]
+    const T *tabY;    // [ney][2][NQ][NBP] (NB values, zero-padded to 16-byte rows)
     const T *CP;      // GEOM 1: (x, y) per control point, in T
     const T *wq;      // GEOM 1: w_qx * w_qy, [NQ*NQ] (qx fastest)
     const T *kappa;   // GEOM 1: per quadrature point or null
@@ -60,7 +60,8 @@ struct ApplyShape {
     static constexpr int TABX = 2 * QH * NB * 32;       // x tables of a column strip
     static constexpr int XR = 8;                        // x / CP rows in flight per warp
     static constexpr int XW = 24;                       // >= SW + P, padded
-    static constexpr int TYW = 2 * NQ * NB;             // one element row's y tables
+    static constexpr int NBP = tab_nbp(NB, (int)sizeof(T));   // y-table row length
+    static constexpr int TYW = 2 * NQ * NBP;            // one element row's y tables
     static_assert(GBYTES % 16 == 0, "bulk copy size must be a multiple of 16 bytes");
     static_assert(kSW + P <= XW, "row buffer too narrow");
 };
@@ -186,10 +187,12 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
             cp_async_zfill<sizeof(T)>(xr + (k % S::XR) * S::XW + lane, x + gi, v);
             if (GEOM == 1) cp_async_zfill<2 * sizeof(T)>(cr + ((k % S::XR) * S::XW + lane) * 2, a.CP + 2 * gi, v);
         }
-        if (k >= P && k < nrows)
-            for (int t = lane; t < S::TYW; t += 32)
-                cp_async_zfill<sizeof(T)>(yr + (k % S::XR) * S::TYW + t, a.tabY + (size_t)(ey0 + k - P) * S::TYW + t,
-                                          true);
+        if (k >= P && k < nrows) {   // 16-byte copies (rows are whole 16-byte words)
+            constexpr int CH = S::TYW * (int)sizeof(T) / 16;
+            const unsigned char *src = reinterpret_cast<const unsigned char *>(a.tabY + (size_t)(ey0 + k - P) * S::TYW);
+            unsigned char *dst = reinterpret_cast<unsigned char *>(yr + (k % S::XR) * S::TYW);
+            for (int t = lane; t < CH; t += 32) cp_async_zfill<16>(dst + 16 * t, src + 16 * t, true);
+        }
         cp_async_commit();
     };
     constexpr int D = S::XR - 1;
@@ -342,29 +345,22 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
 #pragma unroll
         for (int qy = 0; qy < NQ; ++qy) {
             T n2[NB], d2[NB];
-            // A row's tables start 16-byte aligned in the ring (its offsets are
-            // multiples of TYW * sizeof(T)); when a qy row is a whole number of
-            // 16-byte words it loads as vectors.
-            if constexpr ((NB * sizeof(T)) % 16 == 0) {
-                constexpr int V = 16 / sizeof(T);
+            {   // rows of NBP entries, 16-byte aligned in the ring: vector loads
+                constexpr int V = 16 / sizeof(T), NBP = S::NBP;
                 using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
-                const VT *a = reinterpret_cast<const VT *>(ty + qy * NB);
-                const VT *b = reinterpret_cast<const VT *>(ty + (NQ + qy) * NB);
+                const VT *va = reinterpret_cast<const VT *>(ty + qy * NBP);
+                const VT *vb = reinterpret_cast<const VT *>(ty + (NQ + qy) * NBP);
 #pragma unroll
-                for (int v = 0; v < NB / V; ++v) {
-                    const VT ua = a[v], ub = b[v];
+                for (int v = 0; v < NBP / V; ++v) {
+                    const VT ua = va[v], ub = vb[v];
                     const T *pa = reinterpret_cast<const T *>(&ua), *pb = reinterpret_cast<const T *>(&ub);
 #pragma unroll
                     for (int e = 0; e < V; ++e) {
-                        n2[v * V + e] = pa[e];
-                        d2[v * V + e] = pb[e];
+                        if (v * V + e < NB) {
+                            n2[v * V + e] = pa[e];
+                            d2[v * V + e] = pb[e];
+                        }
                     }
-                }
-            } else {
-#pragma unroll
-                for (int jl = 0; jl < NB; ++jl) {
-                    n2[jl] = ty[qy * NB + jl];
-                    d2[jl] = ty[(NQ + qy) * NB + jl];
                 }
             }
 #pragma unroll

@@ -85,6 +85,14 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// Entries per (kind, qy) row of the apply kernel's y tables: the NB basis
+// values padded so that a row is a whole number of 16-byte words (vector
+// loads, 16-byte copies).
+__host__ __device__ constexpr int tab_nbp(int NB, int esz)
+{
+    return (NB * esz) % 16 == 0 ? NB : ((NB * esz + 15) / 16 * 16) / esz;
+}
+
 // ---------------------------------------------------------------- strips
 // Element columns per warp strip (two lanes per element column).
 constexpr int kSW = 16;

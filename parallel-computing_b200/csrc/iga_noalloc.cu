@@ -62,7 +62,8 @@ __global__ void noalloc_tables_kernel(double *__restrict__ tabX, double *__restr
 {
     const int NB = P + 1, NQ = P + 1, QH = (NQ + 1) / 2;
     const long long nX = (long long)NSX * 2 * QH * NB * 32;
-    const long long nY = (long long)ney * 2 * NQ * NB;
+    const int NBP = iga::tab_nbp(NB, (int)sizeof(double));
+    const long long nY = (long long)ney * 2 * NQ * NBP;
     const long long tid0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (tid0 == 0) *err = 0;
     for (long long t = tid0; t < nX + nY + NQ * NQ; t += (long long)gridDim.x * blockDim.x) {
@@ -83,18 +84,20 @@ __global__ void noalloc_tables_kernel(double *__restrict__ tabX, double *__restr
                 for (int k = 0; k < NB; ++k) v += Ce[k] * Bq[k];
             }
             tabX[t] = v;
-        } else if (t < nX + nY) {   // [ey][kind][qy][jl]
+        } else if (t < nX + nY) {   // [ey][kind][qy][jl], jl < NBP (zero past NB)
             const long long u = t - nX;
-            const int jl = (int)(u % NB);
-            long long r = u / NB;
+            const int jl = (int)(u % NBP);
+            long long r = u / NBP;
             const int qy = (int)(r % NQ);
             r /= NQ;
             const int kind = (int)(r % 2);
             const int ey = (int)(r / 2);
-            const double *Ce = C2 + (size_t)ey * NB * NB + jl * NB;
-            const double *Bq = (kind ? dB2 : B2) + qy * NB;
             double v = 0.0;
-            for (int k = 0; k < NB; ++k) v += Ce[k] * Bq[k];
+            if (jl < NB) {
+                const double *Ce = C2 + (size_t)ey * NB * NB + jl * NB;
+                const double *Bq = (kind ? dB2 : B2) + qy * NB;
+                for (int k = 0; k < NB; ++k) v += Ce[k] * Bq[k];
+            }
             tabY[u] = v;
         } else {
             const int k = (int)(t - nX - nY);
@@ -118,7 +121,7 @@ Layout layout_for(int P, int nex, int ney, int TY)
     L.off_wq = 256;
     L.off_tabX = L.off_wq + up256(sizeof(double) * NQ * NQ);
     L.off_tabY = L.off_tabX + up256(sizeof(double) * NSX * 2 * QH * NB * 32);
-    L.off_frame = L.off_tabY + up256(sizeof(double) * (size_t)ney * 2 * NQ * NB);
+    L.off_frame = L.off_tabY + up256(sizeof(double) * (size_t)ney * 2 * NQ * iga::tab_nbp(NB, (int)sizeof(double)));
     L.total = L.off_frame + up256(sizeof(double) * NSX * NSY * iga::frame_size(P, TY));
     return L;
 }
