@@ -47,7 +47,8 @@ typedef struct {
     double pc_rtol;    /* IGA_PC_FEM_CG inner tolerance (reference: 1e-10) */
     int pc_max_it;     /* IGA_PC_FEM_CG inner iteration cap (reference: 10000) */
     double sweep_rtol; /* IGA_MIXED: residual reduction asked of each FP32 sweep (default 1e-3:
-                          shallow sweeps restart the Krylov space before FP32 rounding slows it) */
+                          shallow sweeps restart the Krylov space before FP32 rounding slows it);
+                          a sweep asks for less when less is left to reach rtol */
     int max_sweeps;    /* IGA_MIXED: refinement sweeps */
     int x0_nonzero;    /* 1: use x as the initial guess, 0: start from x = 0 */
 } iga_solve_opts;

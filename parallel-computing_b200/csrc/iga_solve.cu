@@ -1700,13 +1700,17 @@ int iga_solve(iga_plan *pl, const double *b, double *x, const iga_solve_opts *o_
         for (int sw = 0; sw < o.max_sweeps && rel > o.rtol; ++sw) {
             // rhs of the sweep: r64 / ||r64|| in FP32; correction d solves K d = r / ||r||.
             const double scale = std::sqrt(S->h->rr);
+            // A sweep asks for sweep_rtol, or for less when less is left to do:
+            // a fifth of the reduction that would reach rtol (margin for the
+            // FP32 recurrence residual drifting from the FP64 one).
+            const double need = o.rtol * bnorm / scale;
+            const double srtol = std::max(o.sweep_rtol, std::min(0.2 * need, 0.5));
             scale_down_kernel<<<kRedBlocks, kThreads, 0, S->stream>>>(S->r64, S->f.b, N, S->s);
             zero_kernel<float><<<kRedBlocks, kThreads, 0, S->stream>>>(S->f.x, N);
             st = o.pc == IGA_PC_FEM_CG
-                     ? pcg<float>(pl, S, S->f, o, S->f.b, S->f.x, o.sweep_rtol, 1.0, o.pc_rtol, IGA_FP32,
-                                  stt.iterations, stt.pc_iterations)
-                     : pcg_graph<float>(pl, S, S->f, o, S->f.b, S->f.x, o.sweep_rtol, 1.0, IGA_FP32, stt.iterations,
-                                        true);
+                     ? pcg<float>(pl, S, S->f, o, S->f.b, S->f.x, srtol, 1.0, o.pc_rtol, IGA_FP32, stt.iterations,
+                                  stt.pc_iterations)
+                     : pcg_graph<float>(pl, S, S->f, o, S->f.b, S->f.x, srtol, 1.0, IGA_FP32, stt.iterations, true);
             if (st && st != IGA_ERR_NOT_CONVERGED) {
                 result = st;
                 break;
