@@ -47,6 +47,9 @@ struct ApplyParams {
     T sign;
     int bc;
     int *err;
+    // apply_kernel's window of strip rows: gy0 .. gy0 + gyn - 1 (default: all;
+    // a host-buffer MatMult applies the patch slab by slab to overlap copies)
+    int gy0 = 0, gyn = 1 << 30;
 };
 
 template <int P, typename T>
@@ -466,12 +469,14 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
 template <int P, typename T, int GEOM, int NST>
 __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kernel(ApplyParams<T> a)
 {
+    const int rows = min(a.gyn, a.g.NSY - a.gy0);   // strip rows of the window
     if constexpr (apply_txreg<P, T, GEOM>()) {
         const int sid = blockIdx.x * blockDim.y + threadIdx.y;
-        const int gx = sid / a.g.NSY;
-        apply_tile<P, T, GEOM, NST>(a, a.x, a.y, gx, sid - gx * a.g.NSY);
+        const int gx = sid / rows;
+        apply_tile<P, T, GEOM, NST>(a, a.x, a.y, gx, a.gy0 + (sid - gx * rows));
     } else {
-        apply_tile<P, T, GEOM, NST>(a, a.x, a.y, blockIdx.x, blockIdx.y * blockDim.y + threadIdx.y);
+        const int r = blockIdx.y * blockDim.y + threadIdx.y;
+        apply_tile<P, T, GEOM, NST>(a, a.x, a.y, blockIdx.x, r < rows ? a.gy0 + r : a.g.NSY);
     }
 }
 
@@ -498,6 +503,28 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, 0>(), 1)
 // Sums the frames of the strips covering each seam control point, strip
 // (row, then column) in ascending order, and stores sign * sum (boundary
 // rules as in apply_kernel: bc 0 zero, 1 identity, 2 none). idx enumerates the seam points of grid g.
+// The seam control point (R, C): the covering strips' frame values summed
+// in fixed strip order, stored with the boundary rule.
+template <int P, typename T>
+__device__ __forceinline__ void seam_point_rc(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
+                                              const StripGrid &g, T sign, int bc, int R, int C)
+{
+    int fa, fb;
+    const int ca = cover(C, kSW, g.NSX, P, fa);
+    const int cb = cover(R, g.TY, g.NSY, P, fb);
+    T v = 0;
+    for (int bi = 0; bi < cb; ++bi) {
+        const int b = fb + bi;
+        for (int ai = 0; ai < ca; ++ai) {
+            const int aa = fa + ai;
+            v += frame[(size_t)(aa * g.NSY + b) * g.FS + frame_index(R - g.TY * b, C - kSW * aa, P, g.TY)];
+        }
+    }
+    const size_t i = (size_t)R * g.m + C;
+    const bool bnd = bc != 2 && (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
+    y[i] = bnd ? (bc == 1 ? x[i] : T(0)) : sign * v;
+}
+
 template <int P, typename T>
 __device__ __forceinline__ void seam_point(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
                                            const StripGrid &g, T sign, int bc, long long idx)
@@ -522,20 +549,41 @@ __device__ __forceinline__ void seam_point(const T *__restrict__ frame, const T 
         const int s = C / kSW;
         if (C % kSW < P && s >= 1 && s < g.NSX) return;   // handled as a vertical seam
     }
-    int fa, fb;
-    const int ca = cover(C, kSW, g.NSX, P, fa);
-    const int cb = cover(R, g.TY, g.NSY, P, fb);
-    T v = 0;
-    for (int bi = 0; bi < cb; ++bi) {
-        const int b = fb + bi;
-        for (int ai = 0; ai < ca; ++ai) {
-            const int aa = fa + ai;
-            v += frame[(size_t)(aa * g.NSY + b) * g.FS + frame_index(R - g.TY * b, C - kSW * aa, P, g.TY)];
+    seam_point_rc<P, T>(frame, x, y, g, sign, bc, R, C);
+}
+
+// The seam points of control-point rows R0 .. R1 - 1, where R0 = TY * s0 is a
+// strip-row boundary: the vertical seams' points in those rows and the
+// horizontal seams TY * s .. TY * s + P - 1 for 1 <= s, s0 <= s, TY * s < R1.
+// Valid once every strip covering those rows has written its frame.
+template <int P, typename T>
+__global__ void seam_fixup_rows_kernel(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
+                                       StripGrid g, T sign, int bc, int R0, int R1)
+{
+    const int s0 = max(R0 / g.TY, 1), s1 = (R1 + g.TY - 1) / g.TY;   // horizontal seams s0 .. s1 - 1
+    const long long nv = (long long)(g.NSX - 1) * P * (R1 - R0);
+    const long long nh = (long long)max(0, min(s1, g.NSY) - s0) * P * g.m;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < nv + nh;
+         idx += (long long)gridDim.x * blockDim.x) {
+        int R, C;
+        if (idx < nv) {   // seam by seam, row by row, its P columns fastest
+            const long long per = (long long)(R1 - R0) * P;
+            const int cg = (int)(idx / per);
+            const int rem = (int)(idx - cg * per);
+            R = R0 + rem / P;
+            C = kSW * (1 + cg) + rem % P;
+            if (C >= g.m) continue;
+        } else {
+            const long long j = idx - nv;
+            C = (int)(j % g.m);
+            const int rid = (int)(j / g.m);
+            R = g.TY * (s0 + rid / P) + rid % P;
+            if (R >= R1 || R >= g.n) continue;
+            const int s = C / kSW;
+            if (C % kSW < P && s >= 1 && s < g.NSX) continue;   // a vertical seam's point
         }
+        seam_point_rc<P, T>(frame, x, y, g, sign, bc, R, C);
     }
-    const size_t i = (size_t)R * g.m + C;
-    const bool bnd = bc != 2 && (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
-    y[i] = bnd ? (bc == 1 ? x[i] : T(0)) : sign * v;
 }
 
 __host__ __device__ __forceinline__ long long seam_count(const StripGrid &g)

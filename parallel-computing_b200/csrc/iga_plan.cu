@@ -294,8 +294,15 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
     return IGA_OK;
 }
 
+// Win: a window of strip rows (gyn >= 0: strip rows gy0 .. gy0 + gyn - 1, and
+// the seams of control-point rows R0 .. R1 - 1 instead of all seams).
+struct Win {
+    int gy0 = 0, gyn = -1, R0 = 0, R1 = 0;
+};
+
 template <int P, typename T, int GEOM, int NST>
-static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s, int sign, int bc)
+static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s, int sign, int bc,
+                          Win win = Win())
 {
     ApplyParams<T> a;
     a.x = x;
@@ -320,36 +327,50 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
         attr_set = true;
     }
     const StripGrid &g = op.grid;
-    const long long nstrips = (long long)g.NSX * g.NSY;
-    dim3 grid = apply_txreg<P, T, GEOM>() ? dim3((unsigned)((nstrips + W - 1) / W)) : dim3(g.NSX, (g.NSY + W - 1) / W);
+    const int rows = win.gyn >= 0 ? std::min(win.gyn, g.NSY - win.gy0) : g.NSY;
+    if (win.gyn >= 0) {
+        a.gy0 = win.gy0;
+        a.gyn = rows;
+    }
+    const long long nstrips = (long long)g.NSX * rows;
+    dim3 grid = apply_txreg<P, T, GEOM>() ? dim3((unsigned)((nstrips + W - 1) / W)) : dim3(g.NSX, (rows + W - 1) / W);
     dim3 block(32, W);
-    kern<<<grid, block, smem, s>>>(a);
-    const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
-    if (nseam > 0) {
-        const int blocks = (int)std::min<long long>((nseam + 255) / 256, 4 * 148);
-        seam_fixup_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)sign, bc);
+    if (rows > 0) kern<<<grid, block, smem, s>>>(a);
+    if (win.gyn < 0) {
+        const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
+        if (nseam > 0) {
+            const int blocks = (int)std::min<long long>((nseam + 255) / 256, 4 * 148);
+            seam_fixup_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)sign, bc);
+        }
+    } else if (win.R1 > win.R0) {
+        const long long nseam = (long long)(g.NSX - 1) * P * (win.R1 - win.R0) + (long long)2 * P * g.m * (rows + 1);
+        const int blocks = (int)std::max<long long>(1, std::min<long long>((nseam + 255) / 256, 4 * 148));
+        seam_fixup_rows_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)sign, bc, win.R0,
+                                                             win.R1);
     }
     IGA_CUDA_TRY(cudaGetLastError());
     return IGA_OK;
 }
 
 template <int P, typename T>
-static int launch_apply_p(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s, int sign, int bc)
+static int launch_apply_p(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s, int sign, int bc,
+                          Win win = Win())
 {
     constexpr int NST = apply_stages<P, T>();
-    if (pl->geometry == IGA_GEOM_PRECOMPUTED) return launch_apply_t<P, T, 0, NST>(pl, op, x, y, s, sign, bc);
-    return launch_apply_t<P, T, 1, NST>(pl, op, x, y, s, sign, bc);
+    if (pl->geometry == IGA_GEOM_PRECOMPUTED) return launch_apply_t<P, T, 0, NST>(pl, op, x, y, s, sign, bc, win);
+    return launch_apply_t<P, T, 1, NST>(pl, op, x, y, s, sign, bc, win);
 }
 
 template <typename T>
-static int launch_apply(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s, int sign, int bc)
+static int launch_apply(iga_plan *pl, const OperatorData &op, const T *x, T *y, cudaStream_t s, int sign, int bc,
+                        Win win = Win())
 {
     switch (pl->p) {
-    case 1: return launch_apply_p<1, T>(pl, op, x, y, s, sign, bc);
-    case 2: return launch_apply_p<2, T>(pl, op, x, y, s, sign, bc);
-    case 3: return launch_apply_p<3, T>(pl, op, x, y, s, sign, bc);
-    case 4: return launch_apply_p<4, T>(pl, op, x, y, s, sign, bc);
-    case 5: return launch_apply_p<5, T>(pl, op, x, y, s, sign, bc);
+    case 1: return launch_apply_p<1, T>(pl, op, x, y, s, sign, bc, win);
+    case 2: return launch_apply_p<2, T>(pl, op, x, y, s, sign, bc, win);
+    case 3: return launch_apply_p<3, T>(pl, op, x, y, s, sign, bc, win);
+    case 4: return launch_apply_p<4, T>(pl, op, x, y, s, sign, bc, win);
+    case 5: return launch_apply_p<5, T>(pl, op, x, y, s, sign, bc, win);
     default: return IGA_ERR_UNSUPPORTED;
     }
 }
@@ -590,6 +611,12 @@ int iga_plan_destroy(iga_plan *pl)
                     (void *)pl->h_stage_x, (void *)pl->d_stage_x, (void *)pl->d_stage_y})
         if (p) cudaFree(p);
     if (pl->h_pinned) cudaFreeHost(pl->h_pinned);
+    for (cudaStream_t hs : pl->host_st)
+        if (hs) cudaStreamDestroy(hs);
+    for (auto &row : pl->host_ev)
+        for (cudaEvent_t e : row)
+            if (e) cudaEventDestroy(e);
+    if (pl->host_ev0) cudaEventDestroy(pl->host_ev0);
     iga_solver_release(pl);
     delete pl;
     return IGA_OK;
@@ -658,6 +685,16 @@ int iga_apply_prec(iga_plan *pl, int prec, const void *x, void *y, void *stream)
     return iga_apply_internal(pl, prec, x, y, (cudaStream_t)stream);
 }
 
+// Host buffers: the patch is applied in up to kHostSlabs slabs of strip rows
+// (about one wave of strips each),
+// so that the upload of x, the kernels and the download of y overlap on three
+// streams (PCIe carries both directions at once). Slab k needs the x rows
+// its strips touch (up to P rows past its last element row); after its strips
+// and the seams of its control-point rows (those shared with slab k - 1
+// included) its y rows are final and go back while slab k + 1 computes. Each
+// point is computed exactly as by iga_apply: the result is bitwise the same.
+constexpr int kHostSlabs = 8;
+
 int iga_apply_host(iga_plan *pl, const double *xh, double *yh)
 {
     if (!pl || !xh || !yh || !pl->op64.ready) return IGA_ERR_ARG;
@@ -667,11 +704,52 @@ int iga_apply_host(iga_plan *pl, const double *xh, double *yh)
         IGA_CUDA_TRY(cudaMalloc((void **)&pl->d_stage_x, bytes));
         IGA_CUDA_TRY(cudaMalloc((void **)&pl->d_stage_y, bytes));
     }
-    IGA_CUDA_TRY(cudaMemcpyAsync(pl->d_stage_x, xh, bytes, cudaMemcpyHostToDevice, 0));
-    int st = iga_apply_internal(pl, IGA_FP64, pl->d_stage_x, pl->d_stage_y, 0);
-    if (st) return st;
-    IGA_CUDA_TRY(cudaMemcpyAsync(yh, pl->d_stage_y, bytes, cudaMemcpyDeviceToHost, 0));
-    IGA_CUDA_TRY(cudaStreamSynchronize(0));
+    if (!pl->host_st[0]) {
+        for (int k = 0; k < 3; ++k) IGA_CUDA_TRY(cudaStreamCreateWithFlags(&pl->host_st[k], cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k)
+            for (int i = 0; i < kHostSlabs; ++i)
+                IGA_CUDA_TRY(cudaEventCreateWithFlags(&pl->host_ev[k][i], cudaEventDisableTiming));
+        IGA_CUDA_TRY(cudaEventCreateWithFlags(&pl->host_ev0, cudaEventDisableTiming));
+    }
+    cudaStream_t sin = pl->host_st[0], scmp = pl->host_st[1], sout = pl->host_st[2];
+    // after the caller's work on the legacy stream
+    IGA_CUDA_TRY(cudaEventRecord(pl->host_ev0, 0));
+    for (int k = 0; k < 3; ++k) IGA_CUDA_TRY(cudaStreamWaitEvent(pl->host_st[k], pl->host_ev0, 0));
+    const StripGrid &g = pl->op64.grid;
+    // slabs of about one wave of strips each (fewer strips leave SMs idle)
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, pl->device);
+    const long long wave = (long long)nsm * pl->op64.warps;
+    const int K = (int)std::max<long long>(1, std::min<long long>({(long long)kHostSlabs, (long long)g.NSY,
+                                                                    ((long long)g.NSX * g.NSY + wave / 2) / wave}));
+    const int m = g.m, n = g.n, P = g.P;
+    int in_rows = 0;   // x rows uploaded so far
+    for (int k = 0; k < K; ++k) {
+        const int gA = (int)((long long)g.NSY * k / K), gB = (int)((long long)g.NSY * (k + 1) / K);
+        const int R0 = g.TY * gA, R1 = k + 1 == K ? n : g.TY * gB;
+        const int need = k + 1 == K ? n : std::min(n, g.TY * gB + P);
+        if (need > in_rows) {
+            const size_t o = (size_t)in_rows * m, c = (size_t)(need - in_rows) * m;
+            IGA_CUDA_TRY(cudaMemcpyAsync(pl->d_stage_x + o, xh + o, c * sizeof(double), cudaMemcpyHostToDevice, sin));
+            in_rows = need;
+        }
+        IGA_CUDA_TRY(cudaEventRecord(pl->host_ev[0][k], sin));
+        IGA_CUDA_TRY(cudaStreamWaitEvent(scmp, pl->host_ev[0][k], 0));
+        Win w;
+        w.gy0 = gA;
+        w.gyn = gB - gA;
+        w.R0 = R0;
+        w.R1 = R1;
+        const int st = launch_apply<double>(pl, pl->op64, pl->d_stage_x, pl->d_stage_y, scmp, pl->sign, pl->bc, w);
+        if (st) return st;
+        IGA_CUDA_TRY(cudaEventRecord(pl->host_ev[1][k], scmp));
+        IGA_CUDA_TRY(cudaStreamWaitEvent(sout, pl->host_ev[1][k], 0));
+        if (R1 > R0) {
+            const size_t o = (size_t)R0 * m, c = (size_t)(R1 - R0) * m;
+            IGA_CUDA_TRY(cudaMemcpyAsync(yh + o, pl->d_stage_y + o, c * sizeof(double), cudaMemcpyDeviceToHost, sout));
+        }
+    }
+    IGA_CUDA_TRY(cudaStreamSynchronize(sout));
     return iga_check_error_flag(pl);
 }
 

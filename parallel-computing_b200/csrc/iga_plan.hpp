@@ -49,6 +49,11 @@ struct iga_plan {
     double *kappa_dev = nullptr;   // coefficient at the quadrature points (null: 1)
     int kappa_version = 0;         // bumped by every change of kappa
     double *h_stage_x = nullptr, *d_stage_x = nullptr, *d_stage_y = nullptr;
+    // iga_apply_host's pipeline: copy-in, compute and copy-out streams, one
+    // event per slab and stage, and the start event
+    cudaStream_t host_st[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t host_ev[2][16] = {};
+    cudaEvent_t host_ev0 = nullptr;
     void *h_pinned = nullptr;
     iga::SolverState *solver = nullptr;
 };

@@ -114,11 +114,19 @@ def test_bitwise_reproducible(torch_cuda, ib, geom):
     assert torch.equal(ys[0], ys[1]) and torch.equal(ys[0], ys[2])
 
 
-def test_host_buffer_apply_equals_device_apply(torch_cuda, ib):
-    M = ib.unit_square(3, 64, 64)
-    plan = ib.Plan(M)
+@pytest.mark.parametrize("p,nex,ney,geom,bc,ty", [(3, 64, 64, 0, 0, 0), (3, 200, 150, 0, 0, 0), (2, 90, 333, 0, 1, 0),
+                                                  (4, 70, 45, 0, 0, 0), (3, 48, 200, 1, 0, 0), (3, 40, 37, 0, 1, 37),
+                                                  (2, 33, 500, 1, 2, 16)])
+def test_host_buffer_apply_equals_device_apply(torch_cuda, ib, p, nex, ney, geom, bc, ty):
+    """iga_apply_host uploads x, applies and downloads y slab by slab on three
+    streams; every point is computed as by the device apply: bitwise equal,
+    for either geometry mode, every boundary rule and one-slab patches."""
+    M = distorted(ib.unit_square(p, nex, ney))
+    plan = ib.Plan(M, geometry=geom, bc=bc, rows_per_strip=ty)
     x = splitmix_uniform(6, -1.0, 1.0, plan.nfunc)
-    assert np.array_equal(plan.apply_host(x), run(torch_cuda, plan, x))
+    ref = run(torch_cuda, plan, x)
+    assert np.array_equal(plan.apply_host(x), ref)
+    assert np.array_equal(plan.apply_host(x), ref)   # the pipeline's streams and events reused
 
 
 def test_reference_shaped_entry_point(torch_cuda, ib, gold):
