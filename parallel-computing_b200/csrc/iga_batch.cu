@@ -182,7 +182,9 @@ __global__ void __launch_bounds__(kBT) bk_res64(BDev d, int *__restrict__ act64,
     }
 }
 
-// Mixed sweep start: r32 = r64 / ||r64||, x32 = 0, rr; tol2 = sweep_rtol^2 rr.
+// Mixed sweep start: r32 = r64 / ||r64||, x32 = 0, rr; tol2 = t^2 rr with t =
+// sweep_rtol, or less reduction when less is left: a fifth of what would
+// reach rtol (margin for the FP32 recurrence residual's drift).
 __global__ void __launch_bounds__(kBT) bk_sweep_init(BDev d, const int *__restrict__ act64, int *__restrict__ act,
                                                      const double *__restrict__ r64, float *__restrict__ r32,
                                                      float *__restrict__ x32)
@@ -205,7 +207,9 @@ __global__ void __launch_bounds__(kBT) bk_sweep_init(BDev d, const int *__restri
     if (chunk_reduce<1>(v, pr, d, tot) && threadIdx.x == 0) {
         BScal &S = d.sc[pr];
         S.rr = tot[0];
-        S.tol2 = d.cfg->sweep_rtol2 * tot[0];
+        const double need = sc > 0.0 ? d.cfg->rtol * sqrt(S.bb) / sc : 0.0;
+        const double t = fmax(sqrt(d.cfg->sweep_rtol2), fmin(0.2 * need, 0.5));
+        S.tol2 = t * t * tot[0];
         S.it = 0;
         act[pr] = (isfinite(tot[0]) && tot[0] > S.tol2) ? 1 : 0;
     }
