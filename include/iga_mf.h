@@ -135,7 +135,11 @@ int iga_apply(iga_plan *plan, const void *x_dev, void *y_dev, void *stream);
 /* Same, choosing the operator precision of a MIXED plan explicitly. */
 int iga_apply_prec(iga_plan *plan, int precision, const void *x_dev, void *y_dev, void *stream);
 /* Host-buffer MatMult (the MATSHELL callback on host vectors): copies x in,
- * applies the FP64 operator, copies y out, and synchronises. */
+ * applies the FP64 operator, copies y out, and synchronises. The patch goes
+ * through in slabs of strip rows on the plan's own streams, so that the
+ * copies in both directions overlap the kernels (pinned host buffers give
+ * the overlap; pageable ones work, slower). Ordered after prior work on the
+ * legacy default stream; the result is bitwise that of iga_apply. */
 int iga_apply_host(iga_plan *plan, const double *x_host, double *y_host);
 
 /* Load vector F = int R f with F[Dir] = 0 (GlobalAssemblyMF::AssemLoad,
