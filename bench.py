@@ -579,6 +579,11 @@ def our_arm(args):
         rate, kind, threads, t = cpu_reference_apply_rate(256, 3, os.cpu_count() or 1)
         cpu = {"value": rate, "unit": "GDOF/s", "cores": threads, "kind": kind,
                "sample": f"p=3 256x256-element patch ({259 ** 2} DOFs), median of 3 MatMults ({t:.3f} s each)"}
+        # the same element code on one core (the reference's per-rank rate)
+        rate1, kind1, _, t1 = cpu_reference_apply_rate(128, 3, 1)
+        cpu["one_core"] = {"value": rate1, "unit": "GDOF/s", "cores": 1, "kind": kind1,
+                           "sample": f"p=3 128x128-element patch ({131 ** 2} DOFs), median of 3 MatMults "
+                                     f"({t1:.3f} s each)"}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "GDOF/s", "n_gpus": ws, "steps": args.steps,
