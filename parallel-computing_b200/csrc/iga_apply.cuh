@@ -186,8 +186,10 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         if (k < nrows && lane < kSW + P) {
             const int R = ey0 + k, C = ex0 + lane;
             const bool v = R < g.n && C < g.m;
+            // IGA_BC_IDENTITY: boundary entries of x enter the operator as zero
+            const bool xb = a.bc == 1 && (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
             const size_t gi = v ? (size_t)R * g.m + C : 0;
-            cp_async_zfill<sizeof(T)>(xr + (k % S::XR) * S::XW + lane, x + gi, v);
+            cp_async_zfill<sizeof(T)>(xr + (k % S::XR) * S::XW + lane, x + gi, v && !xb);
             if (GEOM == 1) cp_async_zfill<2 * sizeof(T)>(cr + ((k % S::XR) * S::XW + lane) * 2, a.CP + 2 * gi, v);
         }
         if (k >= P && k < nrows) {   // 16-byte copies (rows are whole 16-byte words)
@@ -218,12 +220,6 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         if constexpr (TXREG) return txr[kind][j][il];
         else return tabXs[((kind * QH + j) * NB + il) * 32 + lane];
     };
-    unsigned colmask = 0;   // IGA_BC_IDENTITY: bit il set if column ex+il is a boundary column
-    if (a.bc == 1)
-        for (int il = 0; il <= P; ++il) {
-            const int C = ex + il;
-            if (C == 0 || C == g.m - 1) colmask |= 1u << il;
-        }
 
     T xs0[NB][QH], xs1[NB][QH];     // x contracted with value / derivative tables, rows ey..ey+P
     T acc0[NB][QH], acc1[NB][QH];   // y-transposed partial sums for control-point rows ey..ey+P
@@ -233,11 +229,9 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         cp_async_wait<D - 1>();
         __syncwarp();
         const T *src = xr + (k % S::XR) * S::XW;
-        const int R = ey0 + k;
-        const bool rowb = (a.bc == 1) && (R == 0 || R == g.n - 1);
         T xv[NB];
 #pragma unroll
-        for (int il = 0; il < NB; ++il) xv[il] = (rowb || (colmask >> il) & 1u) ? T(0) : src[c + il];
+        for (int il = 0; il < NB; ++il) xv[il] = src[c + il];
         T px[NB], py[NB];
         if constexpr (GEOM == 1) {
             const T *cp = cr + (k % S::XR) * S::XW * 2;
@@ -377,7 +371,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
                 }
                 T g00 = 0, g01 = 0, g11 = 0;
                 if constexpr (GEOM == 0) {
-                    if (qx < NQ) {
+                    if ((NQ % 2 == 0 || j + 1 < QH) || qx < NQ) {   // only h = 1's last slot can lie past NQ
                         const T *gp = Gst + ((qy * NQ + qx) * 3) * kSW + c;
                         g00 = gp[0];
                         g01 = gp[kSW];
