@@ -339,69 +339,88 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
             }
         }
         const T *ty = yr + ((s + P) % S::XR) * S::TYW;   // landed with x row s + P
+        // y tables (value n2, derivative d2) of quadrature row qy
+        auto load_tab = [&](int qy, T (&n2)[NB], T (&d2)[NB]) {
+            // rows of NBP entries, 16-byte aligned in the ring: vector loads
+            constexpr int V = 16 / sizeof(T), NBP = S::NBP;
+            using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+            const VT *va = reinterpret_cast<const VT *>(ty + qy * NBP);
+            const VT *vb = reinterpret_cast<const VT *>(ty + (NQ + qy) * NBP);
 #pragma unroll
-        for (int qy = 0; qy < NQ; ++qy) {
-            T n2[NB], d2[NB];
-            {   // rows of NBP entries, 16-byte aligned in the ring: vector loads
-                constexpr int V = 16 / sizeof(T), NBP = S::NBP;
-                using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
-                const VT *va = reinterpret_cast<const VT *>(ty + qy * NBP);
-                const VT *vb = reinterpret_cast<const VT *>(ty + (NQ + qy) * NBP);
+            for (int v = 0; v < NBP / V; ++v) {
+                const VT ua = va[v], ub = vb[v];
+                const T *pa = reinterpret_cast<const T *>(&ua), *pb = reinterpret_cast<const T *>(&ub);
 #pragma unroll
-                for (int v = 0; v < NBP / V; ++v) {
-                    const VT ua = va[v], ub = vb[v];
-                    const T *pa = reinterpret_cast<const T *>(&ua), *pb = reinterpret_cast<const T *>(&ub);
-#pragma unroll
-                    for (int e = 0; e < V; ++e) {
-                        if (v * V + e < NB) {
-                            n2[v * V + e] = pa[e];
-                            d2[v * V + e] = pb[e];
-                        }
+                for (int e = 0; e < V; ++e) {
+                    if (v * V + e < NB) {
+                        n2[v * V + e] = pa[e];
+                        d2[v * V + e] = pb[e];
                     }
                 }
             }
+        };
+        // quadrature point (qy, qx) in slot j: gradient of u, times G, back
+        // onto the slot's y-transposed partial sums (valid false: adds zero)
+        auto qpoint = [&](int qy, int qx, int j, bool valid, const T (&n2)[NB], const T (&d2)[NB]) {
+            T uxi = 0, ueta = 0;
 #pragma unroll
-            for (int j = 0; j < QH; ++j) {
-                const int qx = h * QH + j;
-                T uxi = 0, ueta = 0;
+            for (int jl = 0; jl < NB; ++jl) {
+                uxi = fma(n2[jl], xs1[jl][j], uxi);
+                ueta = fma(d2[jl], xs0[jl][j], ueta);
+            }
+            T g00 = 0, g01 = 0, g11 = 0;
+            if constexpr (GEOM == 0) {
+                if (valid) {
+                    const T *gp = Gst + ((qy * NQ + qx) * 3) * kSW + c;
+                    g00 = gp[0];
+                    g01 = gp[kSW];
+                    g11 = gp[2 * kSW];
+                }
+            } else {
+                T x_xi = 0, x_eta = 0, y_xi = 0, y_eta = 0;
 #pragma unroll
                 for (int jl = 0; jl < NB; ++jl) {
-                    uxi = fma(n2[jl], xs1[jl][j], uxi);
-                    ueta = fma(d2[jl], xs0[jl][j], ueta);
+                    x_xi = fma(n2[jl], cs[0][1][jl][j], x_xi);
+                    x_eta = fma(d2[jl], cs[0][0][jl][j], x_eta);
+                    y_xi = fma(n2[jl], cs[1][1][jl][j], y_xi);
+                    y_eta = fma(d2[jl], cs[1][0][jl][j], y_eta);
                 }
-                T g00 = 0, g01 = 0, g11 = 0;
-                if constexpr (GEOM == 0) {
-                    if ((NQ % 2 == 0 || j + 1 < QH) || qx < NQ) {   // only h = 1's last slot can lie past NQ
-                        const T *gp = Gst + ((qy * NQ + qx) * 3) * kSW + c;
-                        g00 = gp[0];
-                        g01 = gp[kSW];
-                        g11 = gp[2 * kSW];
-                    }
-                } else {
-                    T x_xi = 0, x_eta = 0, y_xi = 0, y_eta = 0;
+                if (valid && ex < g.nex) {
+                    T wgt = a.wq[qy * NQ + qx];
+                    if (a.kappa) wgt *= a.kappa[((size_t)ey * g.nex + ex) * S::NQ2 + qy * NQ + qx];
+                    const T f = wgt * recip(x_xi * y_eta - x_eta * y_xi);
+                    g00 = f * fma(x_eta, x_eta, y_eta * y_eta);
+                    g01 = -f * fma(x_xi, x_eta, y_xi * y_eta);
+                    g11 = f * fma(x_xi, x_xi, y_xi * y_xi);
+                }
+            }
+            const T vxi = fma(g00, uxi, g01 * ueta);
+            const T veta = fma(g01, uxi, g11 * ueta);
 #pragma unroll
-                    for (int jl = 0; jl < NB; ++jl) {
-                        x_xi = fma(n2[jl], cs[0][1][jl][j], x_xi);
-                        x_eta = fma(d2[jl], cs[0][0][jl][j], x_eta);
-                        y_xi = fma(n2[jl], cs[1][1][jl][j], y_xi);
-                        y_eta = fma(d2[jl], cs[1][0][jl][j], y_eta);
-                    }
-                    if (qx < NQ && ex < g.nex) {
-                        T wgt = a.wq[qy * NQ + qx];
-                        if (a.kappa) wgt *= a.kappa[((size_t)ey * g.nex + ex) * S::NQ2 + qy * NQ + qx];
-                        const T f = wgt * recip(x_xi * y_eta - x_eta * y_xi);
-                        g00 = f * fma(x_eta, x_eta, y_eta * y_eta);
-                        g01 = -f * fma(x_xi, x_eta, y_xi * y_eta);
-                        g11 = f * fma(x_xi, x_xi, y_xi * y_xi);
-                    }
-                }
-                const T vxi = fma(g00, uxi, g01 * ueta);
-                const T veta = fma(g01, uxi, g11 * ueta);
+            for (int jl = 0; jl < NB; ++jl) {
+                acc0[jl][j] = fma(n2[jl], vxi, acc0[jl][j]);
+                acc1[jl][j] = fma(d2[jl], veta, acc1[jl][j]);
+            }
+        };
+        constexpr bool MID = mid_shared(NQ);
+        constexpr int QJ = MID ? QH - 1 : QH;   // slots of this lane half's own columns
 #pragma unroll
-                for (int jl = 0; jl < NB; ++jl) {
-                    acc0[jl][j] = fma(n2[jl], vxi, acc0[jl][j]);
-                    acc1[jl][j] = fma(d2[jl], veta, acc1[jl][j]);
-                }
+        for (int qy = 0; qy < NQ; ++qy) {
+            T n2[NB], d2[NB];
+            load_tab(qy, n2, d2);
+#pragma unroll
+            for (int j = 0; j < QJ; ++j) {
+                const int qx = h * QH + j;   // only h = 1's last slot can lie past NQ
+                qpoint(qy, qx, j, (NQ % 2 == 0 || j + 1 < QH) || qx < NQ, n2, d2);
+            }
+        }
+        if constexpr (MID) {   // middle column QH - 1: half h takes rows qy = 2 t + h
+#pragma unroll
+            for (int t = 0; t < QH; ++t) {
+                const int qy = min(2 * t + h, NQ - 1);
+                T n2[NB], d2[NB];
+                load_tab(qy, n2, d2);
+                qpoint(qy, QH - 1, QH - 1, 2 * t + h < NQ, n2, d2);
             }
         }
         if (GEOM == 0) {
