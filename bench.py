@@ -460,6 +460,23 @@ def our_arm(args):
             dist.destroy_process_group()
         return
 
+    if args.profile_annulus:
+        # the operators of the mixed-precision solve (p=4 NURBS quarter annulus,
+        # 1024x1024): FP32 (the sweeps) and FP64 (the outer residual), a few
+        # applies outside any graph
+        plan = ib.Plan(ib.quarter_annulus(4, 1024), precision=ib.MIXED)
+        x = torch.from_numpy(splitmix_uniform(SEED, -1.0, 1.0, plan.nfunc)).cuda()
+        y = torch.empty_like(x)
+        x32, y32 = x.float(), torch.empty_like(x, dtype=torch.float32)
+        for _ in range(4):
+            plan.apply(x32, y32, precision=ib.FP32)
+            plan.apply(x, y, precision=ib.FP64)
+        torch.cuda.synchronize()
+        plan.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
     if args.batch_only:
         res = time_batch(ib, torch, torch.cuda.current_stream(), barrier, max_over_ranks)
         if rank == 0:
@@ -625,6 +642,9 @@ def main():
     ap.add_argument("--profile-pc", action="store_true",
                     help="run the exact FEM preconditioner (FP32, FP64) and the FP32 operator of the p=3 patch "
                          "(--ne) a few times outside any graph (a target for ncu; prints nothing else)")
+    ap.add_argument("--profile-annulus", action="store_true",
+                    help="run the FP32 and FP64 operators of the p=4 1024x1024 NURBS annulus a few times "
+                         "outside any graph (a target for ncu; prints nothing else)")
     ap.add_argument("--profile-batch-pc", action="store_true",
                     help="run the batched preconditioner and operator of the 256-problem batch a few times "
                          "outside any graph (a target for ncu; prints nothing else)")
