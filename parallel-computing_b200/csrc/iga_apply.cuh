@@ -402,7 +402,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
                 acc1[jl][j] = fma(d2[jl], veta, acc1[jl][j]);
             }
         };
-        constexpr bool MID = mid_shared(NQ);
+        constexpr bool MID = mid_shared(NQ, (int)sizeof(T));
         constexpr int QJ = MID ? QH - 1 : QH;   // slots of this lane half's own columns
 #pragma unroll
         for (int qy = 0; qy < NQ; ++qy) {

@@ -97,19 +97,20 @@ __host__ __device__ constexpr int tab_nbp(int NB, int esz)
 // Element columns per warp strip (two lanes per element column).
 constexpr int kSW = 16;
 
-// Whether the two lane halves share the middle quadrature column: odd NQ
-// from 5 up (at NQ = 3 the split's extra table loads cost more than the
-// idle slot: p=2 2048^2 FP64 185 -> 192 us; at NQ = 5 it saves 2 of 15
-// quadrature points per lane and element row: p=4 FP32 82 -> 75 us).
-__host__ __device__ constexpr bool mid_shared(int NQ) { return NQ % 2 == 1 && NQ >= 5; }
+// Whether the two lane halves share the middle quadrature column (odd NQ;
+// esz = bytes per value): at NQ = 5 it saves 2 of 15 quadrature points per
+// lane and element row (p=4 FP32 82 -> 75 us at 1024^2); at NQ = 3 it pays in
+// FP32 (p=2 2048^2 153 -> 150 us) but not in FP64, where the split's extra
+// table loads cost more than the idle slot (185 -> 192 us).
+__host__ __device__ constexpr bool mid_shared(int NQ, int esz) { return NQ % 2 == 1 && (NQ >= 5 || esz == 4); }
 
 // Quadrature column of x-table slot j (j < QH = ceil(NQ / 2)) of the lane
-// half h: h QH + j (past NQ: an idle slot); where mid_shared(NQ) the last
+// half h: h QH + j (past NQ: an idle slot); where mid_shared(NQ, esz) the last
 // slot of both halves is the middle column QH - 1 instead, whose quadrature
 // rows the two halves split (h takes qy = h, h + 2, ...).
-__host__ __device__ constexpr int lane_qx(int NQ, int h, int j)
+__host__ __device__ constexpr int lane_qx(int NQ, int esz, int h, int j)
 {
-    return (mid_shared(NQ) && j == (NQ + 1) / 2 - 1) ? j : h * ((NQ + 1) / 2) + j;
+    return (mid_shared(NQ, esz) && j == (NQ + 1) / 2 - 1) ? j : h * ((NQ + 1) / 2) + j;
 }
 
 // The element grid is cut into warp strips of kSW element columns by TY

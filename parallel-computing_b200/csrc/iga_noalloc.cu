@@ -67,7 +67,7 @@ __global__ void noalloc_tables_kernel(double *__restrict__ tabX, double *__restr
     const long long tid0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (tid0 == 0) *err = 0;
     for (long long t = tid0; t < nX + nY + NQ * NQ; t += (long long)gridDim.x * blockDim.x) {
-        if (t < nX) {   // [gx][kind][j][il][lane]: lane 2c+h = column 16 gx + c, qx = lane_qx(NQ, h, j)
+        if (t < nX) {   // [gx][kind][j][il][lane]: lane 2c+h = column 16 gx + c, qx = lane_qx(NQ, 8, h, j)
             const int lane = (int)(t % 32);
             long long r = t / 32;
             const int il = (int)(r % NB);
@@ -76,7 +76,7 @@ __global__ void noalloc_tables_kernel(double *__restrict__ tabX, double *__restr
             r /= QH;
             const int kind = (int)(r % 2);
             const int gx = (int)(r / 2);
-            const int ex = iga::kSW * gx + lane / 2, qx = iga::lane_qx(NQ, lane % 2, j);
+            const int ex = iga::kSW * gx + lane / 2, qx = iga::lane_qx(NQ, 8, lane % 2, j);
             double v = 0.0;
             if (ex < nex && qx < NQ) {
                 const double *Ce = C1 + (size_t)ex * NB * NB + il * NB;

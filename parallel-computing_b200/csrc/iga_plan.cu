@@ -238,7 +238,7 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
     const int p = P.p, NB = p + 1, NQ = p + 1, NQ2 = NQ * NQ;
     const StripGrid &g = op.grid;
     // x tables regrouped per column strip: [gx][kind][j][il][lane], lane = 2c + h
-    // holding element column 16 gx + c at quadrature column lane_qx(NQ, h, j).
+    // holding element column 16 gx + c at quadrature column lane_qx(NQ, sizeof(T), h, j).
     const int QH = (NQ + 1) / 2;
     std::vector<T> hx((size_t)g.NSX * 2 * QH * NB * 32, T(0));
     for (int gx = 0; gx < g.NSX; ++gx)
@@ -246,7 +246,7 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
             for (int j = 0; j < QH; ++j)
                 for (int il = 0; il < NB; ++il)
                     for (int lane = 0; lane < 32; ++lane) {
-                        const int ex = kSW * gx + lane / 2, qx = lane_qx(NQ, lane % 2, j);
+                        const int ex = kSW * gx + lane / 2, qx = lane_qx(NQ, (int)sizeof(T), lane % 2, j);
                         double v = 0.0;
                         if (ex < P.nex && qx < NQ) v = (kind ? tx.der : tx.val)[((size_t)ex * NQ + qx) * NB + il];
                         hx[((((size_t)gx * 2 + kind) * QH + j) * NB + il) * 32 + lane] = (T)v;
