@@ -112,6 +112,13 @@ int iga_adjoint_grad(iga_plan *plan, const double *u_dev, const double *lambda_d
  * abscissae of the IGA knot vector. */
 int iga_fem_nodes(const iga_plan *plan, double *gx, double *gy);
 
+/* The same 1-D nodes without a plan (host only): ne + p coordinates of a
+ * direction with ne elements of degree p and net length L (the mean polyline
+ * length of the control net in that direction; L on an axis-aligned patch of
+ * length L), for callers that hold only part of a patch (the partitioned
+ * FEM matrix of a multi-rank preconditioner). */
+int iga_fem_nodes_1d(int p, int ne, double L, double *g);
+
 /* Extreme eigenvalues of the SPD operator K (pc = IGA_PC_NONE) or of the
  * preconditioned M^-1 K (pc = IGA_PC_FEM_EXACT or IGA_PC_FEM_CG) on the free
  * control points, from `steps` Lanczos steps: the coefficients of a standard

@@ -1542,6 +1542,14 @@ int iga_fem_nodes(const iga_plan *pl, double *gx, double *gy)
     return IGA_OK;
 }
 
+int iga_fem_nodes_1d(int p, int ne, double L, double *g)
+{
+    if (!g || p < 1 || p > 5 || ne < 1 || !(L > 0.0)) return IGA_ERR_ARG;
+    const std::vector<double> a = fem_nodes_1d(p, ne, L);
+    std::memcpy(g, a.data(), a.size() * sizeof(double));
+    return IGA_OK;
+}
+
 int iga_pc_apply(iga_plan *pl, int pc, int prec, const void *r, void *z, double pc_rtol, int pc_max_it,
                  void *stream)
 {

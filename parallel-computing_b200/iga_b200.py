@@ -113,6 +113,7 @@ SIGNATURES = [
     ("iga_fem_apply", ctypes.c_int, [VP, ctypes.c_int, VP, VP, VP]),
     ("iga_fem_assemble_csr", ctypes.c_int, [VP, ctypes.c_int, VP, VP, VP, ctypes.POINTER(ctypes.c_int64), VP]),
     ("iga_fem_nodes", ctypes.c_int, [VP, VP, VP]),
+    ("iga_fem_nodes_1d", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_double, VP]),
     ("iga_pc_apply", ctypes.c_int, [VP, ctypes.c_int, ctypes.c_int, VP, VP, ctypes.c_double, ctypes.c_int, VP]),
     ("iga_plan_set_kappa", ctypes.c_int, [VP, VP, VP]),
     ("iga_adjoint_grad", ctypes.c_int, [VP, VP, VP, VP, VP]),
@@ -187,6 +188,14 @@ def _stream(stream):
     if isinstance(stream, int):
         return stream
     return stream.cuda_stream
+
+
+def fem_nodes_1d(p, ne, L):
+    """ne + p node coordinates of one direction of the FEM preconditioner grid
+    (iga_fem_nodes_1d; host only)."""
+    g = np.empty(ne + p, dtype=np.float64)
+    _check(_lib().iga_fem_nodes_1d(p, ne, float(L), g.ctypes.data_as(VP)), "iga_fem_nodes_1d")
+    return g
 
 
 def unit_square(p, nex, ney=None, Lx=1.0, Ly=1.0):

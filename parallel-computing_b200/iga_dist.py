@@ -19,10 +19,13 @@ The Krylov loop over those ranks (DistPCG) is the reference's KSPSolve across
 MPI ranks (matrix_free/iteration_number_fempc_mf.cpp:193-233 and the
 no-preconditioner driver beside it): flexible PCG on the owned entries, one
 MatMult and two all-reductions per iteration ([p.q], then [r.r, r.z, r.z_old]
-in one call). The preconditioner is either none or BlockFemPC, each rank's
-exact FEM inverse on its own block (a block-Jacobi preconditioner that needs
-no communication); the reference's inner CG on the distributed FEM matrix is
-not reproduced across ranks.
+in one call). The preconditioner is none, BlockFemPC (each rank's exact FEM
+inverse on its own block: a block-Jacobi preconditioner that needs no
+communication) or FemCGPC, the reference's own: an inner Jacobi-preconditioned
+CG to 1e-10 on the FEM matrix distributed over the ranks
+(matrix_free/iteration_number_fempc_mf.cpp:11-17,210-224), one ghost update
+and two all-reductions per inner iteration, its rows those of iga_fem_apply's
+matrix (FemRows).
 """
 import numpy as np
 
@@ -230,6 +233,156 @@ class BlockFemPC:
         z_owned.copy_(self.zb[self.pos])
 
 
+def _fem_1d(g):
+    """Diagonals of the 1-D linear-element stiffness (kd, ko) and mass (md, mo)
+    matrices on nodes g (2-point Gauss, exact), as the device preconditioner
+    builds them."""
+    h = np.diff(g)
+    kd, md = np.zeros(len(g)), np.zeros(len(g))
+    kd[:-1] += 1.0 / h
+    kd[1:] += 1.0 / h
+    md[:-1] += h / 3.0
+    md[1:] += h / 3.0
+    ko, mo = np.zeros(len(g)), np.zeros(len(g))
+    ko[:-1], mo[:-1] = -1.0 / h, h / 6.0
+    return kd, ko, md, mo
+
+
+class FemRows:
+    """The rows a part owns of the patch's FEM preconditioner matrix: bilinear
+    elements on the tensor grid of FEM nodes, K = Kx (x) My + Mx (x) Ky on free
+    rows with the boundary columns dropped, identity rows on the patch
+    boundary (the matrix of iga_fem_apply / iga_fem_assemble_csr, reference
+    matrix_free/src/ElementFEM.cpp:3-117 with the SPD sign). Nine (column,
+    value) pairs per owned entry, columns in the part's local form (owned |
+    ghosts): apply(x_local) needs x_local's ghosts current. gx, gy: the
+    patch's 1-D nodes (default: iga_fem_nodes_1d from the part's info)."""
+
+    def __init__(self, part, device, gx=None, gy=None):
+        import torch
+        i = part.info
+        m, n = i.nElemX + i.p, i.nElemY + i.q
+        if gx is None or gy is None:
+            import iga_b200 as ib
+            gx, gy = ib.fem_nodes_1d(i.p, i.nElemX, i.Lx), ib.fem_nodes_1d(i.q, i.nElemY, i.Ly)
+        gx, gy = np.asarray(gx, dtype=np.float64), np.asarray(gy, dtype=np.float64)
+        if len(gx) != m or len(gy) != n:
+            raise ValueError("FEM node arrays do not match the patch")
+        kd, ko, md, mo = _fem_1d(gx)
+        ld, lo, nd, no = _fem_1d(gy)
+        nl = part.nowned + part.nghost
+        pos = np.empty(nl, dtype=np.int64)
+        pos[part.block_to_local] = np.arange(nl)
+        own = np.arange(part.nowned)
+        bi, bj = pos[own] % i.block_m, pos[own] // i.block_m
+        gi, gj = i.elem_x0 + bi, i.elem_y0 + bj
+        free = (gi > 0) & (gj > 0) & (gi < m - 1) & (gj < n - 1)
+        cols = np.repeat(own[:, None], 9, axis=1)
+        vals = np.zeros((part.nowned, 9))
+        vals[~free, 4] = 1.0
+        gif, gjf = gi[free], gj[free]
+        kx = [ko[gif - 1], kd[gif], ko[gif]]
+        mx = [mo[gif - 1], md[gif], mo[gif]]
+        ky = [lo[gjf - 1], ld[gjf], lo[gjf]]
+        my = [no[gjf - 1], nd[gjf], no[gjf]]
+        for b in range(3):
+            for a in range(3):
+                k = 3 * b + a
+                ii, jj = gif + a - 1, gjf + b - 1
+                use = (ii >= 1) & (ii <= m - 2) & (jj >= 1) & (jj <= n - 2)
+                ci, cj = bi[free] + a - 1, bj[free] + b - 1
+                inside = (ci >= 0) & (ci < i.block_m) & (cj >= 0) & (cj < i.block_n)
+                if np.any(use & ~inside):
+                    raise ValueError("a FEM neighbour of an owned entry lies outside the part's block")
+                c = np.where(use, part.block_to_local[np.clip(cj, 0, i.block_n - 1) * i.block_m
+                                                      + np.clip(ci, 0, i.block_m - 1)], own[free])
+                cols[free, k] = c
+                vals[free, k] = np.where(use, kx[a] * my[b] + mx[a] * ky[b], 0.0)
+        self.cols = torch.as_tensor(cols, device=device)
+        self.vals = torch.as_tensor(vals, device=device)
+        self.diag = self.vals[:, 4].clone()
+
+    def apply(self, x_local, y_owned):
+        """y_owned = the owned rows of K times the local form x_local."""
+        y_owned.copy_((self.vals * x_local[self.cols]).sum(dim=1))
+        return y_owned
+
+
+class FemCGPC:
+    """z = K_fem^-1 r by Jacobi-preconditioned CG to ||res|| <= rtol ||r|| from
+    z = 0 (the reference's PCSHELL: KSPCG + PCJACOBI on the FEM matrix,
+    rtol 1e-10, matrix_free/iteration_number_fempc_mf.cpp:11-17,210-224),
+    over vectors that may be one rank's owned entries. spmv(v, out): out = K v
+    (all ranks together); diag: K's diagonal (owned entries); allreduce(t)
+    sums a small FP64 tensor over the ranks in place. last_iterations: the
+    inner iterations of the last apply."""
+
+    def __init__(self, spmv, diag, allreduce, rtol=1e-10, max_it=10000):
+        self.spmv, self.diag, self.allreduce = spmv, diag, allreduce
+        self.rtol, self.max_it = rtol, max_it
+        self.last_iterations = 0
+
+    def __call__(self, r, z):
+        import torch
+        z.zero_()
+        res = r.clone()
+        w = res / self.diag
+        p = w.clone()
+        q = torch.empty_like(r)
+        d = torch.stack([torch.dot(res, res), torch.dot(res, w)])
+        self.allreduce(d)
+        rr, rz = (float(v) for v in d)
+        tol2 = self.rtol * self.rtol * rr
+        it = 0
+        while rr > tol2 and it < self.max_it:
+            self.spmv(p, q)
+            d = torch.dot(p, q).reshape(1)
+            self.allreduce(d)
+            alpha = rz / float(d[0])
+            z.add_(p, alpha=alpha)
+            res.add_(q, alpha=-alpha)
+            torch.div(res, self.diag, out=w)
+            d = torch.stack([torch.dot(res, res), torch.dot(res, w)])
+            self.allreduce(d)
+            rr, rz_new = (float(v) for v in d)
+            p.mul_(rz_new / rz).add_(w)
+            rz = rz_new
+            it += 1
+        self.last_iterations = it
+        return z
+
+
+def dist_fem_cg_pc(op, rtol=1e-10, max_it=10000, gx=None, gy=None):
+    """FemCGPC over the ranks of op (a DistPartOperator): the FEM rows of op's
+    part, ghost updates through op's exchange, all-reductions on op's group."""
+    fem = FemRows(op.part, op.device, gx, gy)
+    dist = op.dist
+
+    def spmv(v, out):
+        fem.apply(op.forward_update(v), out)
+
+    def allreduce(t):
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return FemCGPC(spmv, fem.diag, allreduce, rtol, max_it)
+
+
+def emulate_fem_cg_pc(parts, device, rtol=1e-10, max_it=10000, gx=None, gy=None):
+    """FemCGPC with every part in one process, on the concatenated owned
+    vectors (partition numbering): each part's rows applied to its local form
+    gathered from the global vector."""
+    import torch
+    fems = [FemRows(pt, device, gx, gy) for pt in parts]
+    ghosts = [torch.as_tensor(pt.ghosts, device=device) for pt in parts]
+    diag = torch.cat([f.diag for f in fems])
+
+    def spmv(v, out):
+        for pt, f, g in zip(parts, fems, ghosts):
+            o = pt.owned_offset
+            x_local = torch.cat([v[o:o + pt.nowned], v[g]])
+            f.apply(x_local, out[o:o + pt.nowned])
+    return FemCGPC(spmv, diag, lambda t: None, rtol, max_it)
+
+
 class DistPCG:
     """Flexible PCG on K x = b over the ranks of a partitioned mesh: op is a
     DistPartOperator whose part was built with sign SPD and bc IDENTITY (so K
@@ -247,18 +400,19 @@ class DistPCG:
         return pcg_solve(self.op.matmult, self.pc, allreduce, b_owned, x_owned, rtol, max_it)
 
 
-def emulate_partitioned_pcg(parts, b_global, pcs=None, local_apply=None, rtol=1e-10, max_it=10000):
+def emulate_partitioned_pcg(parts, b_global, pcs=None, local_apply=None, rtol=1e-10, max_it=10000, pc_global=None):
     """DistPCG with every part in one process (one GPU, or the CPU): the same
     operator, preconditioner and loop on the concatenated owned vectors
-    (partition numbering). pcs: None or one preconditioner per part. Returns
-    (x_global, iterations, relres)."""
+    (partition numbering). pcs: None or one preconditioner per part;
+    pc_global: a preconditioner of the whole vector (emulate_fem_cg_pc)
+    instead. Returns (x_global, iterations, relres)."""
     import torch
     off = [p.owned_offset for p in parts] + [parts[-1].owned_offset + parts[-1].nowned]
 
     def matmult(v, out):
         out.copy_(emulate_partitioned_matmult(parts, v, local_apply=local_apply))
 
-    pc = None
+    pc = pc_global
     if pcs is not None:
         def pc(v, out):
             for k, f in enumerate(pcs):

@@ -123,3 +123,35 @@ def test_partitioned_pcg_matches_single_patch_solve(torch_cuda, ib, orc, tmp_pat
     assert r0 <= 1e-11 and r1 <= 1e-11
     if p == 2:
         assert it1 < it0
+
+
+@pytest.mark.parametrize("p,ne,P", [(2, 96, 2), (3, 90, 3)])
+def test_partitioned_fem_cg_pc_matches_single_patch_fem_cg(torch_cuda, ib, orc, tmp_path, p, ne, P):
+    """The reference's preconditioner across parts (inner Jacobi-CG to 1e-10 on
+    the distributed FEM matrix, iga_dist.FemCGPC) with the part MatMults on
+    the device, all parts emulated on the one GPU: the single-patch solve with
+    IGA_PC_FEM_CG (the same preconditioner on the device), in its iteration
+    count within 2."""
+    torch = torch_cuda
+    from iga_dist import emulate_fem_cg_pc, emulate_partitioned_pcg
+    mesh = unit_square_mesh(orc, p, p, ne, ne)
+    write_partition_files(mesh, P, str(tmp_path))
+    m = ne + p
+    new = torch.from_numpy(partition_numbering(p, p, ne, ne, P)).cuda()
+    b = splitmix_uniform(23, -1.0, 1.0, m * m)
+    mask = np.zeros((m, m), bool)
+    mask[0, :] = mask[-1, :] = mask[:, 0] = mask[:, -1] = True
+    b[mask.ravel()] = 0.0
+    plan = ib.Plan(mesh)
+    bd = torch.from_numpy(b).cuda()
+    xs = torch.zeros_like(bd)
+    st = plan.solve(bd, xs, pc=ib.PC_FEM_CG, rtol=1e-11)
+    b_new = torch.empty_like(bd)
+    b_new[new] = bd
+    parts = parts_of(ib, str(tmp_path), P, sign=ib.SIGN_SPD, bc=ib.BC_IDENTITY)
+    pc = emulate_fem_cg_pc(parts, "cuda:0")
+    x, its, r = emulate_partitioned_pcg(parts, b_new, rtol=1e-11, pc_global=pc)
+    torch.cuda.synchronize()
+    assert r <= 1e-11 and pc.last_iterations > 0
+    assert float((x[new] - xs).norm() / xs.norm()) < 1e-9
+    assert abs(its - st.iterations) <= 2

@@ -267,7 +267,7 @@ def _gloo_pcg_rank(rank, world, port, name, pc, out_dir):
     try:
         from iga_testlib import Oracle
         import iga_b200 as ib
-        from iga_dist import BlockFemPC, DistPartOperator, DistPCG
+        from iga_dist import BlockFemPC, DistPartOperator, DistPCG, dist_fem_cg_pc
         orc = Oracle()
         d = os.path.join(PARTITIONS, name)
         part = ib.Part(os.path.join(d, "info.txt"), ib.partition_filename(os.path.join(d, "part"), rank), rank)
@@ -275,7 +275,10 @@ def _gloo_pcg_rank(rank, world, port, name, pc, out_dir):
         op = DistPartOperator(part, dist, "cpu",
                               local_apply=lambda xl, yl: yl.copy_(torch.from_numpy(
                                   local_oracle_spd(orc, part, sub, xl.numpy()))))
-        prec = BlockFemPC(part, "cpu", local_solve=block_fem_solver(orc, sub)) if pc else None
+        if pc == "femcg":   # the reference's inner CG-Jacobi on the distributed FEM matrix
+            prec = dist_fem_cg_pc(op)
+        else:
+            prec = BlockFemPC(part, "cpu", local_solve=block_fem_solver(orc, sub)) if pc else None
         bp = np.load(os.path.join(out_dir, "b.npy"))
         b_owned = torch.from_numpy(bp[part.owned_offset:part.owned_offset + part.nowned].copy())
         x_owned = torch.empty_like(b_owned)
@@ -287,12 +290,14 @@ def _gloo_pcg_rank(rank, world, port, name, pc, out_dir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("name,pc", [("p3_9x7_2", False), ("p3_9x7_2", True), ("p4_8x11_2", True)])
+@pytest.mark.parametrize("name,pc", [("p3_9x7_2", False), ("p3_9x7_2", True), ("p4_8x11_2", True),
+                                     ("p3_9x7_2", "femcg")])
 def test_gloo_distributed_pcg_matches_serial_solve(ib, orc, name, pc, tmp_path):
     """The multi-rank Krylov loop (one process per part, gloo): ghost updates,
     local element loops, two all-reductions per iteration, optional block FEM
-    preconditioner; the assembled solution equals the serial FP64 solve and
-    every rank agrees on the iteration count."""
+    preconditioner or the reference's distributed inner FEM-CG; the assembled
+    solution equals the serial FP64 solve and every rank agrees on the
+    iteration count."""
     import torch.multiprocessing as mp
     d, p, q, nex, ney, P = case_info(name)
     world = P * P
@@ -369,3 +374,52 @@ def test_emulated_pcg_block_pc_reduces_iterations(ib, orc, tmp_path):
     x0, it0, x1, it1 = emulated_solves(orc, parts, bp)
     assert np.linalg.norm(x1 - x0) / np.linalg.norm(x0) < 1e-9
     assert it1 < 0.6 * it0
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fem_rows_equal_oracle_fem_matrix(ib, orc, name):
+    """The rows each part owns of the FEM preconditioner matrix (nodes from
+    iga_fem_nodes_1d and the part's info), applied to local forms gathered
+    from a global vector: the oracle's assembled FEM matrix-vector product."""
+    import torch
+    from iga_dist import emulate_fem_cg_pc
+    d, p, q, nex, ney, P = case_info(name)
+    parts = open_parts(ib, name)
+    m, n = nex + p, ney + q
+    x = splitmix_uniform(5, -1.0, 1.0, m * n)
+    y_ref = orc.fem_matvec(orc.fem_nodes(p, nex), orc.fem_nodes(q, ney), x)
+    new = partition_numbering(p, q, nex, ney, P)
+    xp = np.empty_like(x)
+    xp[new] = x
+    pc = emulate_fem_cg_pc(parts, "cpu")
+    yp = torch.empty(m * n, dtype=torch.float64)
+    pc.spmv(torch.from_numpy(xp), yp)
+    y = yp.numpy()[new]
+    assert np.linalg.norm(y - y_ref) / np.linalg.norm(y_ref) < 1e-14
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_emulated_pcg_fem_cg_pc_matches_oracle_pcg(ib, orc, name):
+    """All parts in one process with the reference's preconditioner (inner
+    Jacobi-CG to 1e-10 on the distributed FEM matrix): the serial FP64
+    solution, in the iteration count of the oracle's single-patch PCG with
+    the same preconditioner (within 2: its outer loop stops on the true
+    residual)."""
+    import torch
+    from iga_dist import emulate_fem_cg_pc, emulate_partitioned_pcg
+    d, p, q, nex, ney, P = case_info(name)
+    parts = open_parts(ib, name)
+    subs = [pt.mesh() for pt in parts]
+    bp, xp = serial_solution(orc, name)
+
+    def apply(part, xl, yl):
+        yl.copy_(torch.from_numpy(local_oracle_spd(orc, part, subs[part.rank], xl.numpy())))
+    pc = emulate_fem_cg_pc(parts, "cpu")
+    x, its, rel = emulate_partitioned_pcg(parts, torch.from_numpy(bp), local_apply=apply, rtol=1e-11,
+                                          pc_global=pc)
+    assert rel <= 1e-11 and pc.last_iterations > 0
+    assert np.linalg.norm(x.numpy() - xp) / np.linalg.norm(xp) < 1e-9
+    new = partition_numbering(p, q, nex, ney, P)
+    b = bp[new]
+    _, it_ref, _ = orc.pcg(unit_square_mesh(orc, p, q, nex, ney), b, rtol=1e-11, maxit=500)
+    assert it_ref > 0 and abs(its - it_ref) <= 2
