@@ -338,6 +338,8 @@ class FemCGPC:
             self.spmv(p, q)
             d = torch.dot(p, q).reshape(1)
             self.allreduce(d)
+            if not float(d[0]) > 0.0:
+                raise FloatingPointError("inner FEM-CG breakdown: p.Kp <= 0")
             alpha = rz / float(d[0])
             z.add_(p, alpha=alpha)
             res.add_(q, alpha=-alpha)
