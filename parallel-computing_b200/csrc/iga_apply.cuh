@@ -361,7 +361,8 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         };
         // quadrature point (qy, qx) in slot j: gradient of u, times G, back
         // onto the slot's y-transposed partial sums (valid false: adds zero)
-        auto qpoint = [&](int qy, int qx, int j, bool valid, const T (&n2)[NB], const T (&d2)[NB]) {
+        // gv: this lane's G values of row qy (lane-major G), else read here
+        auto qpoint = [&](int qy, int qx, int j, bool valid, const T (&n2)[NB], const T (&d2)[NB], const T *gv) {
             T uxi = 0, ueta = 0;
 #pragma unroll
             for (int jl = 0; jl < NB; ++jl) {
@@ -370,7 +371,11 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
             }
             T g00 = 0, g01 = 0, g11 = 0;
             if constexpr (GEOM == 0) {
-                if (valid) {
+                if constexpr (g_lane_major(NQ)) {
+                    g00 = gv[3 * j];
+                    g01 = gv[3 * j + 1];
+                    g11 = gv[3 * j + 2];
+                } else if (valid) {
                     const T *gp = Gst + ((qy * NQ + qx) * 3) * kSW + c;
                     g00 = gp[0];
                     g01 = gp[kSW];
@@ -408,10 +413,24 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         for (int qy = 0; qy < NQ; ++qy) {
             T n2[NB], d2[NB];
             load_tab(qy, n2, d2);
+            T gv[g_lane_major(NQ) ? 3 * QH : 1];
+            if constexpr (GEOM == 0 && g_lane_major(NQ)) {   // 3 QH contiguous values, widest aligned loads
+                const T *src = Gst + (size_t)(qy * 32 + lane) * (3 * QH);
+                constexpr int BYTES = 3 * QH * (int)sizeof(T);
+                constexpr int VB = BYTES % 16 == 0 ? 16 : BYTES % 8 == 0 ? 8 : (int)sizeof(T);
+                using VT = typename std::conditional<VB == 16, float4, typename std::conditional<VB == 8, float2, T>::type>::type;
+#pragma unroll
+                for (int v = 0; v < BYTES / VB; ++v) {
+                    const VT u = reinterpret_cast<const VT *>(src)[v];
+                    const T *pu = reinterpret_cast<const T *>(&u);
+#pragma unroll
+                    for (int e = 0; e < VB / (int)sizeof(T); ++e) gv[v * (VB / (int)sizeof(T)) + e] = pu[e];
+                }
+            }
 #pragma unroll
             for (int j = 0; j < QJ; ++j) {
                 const int qx = h * QH + j;   // only h = 1's last slot can lie past NQ
-                qpoint(qy, qx, j, (NQ % 2 == 0 || j + 1 < QH) || qx < NQ, n2, d2);
+                qpoint(qy, qx, j, (NQ % 2 == 0 || j + 1 < QH) || qx < NQ, n2, d2, gv);
             }
         }
         if constexpr (MID) {   // middle column QH - 1: half h takes rows qy = 2 t + h
@@ -420,7 +439,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
                 const int qy = min(2 * t + h, NQ - 1);
                 T n2[NB], d2[NB];
                 load_tab(qy, n2, d2);
-                qpoint(qy, QH - 1, QH - 1, 2 * t + h < NQ, n2, d2);
+                qpoint(qy, QH - 1, QH - 1, 2 * t + h < NQ, n2, d2, nullptr);
             }
         }
         if (GEOM == 0) {

@@ -104,6 +104,20 @@ constexpr int kSW = 16;
 // table loads cost more than the idle slot (185 -> 192 us).
 __host__ __device__ constexpr bool mid_shared(int NQ, int esz) { return NQ % 2 == 1 && (NQ >= 5 || esz == 4); }
 
+// Layout of one element-row step of a strip's G (NQ^2 points x 3 values x
+// kSW columns). Even NQ: [qy][lane = 2c + h][j][3], qx = h QH + j, so a lane's
+// values of one quadrature row are contiguous (vector loads); odd NQ:
+// [qy][qx][3][c] (the lane halves do not split the columns evenly).
+__host__ __device__ constexpr bool g_lane_major(int NQ) { return NQ % 2 == 0; }
+__host__ __device__ inline int g_index(int NQ, int qy, int qx, int comp, int c)
+{
+    if (g_lane_major(NQ)) {
+        const int QH = NQ / 2, h = qx / QH, j = qx - h * QH;
+        return ((qy * 32 + 2 * c + h) * QH + j) * 3 + comp;
+    }
+    return ((qy * NQ + qx) * 3 + comp) * kSW + c;
+}
+
 // Quadrature column of x-table slot j (j < QH = ceil(NQ / 2)) of the lane
 // half h: h QH + j (past NQ: an idle slot); where mid_shared(NQ, esz) the last
 // slot of both halves is the middle column QH - 1 instead, whose quadrature

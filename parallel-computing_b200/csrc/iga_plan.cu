@@ -66,10 +66,10 @@ __global__ void geom_setup_kernel(T *__restrict__ G, const double *__restrict__ 
             g01 = -f * (x_xi * x_eta + y_xi * y_eta);
             g11 = f * (x_xi * x_xi + y_xi * y_xi);
         }
-        const size_t base = ((((size_t)gx * g.NSY + gy) * g.TY + s) * NQ2 + qp) * 3 * kSW + c;
-        G[base] = (T)g00;
-        G[base + kSW] = (T)g01;
-        G[base + 2 * kSW] = (T)g11;
+        T *Gs = G + (((size_t)gx * g.NSY + gy) * g.TY + s) * NQ2 * 3 * kSW;
+        Gs[g_index(NQ, qy, qx, 0, c)] = (T)g00;
+        Gs[g_index(NQ, qy, qx, 1, c)] = (T)g01;
+        Gs[g_index(NQ, qy, qx, 2, c)] = (T)g11;
     }
 }
 
