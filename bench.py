@@ -204,7 +204,41 @@ def reference_arm(args):
                       "dofs": (NE + P) ** 2, "reference_path": "matrix_free ElementMF+LocalAssemblyMF (CPU)"},
            "cpu_baseline": {"value": rate, "unit": "GDOF/s", "cores": threads, "kind": kind, "sample": sample},
            "e2e": {"value": rate, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    gk = reference_gpu_kernel_rate(NE, max(1, min(args.steps, 5)))
+    if gk is not None:
+        out["gpu_kernel"] = gk
     print(json.dumps(out), flush=True)
+
+
+def reference_gpu_kernel_rate(ne, reps):
+    """GDOF/s of the reference's own GPU MatMult kernel (matrix_free_gpu/src/
+    mult.cu: one quadrature point per thread, 16-thread CTAs, atomicAdd
+    scatter), compiled for sm_100a into oracle/_ref, on the same p=3 ne^2
+    patch with its tables uploaded once (the reference re-uploads them on
+    every call); None when that library or a GPU is absent."""
+    try:
+        import torch
+    except ImportError:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from iga_testlib import RefGpuKernel
+    if not torch.cuda.is_available() or not RefGpuKernel.available():
+        return None
+    k = RefGpuKernel(ne, ne)
+    x = torch.from_numpy(splitmix_uniform(SEED, -1.0, 1.0, k.N)).cuda()
+    y = torch.empty_like(x)
+    k.apply(x.data_ptr(), y.data_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        k.apply(x.data_ptr(), y.data_ptr())
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    k.close()
+    return {"value": k.N / (ms * 1e-3) / 1e9, "unit": "GDOF/s", "ms_per_step": ms, "steps": reps,
+            "what": f"the reference's MatrixFreeMatMultCUDA kernel (matrix_free_gpu/src/mult.cu) compiled for "
+                    f"sm_100a, p=3 {ne}x{ne} patch, tables uploaded once, y zeroed each call"}
 
 
 def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):

@@ -369,3 +369,58 @@ def write_partition_files(mesh, P, out_dir, base="part"):
                 f.write("CP\n" + dbls(lcp) + "\n")
                 f.write("NURBSExtraction1\n" + dbls(C1[ex0[i] * e1:(ex1[i] + 1) * e1]) + "\n")
                 f.write("NURBSExtraction2\n" + dbls(C2[ey0[j] * e2:(ey1[j] + 1) * e2]) + "\n")
+
+
+REF_CPU_LIB = os.path.join(ROOT, "oracle", "_ref", "libigaref.so")
+REF_GPU_LIB = os.path.join(ROOT, "oracle", "_ref", "libigaref_gpu.so")
+
+
+class RefGpuKernel:
+    """The reference's own GPU MatMult kernel (matrix_free_gpu/src/mult.cu,
+    compiled for sm_100a with P_ORDER = 3 into oracle/_ref/libigaref_gpu.so)
+    on a unit-square p = 3 mesh made by the reference's own preprocessing
+    (ref_mesh / ref_tables of oracle/_ref/libigaref.so), tables uploaded once.
+    apply(x, y) takes device pointers (ints) of N doubles: y = A_ref x with
+    y[Dir] = 0. Test and benchmark infrastructure, a checker and a baseline
+    only."""
+
+    P = 3
+
+    @staticmethod
+    def available():
+        return os.path.exists(REF_GPU_LIB) and os.path.exists(REF_CPU_LIB)
+
+    def __init__(self, nex, ney, Lx=1.0, Ly=1.0):
+        p = self.P
+        cpu = ctypes.CDLL(REF_CPU_LIB)
+        self.L = ctypes.CDLL(REF_GPU_LIB)
+        m, n = nex + p, ney + p
+        nb = (p + 1) ** 2
+        self.N = m * n
+        CP = np.zeros(2 * m * n)
+        IEN = np.zeros(nex * ney * nb, np.int32)
+        ID = np.zeros(m * n, np.int32)
+        Dir = np.zeros(m * n, np.int32)
+        nd = ctypes.c_int()
+        C1, C2 = np.zeros(nex * nb), np.zeros(ney * nb)
+        h1, h2 = np.zeros(nex), np.zeros(ney)
+        cpu.ref_mesh(p, p, nex, ney, ctypes.c_double(Lx), ctypes.c_double(Ly), _p(CP), _p(IEN), _p(ID), _p(Dir),
+                     ctypes.byref(nd), _p(C1), _p(C2), _p(h1), _p(h2))
+        qp, qw = np.zeros(p + 1), np.zeros(p + 1)
+        B, dB = np.zeros(nb), np.zeros(nb)
+        cpu.ref_tables(p, _p(qp), _p(qw), _p(B), _p(dB))
+        h = VP()
+        st = self.L.refgpu_create(p, nex, ney, _p(B), _p(dB), _p(qw), _p(C1), _p(C2), _p(h1), _p(h2), _p(IEN),
+                                  _p(ID), _p(CP), ctypes.byref(h))
+        if st != 0:
+            raise RuntimeError("refgpu_create failed")
+        self.h = h
+
+    def apply(self, x_ptr, y_ptr):
+        if self.L.refgpu_apply(self.h, VP(x_ptr), VP(y_ptr)) != 0:
+            raise RuntimeError("refgpu_apply failed")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.refgpu_destroy(self.h)
+            self.h = None
