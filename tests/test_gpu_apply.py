@@ -114,6 +114,36 @@ def test_bitwise_reproducible(torch_cuda, ib, geom):
     assert torch.equal(ys[0], ys[1]) and torch.equal(ys[0], ys[2])
 
 
+@pytest.mark.parametrize("p,geom,precision", [(3, 0, 0), (3, 1, 0), (4, 0, 1), (2, 0, 0)])
+def test_apply_captures_into_cuda_graph(torch_cuda, ib, p, geom, precision):
+    """iga_apply is stream-ordered and capturable: the MatMult captured into a
+    CUDA graph (torch.cuda.graph) and replayed on new inputs in the same
+    buffers gives the eager results bitwise."""
+    torch = torch_cuda
+    plan = ib.Plan(distorted(ib.unit_square(p, 96, 80)), geometry=geom, precision=precision)
+    dt = torch.float32 if precision == ib.FP32 else torch.float64
+    x = torch.from_numpy(splitmix_uniform(31, -1.0, 1.0, plan.nfunc)).to(device="cuda", dtype=dt)
+    x2 = torch.from_numpy(splitmix_uniform(32, -1.0, 1.0, plan.nfunc)).to(device="cuda", dtype=dt)
+    y1, y2, y = torch.empty_like(x), torch.empty_like(x), torch.empty_like(x)
+    plan.apply(x, y1)
+    plan.apply(x2, y2)
+    xin = x.clone()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        plan.apply(xin, y, stream=torch.cuda.current_stream())
+    y.fill_(float("nan"))
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(y, y1)
+    xin.copy_(x2)
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(y, y2)
+    del g
+    plan.close()
+
+
 @pytest.mark.parametrize("p,nex,ney,geom,bc,ty", [(3, 64, 64, 0, 0, 0), (3, 200, 150, 0, 0, 0), (2, 90, 333, 0, 1, 0),
                                                   (4, 70, 45, 0, 0, 0), (3, 48, 200, 1, 0, 0), (3, 40, 37, 0, 1, 37),
                                                   (2, 33, 500, 1, 2, 16)])
