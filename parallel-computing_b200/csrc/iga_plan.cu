@@ -339,7 +339,10 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
     if (win.gyn < 0) {
         const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
         if (nseam > 0) {
-            const int blocks = (int)std::min<long long>((nseam + 255) / 256, 4 * 148);
+            // about one seam point per thread: the points' frame loads (L2 hits)
+            // all in flight at once (up to 7 points per thread before: 309.5 -> 306 us at
+            // p=3 2048^2 FP64 with one per thread)
+            const int blocks = (int)std::min<long long>((nseam + 255) / 256, 32 * 148);
             seam_fixup_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)sign, bc);
         }
     } else if (win.R1 > win.R0) {
