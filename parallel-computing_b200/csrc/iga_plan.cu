@@ -339,9 +339,9 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
     if (win.gyn < 0) {
         const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
         if (nseam > 0) {
-            // about one seam point per thread: the points' frame loads (L2 hits)
-            // all in flight at once (up to 7 points per thread before: 309.5 -> 306 us at
-            // p=3 2048^2 FP64 with one per thread)
+            // about one seam point per thread, so that the points' frame loads
+            // (L2 hits) are all in flight at once (p=3 2048^2 FP64 MatMult:
+            // 309.5 us with 7 points per thread, 306 us with one)
             const int blocks = (int)std::min<long long>((nseam + 255) / 256, 32 * 148);
             seam_fixup_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)sign, bc);
         }
