@@ -28,6 +28,7 @@ namespace iga {
 
 constexpr int kRedBlocks = 592;   // fixed grid of every reduction kernel (4 x 148 SMs)
 constexpr int kThreads = 256;
+constexpr size_t kBlasWorkspace = size_t(256) << 20;   // cuBLAS workspace of a solver (bytes)
 constexpr int kChunk = 16;        // inner CG iterations per captured graph
 
 struct DevScalars {
@@ -1161,9 +1162,8 @@ static int fd_upload(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
             set_error("cublasCreate failed");
             return IGA_ERR_CUDA;
         }
-        const size_t ws = size_t(256) << 20;
-        SOLVE_TRY(cudaMalloc(&S->blas_ws, ws));
-        if (cublasSetWorkspace(S->blas, S->blas_ws, ws) != CUBLAS_STATUS_SUCCESS) {
+        SOLVE_TRY(cudaMalloc(&S->blas_ws, kBlasWorkspace));
+        if (cublasSetWorkspace(S->blas, S->blas_ws, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS) {
             set_error("cublasSetWorkspace failed");
             return IGA_ERR_CUDA;
         }
@@ -1209,7 +1209,12 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
     const int nxp = ps.nxp, nyp = ps.nyp;
     int seg = (ny + 31) / 32;
     seg |= 1;   // odd: conflict-free shared-memory rows
+    // cublasSetStream puts the handle back on cuBLAS's own workspace pool;
+    // the fixed workspace goes back with it, or a GEMM captured into the
+    // solver's loop graph allocates (a memory-allocation node, which a
+    // conditional body may not hold)
     cublasSetStream(S->blas, S->stream);
+    cublasSetWorkspace(S->blas, S->blas_ws, kBlasWorkspace);
     constexpr int VN = Pk<T>::n;
     fd_gather_kernel<T, V><<<grid2d(nxp / VN, nyp), 128, 0, S->stream>>>(r, ps.W2, z, m, n, nx, ny, nxp, nyp, sc);
     cublasStatus_t e = gemm(S->blas, CUBLAS_OP_T, CUBLAS_OP_N, nyp, nxp, nxp, ps.W2, nxp, ps.Vx, nxp, ps.W1, nyp);
