@@ -238,3 +238,23 @@ def test_exact_pc_solve_matches_inner_cg_solve(torch_cuda, ib, orc, p, ne):
     ref = xa.cpu().numpy()
     assert rel(xb.cpu().numpy(), ref) < 1e-7
     assert rel(xc.cpu().numpy(), ref) < 1e-7
+
+
+@pytest.mark.parametrize("precision", [0, 2])
+def test_large_solve_runs_as_one_conditional_graph(torch_cuda, ib, precision):
+    """p=3 1536^2 (where cuBLAS's GEMMs would otherwise allocate inside the
+    captured loop): the PCG loop graph instantiates, so no fallback message
+    is left behind, and the solve converges."""
+    torch = torch_cuda
+    plan = ib.Plan(ib.unit_square(3, 1536), precision=ib.MIXED)
+    b = torch.empty(plan.nfunc, dtype=torch.float64, device="cuda")
+    plan.rhs(b, ib.F_SINSIN)
+    x = torch.zeros_like(b)
+    kw = dict(pc=ib.PC_FEM_EXACT, precision=precision)
+    if precision == ib.MIXED:
+        kw["sweep_rtol"] = 1e-3
+    st = plan.solve(b, x, **kw)
+    torch.cuda.synchronize()
+    assert st.status == 0 and st.relres <= 1e-10
+    assert "PCG loop" not in ib._lib().iga_last_error().decode()
+    plan.close()
