@@ -34,6 +34,8 @@ int up(T **dst, const T *src, size_t n)
 
 extern "C" {
 
+int refgpu_destroy(void *h);
+
 // Host arrays in the reference's layouts: B, dB [(p+1) qps][(p+1)] Bernstein
 // values / derivatives at the Gauss points, qw [p+1], C1 [nex (p+1)^2],
 // C2 [ney (p+1)^2], h1 [nex], h2 [ney], IEN [nex ney (p+1)^2], ID [N],
@@ -52,7 +54,8 @@ int refgpu_create(int p, int nex, int ney, const double *B, const double *dB, co
             up(&r->C1, C1, nb * nex) | up(&r->C2, C2, nb * ney) | up(&r->h1, h1, (size_t)nex) |
             up(&r->h2, h2, (size_t)ney) | up(&r->CP, CP, 2 * N) | up(&r->qw1, qw, (size_t)p + 1) |
             up(&r->qw2, qw, (size_t)p + 1) | up(&r->IEN, IEN, nb * nex * ney) | up(&r->ID, ID, N);
-    *out = r;
+    *out = e ? nullptr : r;
+    if (e) refgpu_destroy(r);
     return e;
 }
 
