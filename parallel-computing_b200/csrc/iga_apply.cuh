@@ -339,6 +339,8 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
             }
         }
         const T *ty = yr + ((s + P) % S::XR) * S::TYW;   // landed with x row s + P
+        constexpr bool MID = mid_shared(NQ, (int)sizeof(T));
+        constexpr int QJ = MID ? QH - 1 : QH;   // slots of this lane half's own columns
         // y tables (value n2, derivative d2) of quadrature row qy
         auto load_tab = [&](int qy, T (&n2)[NB], T (&d2)[NB]) {
             // rows of NBP entries, 16-byte aligned in the ring: vector loads
@@ -375,6 +377,17 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
                     g00 = gv[3 * j];
                     g01 = gv[3 * j + 1];
                     g11 = gv[3 * j + 2];
+                } else if constexpr (g_mid_lane_major(NQ, (int)sizeof(T))) {
+                    if (j + 1 < QH) {   // a column of this lane half
+                        g00 = gv[3 * j];
+                        g01 = gv[3 * j + 1];
+                        g11 = gv[3 * j + 2];
+                    } else if (valid) {   // the middle column, row qy of this half
+                        const T *gp = Gst + qy * (NQ * 3 * kSW) + 32 * (QH - 1) * 3 + c * 3;
+                        g00 = gp[0];
+                        g01 = gp[1];
+                        g11 = gp[2];
+                    }
                 } else if (valid) {
                     const T *gp = Gst + ((qy * NQ + qx) * 3) * kSW + c;
                     g00 = gp[0];
@@ -407,16 +420,18 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
                 acc1[jl][j] = fma(d2[jl], veta, acc1[jl][j]);
             }
         };
-        constexpr bool MID = mid_shared(NQ, (int)sizeof(T));
-        constexpr int QJ = MID ? QH - 1 : QH;   // slots of this lane half's own columns
+
 #pragma unroll
         for (int qy = 0; qy < NQ; ++qy) {
             T n2[NB], d2[NB];
             load_tab(qy, n2, d2);
-            T gv[g_lane_major(NQ) ? 3 * QH : 1];
-            if constexpr (GEOM == 0 && g_lane_major(NQ)) {   // 3 QH contiguous values, widest aligned loads
-                const T *src = Gst + (size_t)(qy * 32 + lane) * (3 * QH);
-                constexpr int BYTES = 3 * QH * (int)sizeof(T);
+            // this lane's G values of row qy for its own columns: 3 QJ contiguous
+            // values (lane-major G rows), widest aligned loads
+            constexpr int GVN = (g_lane_major(NQ) || g_mid_lane_major(NQ, (int)sizeof(T))) ? 3 * QJ : 1;
+            T gv[GVN];
+            if constexpr (GEOM == 0 && GVN > 1) {
+                const T *src = Gst + (size_t)qy * (NQ * 3 * kSW) + (size_t)lane * GVN;
+                constexpr int BYTES = GVN * (int)sizeof(T);
                 constexpr int VB = BYTES % 16 == 0 ? 16 : BYTES % 8 == 0 ? 8 : (int)sizeof(T);
                 using VT = typename std::conditional<VB == 16, float4, typename std::conditional<VB == 8, float2, T>::type>::type;
 #pragma unroll

@@ -104,19 +104,6 @@ constexpr int kSW = 16;
 // table loads cost more than the idle slot (185 -> 192 us).
 __host__ __device__ constexpr bool mid_shared(int NQ, int esz) { return NQ % 2 == 1 && (NQ >= 5 || esz == 4); }
 
-// Layout of one element-row step of a strip's G (NQ^2 points x 3 values x
-// kSW columns). Even NQ: [qy][lane = 2c + h][j][3], qx = h QH + j, so a lane's
-// values of one quadrature row are contiguous (vector loads); odd NQ:
-// [qy][qx][3][c] (the lane halves do not split the columns evenly).
-__host__ __device__ constexpr bool g_lane_major(int NQ) { return NQ % 2 == 0; }
-__host__ __device__ inline int g_index(int NQ, int qy, int qx, int comp, int c)
-{
-    if (g_lane_major(NQ)) {
-        const int QH = NQ / 2, h = qx / QH, j = qx - h * QH;
-        return ((qy * 32 + 2 * c + h) * QH + j) * 3 + comp;
-    }
-    return ((qy * NQ + qx) * 3 + comp) * kSW + c;
-}
 
 // Quadrature column of x-table slot j (j < QH = ceil(NQ / 2)) of the lane
 // half h: h QH + j (past NQ: an idle slot); where mid_shared(NQ, esz) the last
@@ -125,6 +112,31 @@ __host__ __device__ inline int g_index(int NQ, int qy, int qx, int comp, int c)
 __host__ __device__ constexpr int lane_qx(int NQ, int esz, int h, int j)
 {
     return (mid_shared(NQ, esz) && j == (NQ + 1) / 2 - 1) ? j : h * ((NQ + 1) / 2) + j;
+}
+
+// Layout of one element-row step of a strip's G (NQ^2 points x 3 values x
+// kSW columns), per quadrature row qy. Even NQ: [lane = 2c + h][j][3] with
+// qx = h QH + j, a lane's values contiguous (vector loads). Where the lane
+// halves share the middle column at NQ = 3 (g_mid_lane_major): [lane][3] for
+// the column of its own (qx = 0 or 2), then [c][3] for the middle column
+// (p=2 2048^2 FP32 148.8 -> 144.9 us; at NQ = 5 the vector-loaded values
+// spill under the FP32 kernel's 128-register cap, 75.6 -> 81.3 us, so p = 4
+// keeps the columns apart). Otherwise: [qx][3][c].
+__host__ __device__ constexpr bool g_lane_major(int NQ) { return NQ % 2 == 0; }
+__host__ __device__ constexpr bool g_mid_lane_major(int NQ, int esz) { return mid_shared(NQ, esz) && NQ < 5; }
+__host__ __device__ inline int g_index(int NQ, int esz, int qy, int qx, int comp, int c)
+{
+    const int QH = (NQ + 1) / 2, QB = NQ * 3 * kSW;
+    if (g_lane_major(NQ)) {
+        const int h = qx / QH, j = qx - h * QH;
+        return qy * QB + ((2 * c + h) * QH + j) * 3 + comp;
+    }
+    if (g_mid_lane_major(NQ, esz)) {
+        if (qx == QH - 1) return qy * QB + 32 * (QH - 1) * 3 + c * 3 + comp;
+        const int h = qx < QH - 1 ? 0 : 1, j = h ? qx - QH : qx;
+        return qy * QB + ((2 * c + h) * (QH - 1) + j) * 3 + comp;
+    }
+    return ((qy * NQ + qx) * 3 + comp) * kSW + c;
 }
 
 // The element grid is cut into warp strips of kSW element columns by TY

@@ -67,9 +67,9 @@ __global__ void geom_setup_kernel(T *__restrict__ G, const double *__restrict__ 
             g11 = f * (x_xi * x_xi + y_xi * y_xi);
         }
         T *Gs = G + (((size_t)gx * g.NSY + gy) * g.TY + s) * NQ2 * 3 * kSW;
-        Gs[g_index(NQ, qy, qx, 0, c)] = (T)g00;
-        Gs[g_index(NQ, qy, qx, 1, c)] = (T)g01;
-        Gs[g_index(NQ, qy, qx, 2, c)] = (T)g11;
+        Gs[g_index(NQ, (int)sizeof(T), qy, qx, 0, c)] = (T)g00;
+        Gs[g_index(NQ, (int)sizeof(T), qy, qx, 1, c)] = (T)g01;
+        Gs[g_index(NQ, (int)sizeof(T), qy, qx, 2, c)] = (T)g11;
     }
 }
 
