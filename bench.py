@@ -146,46 +146,65 @@ def ref_lib():
     return None, None
 
 
-def cpu_reference_apply_rate(ne_sample, reps, threads):
-    """GDOF/s of the reference's CPU MatMult (ElementMF + LocalAssemblyMF, the
-    loop of GlobalAssemblyMF::MatMulMF) on a p=3 ne_sample^2 patch; falls back
-    to the C oracle restatement when the compiled reference is absent."""
-    L, kind = ref_lib()
-    vp = ctypes.c_void_p
-    m = ne_sample + P
-    nf = m * m
-    x = splitmix_uniform(SEED, -1.0, 1.0, nf)
-    y = np.zeros(nf)
-    if L is not None:
-        CP = np.zeros(2 * nf)
-        IEN = np.zeros(ne_sample * ne_sample * 16, np.int32)
-        ID = np.zeros(nf, np.int32)
-        Dir = np.zeros(nf, np.int32)
+class CpuReference:
+    """The reference's CPU MatMult on a p=3 ne^2 unit-square patch built by
+    the reference's own preprocessing (oracle/_ref/libigaref.so): rate(path)
+    times ElementMF + LocalAssemblyMF ("mf", the mult_mf path of
+    matrix_free/iteration_number_fempc_mf.cpp) or ElementMFSF +
+    LocalAssemblyMFSF ("sf", the mult_sf path), each in the element loop of
+    GlobalAssemblyMF::MatMulMF, on `threads` host threads (element-row
+    blocks, one per thread, like the reference's MPI ranks). Falls back to
+    the C oracle restatement (one thread) when the compiled reference is
+    absent."""
+
+    def __init__(self, ne):
+        self.L, self.kind = ref_lib()
+        self.ne = ne
+        m = ne + P
+        self.nf = m * m
+        self.x = splitmix_uniform(SEED, -1.0, 1.0, self.nf)
+        self.y = np.zeros(self.nf)
+        if self.L is None:
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            from iga_testlib import Oracle, unit_square_mesh
+            self.orc = Oracle()
+            self.mesh = unit_square_mesh(self.orc, P, P, ne, ne)
+            self.kind = "port"
+            return
+        vp = ctypes.c_void_p
+        self.a = dict(CP=np.zeros(2 * self.nf), IEN=np.zeros(ne * ne * 16, np.int32), ID=np.zeros(self.nf, np.int32),
+                      Dir=np.zeros(self.nf, np.int32), C1=np.zeros(ne * 16), C2=np.zeros(ne * 16), h1=np.zeros(ne),
+                      h2=np.zeros(ne))
+        ptr = lambda k: self.a[k].ctypes.data_as(vp)  # noqa: E731
         nd = ctypes.c_int()
-        C1 = np.zeros(ne_sample * 16)
-        C2 = np.zeros(ne_sample * 16)
-        h1 = np.zeros(ne_sample)
-        h2 = np.zeros(ne_sample)
-        ptr = lambda a: a.ctypes.data_as(vp)  # noqa: E731
-        L.ref_mesh(P, P, ne_sample, ne_sample, ctypes.c_double(1.0), ctypes.c_double(1.0), ptr(CP), ptr(IEN),
-                   ptr(ID), ptr(Dir), ctypes.byref(nd), ptr(C1), ptr(C2), ptr(h1), ptr(h2))
-        args = [P, P, ne_sample, ne_sample, ptr(CP), ptr(IEN), ptr(ID), ptr(Dir), nd.value, ptr(C1), ptr(C2),
-                ptr(h1), ptr(h2), ptr(x), ptr(y), threads]
-        run = lambda: L.ref_apply_mf(*args)  # noqa: E731
-    else:
-        sys.path.insert(0, os.path.join(ROOT, "tests"))
-        from iga_testlib import Oracle, unit_square_mesh
-        orc = Oracle()
-        mesh = unit_square_mesh(orc, P, P, ne_sample, ne_sample)
-        kind, threads = "port", 1
-        run = lambda: orc.apply_mf(mesh, x)  # noqa: E731
-    times = []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        run()
-        times.append(time.perf_counter() - t0)
-    t = statistics.median(times)
-    return nf / t / 1e9, kind, threads, t
+        self.L.ref_mesh(P, P, ne, ne, ctypes.c_double(1.0), ctypes.c_double(1.0), ptr("CP"), ptr("IEN"), ptr("ID"),
+                        ptr("Dir"), ctypes.byref(nd), ptr("C1"), ptr("C2"), ptr("h1"), ptr("h2"))
+        self.args = [P, P, ne, ne, ptr("CP"), ptr("IEN"), ptr("ID"), ptr("Dir"), nd.value, ptr("C1"), ptr("C2"),
+                     ptr("h1"), ptr("h2"), self.x.ctypes.data_as(vp), self.y.ctypes.data_as(vp)]
+
+    def rate(self, path, reps, threads):
+        """(GDOF/s, threads used, median seconds per MatMult)."""
+        if self.L is None:
+            threads = 1
+            run = (lambda: self.orc.apply_mf(self.mesh, self.x)) if path == "mf" else \
+                (lambda: self.orc.apply_sf(self.mesh, self.x))
+        else:
+            fn = self.L.ref_apply_mf if path == "mf" else self.L.ref_apply_sf
+            run = lambda: fn(*self.args, threads)  # noqa: E731
+        times = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            run()
+            times.append(time.perf_counter() - t0)
+        t = statistics.median(times)
+        return self.nf / t / 1e9, threads, t
+
+
+def cpu_reference_apply_rate(ne_sample, reps, threads, path="mf"):
+    """GDOF/s of the reference's CPU MatMult on a p=3 ne_sample^2 patch."""
+    ref = CpuReference(ne_sample)
+    rate, threads, t = ref.rate(path, reps, threads)
+    return rate, ref.kind, threads, t
 
 
 def reference_arm(args):
@@ -193,16 +212,25 @@ def reference_arm(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    ne_sample = 512
-    rate, kind, threads, t = cpu_reference_apply_rate(ne_sample, max(1, min(args.steps, 3)), threads)
-    sample = (f"p=3 {ne_sample}x{ne_sample}-element unit-square patch ({(ne_sample + 3) ** 2} DOFs), "
-              f"{max(1, min(args.steps, 3))} MatMults, median {t:.3f} s each; per-element cost is size-independent")
+    # the benchmark's own configuration, p=3 2048^2 (about 7 s per MatMult on 16 cores)
+    ref = CpuReference(NE)
+    reps_mf, reps_sf = max(1, min(args.steps, 3)), max(1, min(args.steps, 2))
+    rate, threads, t = ref.rate("mf", reps_mf, threads)
+    rate_sf, _, t_sf = ref.rate("sf", reps_sf, threads)
+    sample = (f"the full workload, p=3 {NE}x{NE} elements ({(NE + P) ** 2} DOFs): median of {reps_mf} MatMults, "
+              f"{t:.3f} s each")
     out = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "GDOF/s", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "config": {"workload": f"matmul_p3_{NE}x{NE}_fp64_precomputed_geometry", "p": P, "nElem": [NE, NE],
-                      "dofs": (NE + P) ** 2, "reference_path": "matrix_free ElementMF+LocalAssemblyMF (CPU)"},
-           "cpu_baseline": {"value": rate, "unit": "GDOF/s", "cores": threads, "kind": kind, "sample": sample},
+                      "dofs": (NE + P) ** 2, "same_config": True,
+                      "reference_path": "matrix_free ElementMF+LocalAssemblyMF (CPU, the mult_mf path: the faster "
+                                        "of the reference's two CPU MatMults)"},
+           "cpu_baseline": {"value": rate, "unit": "GDOF/s", "cores": threads, "kind": ref.kind, "sample": sample},
+           "mult_sf": {"value": rate_sf, "unit": "GDOF/s", "cores": threads, "kind": ref.kind,
+                       "ms_per_step": t_sf * 1e3,
+                       "what": f"ElementMFSF + LocalAssemblyMFSF (the mult_sf path), same patch, median of "
+                               f"{reps_sf} MatMults"},
            "e2e": {"value": rate, "unit": "GDOF/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     gk = reference_gpu_kernel_rate(NE, max(1, min(args.steps, 5)))
     if gk is not None:
@@ -511,6 +539,21 @@ def our_arm(args):
             dist.destroy_process_group()
         return
 
+    if args.profile_solve:
+        # the mixed-precision solve of the p=4 1024x1024 NURBS annulus cut to
+        # one FP32 sweep of 12 iterations (a target for a per-iteration launch list)
+        plan = ib.Plan(ib.quarter_annulus(4, 1024), precision=ib.MIXED)
+        b = torch.empty(plan.nfunc, dtype=torch.float64, device="cuda")
+        plan.rhs(b, ib.F_ANNULUS)
+        x = torch.zeros_like(b)
+        plan.solve(b, x, check=False, pc=ib.PC_FEM_EXACT, precision=ib.MIXED, sweep_rtol=1e-2, max_it=12,
+                   max_sweeps=1)
+        torch.cuda.synchronize()
+        plan.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
     if args.batch_only:
         res = time_batch(ib, torch, torch.cuda.current_stream(), barrier, max_over_ranks)
         if rank == 0:
@@ -627,9 +670,16 @@ def our_arm(args):
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        rate, kind, threads, t = cpu_reference_apply_rate(256, 3, os.cpu_count() or 1)
-        cpu = {"value": rate, "unit": "GDOF/s", "cores": threads, "kind": kind,
-               "sample": f"p=3 256x256-element patch ({259 ** 2} DOFs), median of 3 MatMults ({t:.3f} s each)"}
+        ref = CpuReference(512)
+        rate, threads, t = ref.rate("mf", 3, os.cpu_count() or 1)
+        cpu = {"value": rate, "unit": "GDOF/s", "cores": threads, "kind": ref.kind,
+               "sample": f"p=3 512x512-element patch ({515 ** 2} DOFs), median of 3 MatMults ({t:.3f} s each); "
+                         "the per-element cost does not depend on the patch size"}
+        rate_sf, _, t_sf = ref.rate("sf", 2, os.cpu_count() or 1)
+        cpu["mult_sf"] = {"value": rate_sf, "unit": "GDOF/s", "cores": threads, "kind": ref.kind,
+                          "sample": f"ElementMFSF + LocalAssemblyMFSF (the mult_sf path), same patch, median of 2 "
+                                    f"MatMults ({t_sf:.3f} s each)"}
+        del ref
         # the same element code on one core (the reference's per-rank rate)
         rate1, kind1, _, t1 = cpu_reference_apply_rate(128, 3, 1)
         cpu["one_core"] = {"value": rate1, "unit": "GDOF/s", "cores": 1, "kind": kind1,
@@ -679,6 +729,9 @@ def main():
     ap.add_argument("--profile-annulus", action="store_true",
                     help="run the FP32 and FP64 operators of the p=4 1024x1024 NURBS annulus a few times "
                          "outside any graph (a target for ncu; prints nothing else)")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="run one 12-iteration FP32 sweep of the annulus mixed-precision solve (a target for a "
+                         "per-iteration ncu launch list; prints nothing else)")
     ap.add_argument("--profile-batch-pc", action="store_true",
                     help="run the batched preconditioner and operator of the 256-problem batch a few times "
                          "outside any graph (a target for ncu; prints nothing else)")

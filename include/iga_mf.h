@@ -142,17 +142,57 @@ int iga_apply_prec(iga_plan *plan, int precision, const void *x_dev, void *y_dev
  * legacy default stream; the result is bitwise that of iga_apply. */
 int iga_apply_host(iga_plan *plan, const double *x_host, double *y_host);
 
+/* Synchronises `stream` (a cudaStream_t or NULL), then reads and clears the
+ * plan's device error flag: IGA_OK, or the status a kernel recorded since the
+ * last query (IGA_ERR_TIMEOUT: a bounded wait for a bulk copy gave up; the
+ * kernel stopped, let its copies land and returned, and the plan stays usable).
+ * The stream-ordered calls (iga_apply, iga_apply_prec, iga_rhs) cannot report
+ * such errors themselves; iga_apply_host and the solver check the flag. No
+ * counterpart in the reference, which calls exit() on any CUDA error
+ * (matrix_free_gpu/include/memory.cuh:9-12). */
+int iga_plan_device_status(iga_plan *plan, void *stream);
+/* Polls each bounded wait of the plan's MatMult kernel makes before it gives
+ * up with IGA_ERR_TIMEOUT: polls >= 0 sets the limit (0: every wait gives up
+ * at once, for tests of the timeout path; the kernel still waits, with the
+ * full limit, for the copies it issued before returning), polls < 0 restores
+ * the default (2^24 polls, seconds of wall time). A test hook: no counterpart
+ * in the reference. */
+int iga_plan_set_wait_limit(iga_plan *plan, long long polls);
+
 /* Load vector F = int R f with F[Dir] = 0 (GlobalAssemblyMF::AssemLoad,
  * matrix_free/src/GlobalAssemblyMF.cpp:26-80), FP64, device output. */
 int iga_rhs(iga_plan *plan, int fkind, double *F_dev, void *stream);
 
 /* Reference-shaped entry point: the argument list of MatrixFreeMatMultCUDA
- * (matrix_free_gpu/include/mult.cuh:16-24, all device pointers). B1/B2/dB1/dB2
- * (Bernstein tables), h1/h2 and qw1/qw2 are accepted and not needed. The
- * first call with a given mesh builds and caches a plan from CP and the
- * extraction operators (one device-to-host copy of those), later calls reuse
- * it. Unlike the reference it does not exit on error and applies y[Dir] = 0
- * itself (the reference caller runs DirichletBCCUDA afterwards). */
+ * (matrix_free_gpu/include/mult.cuh:16-24, all device pointers), synchronous
+ * like the reference's (cudaDeviceSynchronize after the kernel,
+ * matrix_free_gpu/src/mult.cu:550); the status covers the kernels' run.
+ *   - d_IEN must be the structured single-patch connectivity the reference's
+ *     IENGenerator::GenerateIEN2D writes (matrix_free/src/IENGenerator.cpp:
+ *     68-103); anything else returns IGA_ERR_UNSUPPORTED. NULL: assumed.
+ *   - d_ID is honoured as the reference kernel honours it
+ *     (matrix_free_gpu/src/mult.cu:455-460): control point A's row goes to
+ *     y[ID[A]] when ID[A] >= 0 and nowhere otherwise. ID values must lie below
+ *     nfunc = (nElemX+p)*(nElemY+q) and name no row twice (else
+ *     IGA_ERR_UNSUPPORTED). With the reference's serial numbering (-1 on the
+ *     boundary ring, A elsewhere; or NULL) the boundary rows are written as
+ *     zero (y[Dir] = 0, which the reference caller's DirichletBCCUDA does);
+ *     with any other ID the entries of y no ID value names keep their
+ *     contents, so the caller zeroes y first, as the reference's caller does
+ *     (matrix_free_gpu/src/GlobalAssemblyMF.cu:210).
+ *   - d_B1/d_B2/d_dB1/d_dB2 and qw1/qw2 (Bernstein values/derivatives at the
+ *     p+1 Gauss points on [0,1], point-major, and the Gauss weights) are
+ *     checked once against the rule this library integrates with
+ *     (IGA_ERR_UNSUPPORTED if they differ); all NULL: the library's own.
+ *   - h1/h2 are accepted and not needed (they cancel in the operator).
+ *   - d_F_array_in / d_F_array_out: 8-byte aligned, nfunc doubles.
+ * The first call with a given set of arrays on a device builds and caches a
+ * plan (one device-to-host copy of CP and the extraction operators, a device
+ * check of IEN/ID); later calls with the same pointers on the same device
+ * reuse it and assume the arrays' contents unchanged: after rewriting any of
+ * them in place (or freeing them and reusing the addresses), call
+ * iga_MatrixFreeMatMultCUDA_release. Unlike the reference it does not exit on
+ * error. */
 int iga_MatrixFreeMatMultCUDA(int p, int q, int nlocalelemx, int nlocalelemy,
                               const double *d_B1, const double *d_B2,
                               const double *d_dB1, const double *d_dB2,
@@ -172,16 +212,25 @@ int iga_MatrixFreeMatMultCUDA_release(void);
  * array, and d_B1/d_dB1 (d_B2/d_dB2) must hold the Bernstein values/derivatives
  * at the p+1 (q+1) Gauss points on [0,1], point-major, and qw1/qw2 the Gauss
  * weights (the arrays the reference uploads). Geometry is computed on the fly
- * from d_CP (no NURBS weights). Computes y = A_ref x with y[Dir] = 0.
+ * from d_CP (no NURBS weights). Computes y = A_ref x; d_IEN and d_ID are
+ * checked and honoured exactly as by iga_MatrixFreeMatMultCUDA (on every call,
+ * before y is touched; NULL: the structured connectivity and the reference's
+ * serial numbering, with y[Dir] = 0). Alignment: d_CP 16 bytes (it is read as
+ * (x, y) pairs), the other double arrays 8 bytes, d_IEN/d_ID 4 bytes;
+ * otherwise IGA_ERR_ARG before anything runs. p == q with 1 <= p <= 5, else
+ * IGA_ERR_UNSUPPORTED. The call runs on `stream` and returns after the
+ * stream's work is done (the kernels' error slot is read back: IGA_ERR_TIMEOUT
+ * when a bounded wait gave up).
  * This entry point calls no cudaMalloc, cudaFree or other allocating routine:
- * its scratch (basis tables and seam frames) is a fixed 16 MiB device array
- * held by every GPU that loads the library until the process exits. Meshes whose
- * scratch would exceed 16 MiB are rejected with IGA_ERR_UNSUPPORTED (p = 3 up to
- * about 2048 x 2048 elements fits). The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) and sets the kernel's shared
- * memory limit; make that first call before any stream capture. All calls share
- * the one array, so calls that overlap on the GPU (other streams, other host
- * threads) race and must be serialised by the caller. */
+ * its scratch (basis tables, seam frames, the IEN/ID check words) is a fixed
+ * 16 MiB device array held by every GPU that loads the library until the
+ * process exits. Meshes whose scratch would exceed 16 MiB are rejected with
+ * IGA_ERR_UNSUPPORTED (p = 3 up to about 2048 x 2048 elements fits). The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress)
+ * and sets the kernel's shared memory limit; make that first call before any
+ * stream capture. All calls share the one array, so calls that overlap on the
+ * GPU (other streams, other host threads) race and must be serialised by the
+ * caller. */
 int iga_MatrixFreeMatMultCUDA_noalloc(int p, int q, int nlocalelemx, int nlocalelemy,
                                       const double *d_B1, const double *d_B2,
                                       const double *d_dB1, const double *d_dB2,

@@ -50,7 +50,31 @@ struct ApplyParams {
     // apply_kernel's window of strip rows: gy0 .. gy0 + gyn - 1 (default: all;
     // a host-buffer MatMult applies the patch slab by slab to overlap copies)
     int gy0 = 0, gyn = 1 << 30;
+    // Equation numbers (the reference's ID array, matrix_free_gpu/src/mult.cu:
+    // 455-460): when set, control point A's value goes to y[ID[A]] if
+    // 0 <= ID[A] < m n and nowhere otherwise (use with bc = 2: every row the
+    // full element sum, x read everywhere).
+    const int *ID = nullptr;
+    // Polls of each wait for a G stage before it reports IGA_ERR_TIMEOUT.
+    long long wait_polls = kWaitLimit;
 };
+
+// Stores sign * v for control point i = R m + C under boundary rule bc
+// (0: y[boundary] = 0, 1: y[boundary] = x[boundary], 2: none) or, when ID is
+// set, at equation ID[i] (skipped for ID[i] < 0 or out of range).
+template <typename T>
+__device__ __forceinline__ void store_point(const StripGrid &g, const T *__restrict__ x, T *__restrict__ y,
+                                            const int *__restrict__ ID, T sign, int bc, int R, int C, T v)
+{
+    const size_t i = (size_t)R * g.m + C;
+    if (ID) {
+        const int e = ID[i];
+        if (e >= 0 && (long long)e < (long long)g.m * g.n) y[e] = sign * v;
+        return;
+    }
+    const bool bnd = bc != 2 && (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
+    y[i] = bnd ? (bc == 1 ? x[i] : T(0)) : sign * v;
+}
 
 template <int P, typename T>
 struct ApplyShape {
@@ -273,11 +297,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         }
     };
 
-    auto store = [&](int R, int C, T v) {
-        const size_t i = (size_t)R * g.m + C;
-        const bool bnd = a.bc != 2 && (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
-        y[i] = bnd ? (a.bc == 1 ? x[i] : T(0)) : a.sign * v;
-    };
+    auto store = [&](int R, int C, T v) { store_point<T>(g, x, y, a.ID, a.sign, a.bc, R, C, v); };
     T *frame = a.frame + (size_t)(gx * g.NSY + gy) * g.FS;
     auto write_row = [&](int lr, const T (&r0)[QH], const T (&r1)[QH]) {
         T out[NB];
@@ -332,7 +352,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         const int slot = s % NST;
         const T *Gst = Gs + (size_t)slot * S::GE;
         if (GEOM == 0) {
-            if (!mbar_wait_bounded(&wbar[slot], (uint32_t)((s / NST) & 1))) {
+            if (!mbar_wait_bounded(&wbar[slot], (uint32_t)((s / NST) & 1), a.wait_polls)) {
                 ok = false;
                 failed_step = s;
                 break;
@@ -487,7 +507,8 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     if (!ok) {
         if (lane == 0) atomicExch(a.err, 8 /* IGA_ERR_TIMEOUT */);
         // Let the copies already issued (steps failed_step .. failed_step+NST-1)
-        // land before the CTA's shared memory is released; bounded as well.
+        // land before the CTA's shared memory is released; bounded as well,
+        // always with the full poll limit.
         for (int t = failed_step; t < nsteps && t < failed_step + NST; ++t)
             mbar_wait_bounded(&wbar[t % NST], (uint32_t)((t / NST) & 1));
         cp_async_wait<0>();
@@ -554,7 +575,8 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, 0>(), 1)
 // in fixed strip order, stored with the boundary rule.
 template <int P, typename T>
 __device__ __forceinline__ void seam_point_rc(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
-                                              const StripGrid &g, T sign, int bc, int R, int C)
+                                              const StripGrid &g, T sign, int bc, const int *__restrict__ ID, int R,
+                                              int C)
 {
     int fa, fb;
     const int ca = cover(C, kSW, g.NSX, P, fa);
@@ -567,14 +589,13 @@ __device__ __forceinline__ void seam_point_rc(const T *__restrict__ frame, const
             v += frame[(size_t)(aa * g.NSY + b) * g.FS + frame_index(R - g.TY * b, C - kSW * aa, P, g.TY)];
         }
     }
-    const size_t i = (size_t)R * g.m + C;
-    const bool bnd = bc != 2 && (R == 0 || C == 0 || R == g.n - 1 || C == g.m - 1);
-    y[i] = bnd ? (bc == 1 ? x[i] : T(0)) : sign * v;
+    store_point<T>(g, x, y, ID, sign, bc, R, C, v);
 }
 
 template <int P, typename T>
 __device__ __forceinline__ void seam_point(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
-                                           const StripGrid &g, T sign, int bc, long long idx)
+                                           const StripGrid &g, T sign, int bc, const int *__restrict__ ID,
+                                           long long idx)
 {
     const long long per = (long long)g.n * P;            // points of one vertical seam
     const long long nV = (long long)(g.NSX - 1) * per;
@@ -596,7 +617,7 @@ __device__ __forceinline__ void seam_point(const T *__restrict__ frame, const T 
         const int s = C / kSW;
         if (C % kSW < P && s >= 1 && s < g.NSX) return;   // handled as a vertical seam
     }
-    seam_point_rc<P, T>(frame, x, y, g, sign, bc, R, C);
+    seam_point_rc<P, T>(frame, x, y, g, sign, bc, ID, R, C);
 }
 
 // The seam points of control-point rows R0 .. R1 - 1, where R0 = TY * s0 is a
@@ -605,7 +626,7 @@ __device__ __forceinline__ void seam_point(const T *__restrict__ frame, const T 
 // Valid once every strip covering those rows has written its frame.
 template <int P, typename T>
 __global__ void seam_fixup_rows_kernel(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
-                                       StripGrid g, T sign, int bc, int R0, int R1)
+                                       StripGrid g, T sign, int bc, int R0, int R1, const int *__restrict__ ID)
 {
     const int s0 = max(R0 / g.TY, 1), s1 = (R1 + g.TY - 1) / g.TY;   // horizontal seams s0 .. s1 - 1
     const long long nv = (long long)(g.NSX - 1) * P * (R1 - R0);
@@ -629,7 +650,7 @@ __global__ void seam_fixup_rows_kernel(const T *__restrict__ frame, const T *__r
             const int s = C / kSW;
             if (C % kSW < P && s >= 1 && s < g.NSX) continue;   // a vertical seam's point
         }
-        seam_point_rc<P, T>(frame, x, y, g, sign, bc, R, C);
+        seam_point_rc<P, T>(frame, x, y, g, sign, bc, ID, R, C);
     }
 }
 
@@ -640,12 +661,12 @@ __host__ __device__ __forceinline__ long long seam_count(const StripGrid &g)
 
 template <int P, typename T>
 __global__ void seam_fixup_kernel(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
-                                  StripGrid g, T sign, int bc)
+                                  StripGrid g, T sign, int bc, const int *__restrict__ ID)
 {
     const long long total = seam_count(g);
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x)
-        seam_point<P, T>(frame, x, y, g, sign, bc, idx);
+        seam_point<P, T>(frame, x, y, g, sign, bc, ID, idx);
 }
 
 template <int P, typename T>
@@ -654,7 +675,7 @@ __device__ __forceinline__ void seam_loop(const ApplyParams<T> &a, const T *__re
     const long long total = seam_count(a.g);
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x)
-        seam_point<P, T>(a.frame, x, y, a.g, a.sign, a.bc, idx);
+        seam_point<P, T>(a.frame, x, y, a.g, a.sign, a.bc, a.ID, idx);
 }
 
 // Seams of every active problem of a batch: blockIdx.y = problem.

@@ -62,10 +62,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait for phase `parity` of *bar; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+// Bounded wait for phase `parity` of *bar; returns false after `limit` polls
+// (limit 0: gives up at once, which tests use to exercise the timeout path).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long limit = kWaitLimit)
 {
-    for (long long it = 0; it < kWaitLimit; ++it)
+    for (long long it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }

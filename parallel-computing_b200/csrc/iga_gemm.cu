@@ -1,0 +1,481 @@
+// Dense GEMMs of the exact FEM preconditioner without a BLAS library
+// (interface and operand conventions in iga_gemm.hpp).
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "iga_gemm.hpp"
+#include "iga_plan.hpp"
+#include "iga_umma.cuh"
+
+namespace iga {
+
+// ------------------------------------------------------------ TF32 on tcgen05
+// One CTA computes a 128 x 128 tile of C with the FP32 accumulator in 128
+// TMEM columns. Thread 0 of warp 0 feeds a ring of kGS stages with the
+// tensor-memory accelerator: per stage a 32-wide K slice of A (128 rows) and
+// of B (128 rows), 16 KiB each, in the canonical 128-byte-swizzled layouts of
+// the UMMA descriptors (K-major: 128-byte rows of 32 k values, 8-row groups
+// 1 KiB apart; MN-major: four 4 KiB boxes of 32 k rows x 32 values, one per
+// 32-wide MN atom). Thread 0 of warp 1 issues four 128 x 128 x 8 MMAs per
+// stage and commits them to the stage's "empty" barrier, which releases the
+// stage to the copy thread. After the last slice a commit to "done" hands
+// the accumulator to the epilogue: every warp reads its 32 TMEM lanes
+// (tcgen05.ld 32x32b) and stores its rows of C. No cluster multicast.
+// Two CTAs fit an SM (96 KiB of stages each), so a 2064 x 2064 product
+// (17 x 17 tiles) runs in one wave on 148 SMs.
+constexpr int kGM = 128, kGN = 128, kGK = 32, kGS = 3;
+constexpr int kGTile = kGM * kGK * 4;   // bytes of one operand slice (A and B alike, kGM == kGN)
+constexpr int kGSmem = 1024 + kGS * 2 * kGTile + 256;
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Descriptor of a 128-byte-swizzled operand tile (start 1 KiB aligned up to
+// the K-substep offset); layout type 2 = SWIZZLE_128B in bits [61, 64).
+__device__ __forceinline__ uint64_t sw128_desc(const void *p, uint32_t lbo, uint32_t sbo)
+{
+    return umma::smem_desc(p, lbo, sbo) | ((uint64_t)2 << 61);
+}
+
+// OUT: 0 C, 1 scatter into an FP32 vector, 2 into an FP64 vector (GemmScatter).
+template <bool AMN, bool BMN, int OUT>
+__global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ CUtensorMap ta,
+                                                        const __grid_constant__ CUtensorMap tb, int K, int Mst, int Nst,
+                                                        float *__restrict__ C, int ldc, int *__restrict__ err,
+                                                        GemmScatter sc)
+{
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *sm =
+        reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned char *As = sm, *Bs = sm + kGS * kGTile;
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm + 2 * kGS * kGTile);
+    uint64_t *empty = full + kGS, *done = empty + kGS;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 1);
+    int *cnt = reinterpret_cast<int *>(tslot + 1);   // [0] slices loaded, [1] slices consumed, [2] failure
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * kGM, n0 = blockIdx.y * kGN;
+    const int nk = (K + kGK - 1) / kGK;
+
+    if (warp == 0) {
+        umma::alloc(tslot, kGN);
+        umma::relinquish();
+    }
+    if (tid == 32) {
+        for (int s = 0; s < kGS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        cnt[0] = cnt[1] = cnt[2] = 0;
+        fence_mbar_init();
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 0 && lane == 0) {   // copy thread
+        int kt = 0;
+        for (; kt < nk; ++kt) {
+            const int s = kt % kGS;
+            if (kt >= kGS && !mbar_wait_bounded(&empty[s], (uint32_t)((kt / kGS - 1) & 1))) {
+                cnt[2] = 1;
+                break;
+            }
+            mbar_arrive_expect_tx(&full[s], 2 * kGTile);
+            const int k0 = kt * kGK;
+            unsigned char *a = As + s * kGTile, *b = Bs + s * kGTile;
+            if (AMN) {
+                for (int j = 0; j < kGM / 32; ++j) tma_load_2d(a + j * 4096, &ta, m0 + 32 * j, k0, &full[s]);
+            } else {
+                tma_load_2d(a, &ta, k0, m0, &full[s]);
+            }
+            if (BMN) {
+                for (int j = 0; j < kGN / 32; ++j) tma_load_2d(b + j * 4096, &tb, n0 + 32 * j, k0, &full[s]);
+            } else {
+                tma_load_2d(b, &tb, k0, n0, &full[s]);
+            }
+        }
+        cnt[0] = kt;
+    } else if (warp == 1 && lane == 0) {   // MMA thread
+        constexpr uint32_t IDESC =
+            umma::idesc_tf32<kGM, kGN>() | ((uint32_t)AMN << 15) | ((uint32_t)BMN << 16);
+        int kt = 0;
+        for (; kt < nk; ++kt) {
+            const int s = kt % kGS;
+            if (!mbar_wait_bounded(&full[s], (uint32_t)((kt / kGS) & 1))) {
+                cnt[2] = 1;
+                break;
+            }
+            umma::fence_after_sync();
+            const unsigned char *a = As + s * kGTile, *b = Bs + s * kGTile;
+#pragma unroll
+            for (int j = 0; j < kGK / 8; ++j) {
+                // K substep j: 8 k values = 32 bytes along a K-major row, or 8
+                // rows (one 1 KiB swizzle group) of an MN-major tile
+                const uint64_t ad = AMN ? sw128_desc(a + j * 1024, 4096, 1024) : sw128_desc(a + j * 32, 16, 1024);
+                const uint64_t bd = BMN ? sw128_desc(b + j * 1024, 4096, 1024) : sw128_desc(b + j * 32, 16, 1024);
+                umma::mma_tf32(tmem, ad, bd, IDESC, (kt > 0 || j > 0) ? 1u : 0u);
+            }
+            umma::commit(&empty[s]);
+        }
+        cnt[1] = kt;
+        umma::commit(done);   // arrives once every MMA issued above has completed
+    }
+    __syncwarp();
+    const bool ok = !__syncthreads_or(!mbar_wait_bounded(done, 0));   // uniform over the CTA
+    const bool failed = !ok || cnt[2] || cnt[1] < nk;
+    if (!failed) {
+        umma::fence_after_sync();
+        const int row = m0 + 32 * warp + lane;
+        double f = 1.0;
+        if (OUT != 0 && sc.rr) {
+            const double rr = *sc.rr;
+            f = (rr > 0.0 && rr < 1e300) ? sqrt(rr) : 1.0;
+        }
+#pragma unroll 1
+        for (int c0 = 0; c0 < kGN; c0 += 16) {
+            float v[16];
+            umma::ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+            umma::wait_ld();
+            const int col = n0 + c0;
+            if (OUT != 0) {   // interior block of a vector, unaligned: scalar stores
+                if (row >= sc.rows) continue;
+                const size_t base = (size_t)(row + 1) * sc.ld + col + 1;
+#pragma unroll
+                for (int c = 0; c < 16; ++c) {
+                    if (col + c >= sc.cols) break;
+                    if (OUT == 1) static_cast<float *>(sc.out)[base + c] = (float)(f * (double)v[c]);
+                    else static_cast<double *>(sc.out)[base + c] = f * (double)v[c];
+                }
+                continue;
+            }
+            if (row >= Mst || col >= Nst) continue;
+            float *dst = C + (size_t)row * ldc + col;
+            if (col + 16 <= Nst) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    reinterpret_cast<float4 *>(dst)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 16; ++c)
+                    if (c < Nst - col) dst[c] = v[c];
+            }
+        }
+    } else {
+        if (tid == 0) {
+            atomicExch(err, 8 /* IGA_ERR_TIMEOUT */);
+            // the copies issued and not consumed land before the stages are released
+            for (int kt = cnt[1]; kt < cnt[0]; ++kt) mbar_wait_bounded(&full[kt % kGS], (uint32_t)((kt / kGS) & 1));
+        }
+        if (!ok) mbar_wait_bounded(done, 0);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::dealloc(tmem, kGN);
+}
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encoder()
+{
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// Tensor map of one operand: K-major X[rows][k] (box 32 k x 128 rows) or
+// MN-major X[k][rows] (box 32 rows x 32 k), FP32, 128-byte swizzle, reads
+// outside [0, inner) x [0, outer) zero-filled.
+int make_map(CUtensorMap &map, const GemmOperand &op, int rows, int K)
+{
+    auto enc = encoder();
+    if (!enc) {
+        set_error("cuTensorMapEncodeTiled is not available from the driver");
+        return IGA_ERR_CUDA;
+    }
+    if ((uintptr_t)op.ptr % 16 || (op.ld * 4) % 16) {
+        set_error("TF32 GEMM operands need 16-byte aligned rows");
+        return IGA_ERR_ARG;
+    }
+    const cuuint64_t inner = op.mn_major ? rows : K, outer = op.mn_major ? K : rows;
+    const cuuint64_t dims[2] = {inner, outer};
+    const cuuint64_t strides[1] = {(cuuint64_t)op.ld * 4};
+    const cuuint32_t box[2] = {32u, op.mn_major ? 32u : 128u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(op.ptr), dims, strides, box,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+        return IGA_ERR_CUDA;
+    }
+    return IGA_OK;
+}
+
+template <bool AMN, bool BMN, int OUT>
+int launch_tf32_t(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter &sc)
+{
+    static bool attr = false;   // per instantiation
+    if (!attr) {
+        if (cudaFuncSetAttribute(gemm_tf32_kernel<AMN, BMN, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kGSmem) != cudaSuccess)
+            return IGA_ERR_CUDA;
+        attr = true;
+    }
+    const dim3 grid((g.Mst + kGM - 1) / kGM, (g.Nst + kGN - 1) / kGN);
+    gemm_tf32_kernel<AMN, BMN, OUT><<<grid, 128, kGSmem, s>>>(g.ta, g.tb, g.K, g.Mst, g.Nst, g.C, g.ldc, err, sc);
+    return cudaPeekAtLastError() == cudaSuccess ? IGA_OK : IGA_ERR_CUDA;
+}
+
+template <bool AMN, bool BMN>
+int launch_tf32(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter &sc)
+{
+    if (!sc.out) return launch_tf32_t<AMN, BMN, 0>(g, s, err, sc);
+    return sc.f64 ? launch_tf32_t<AMN, BMN, 2>(g, s, err, sc) : launch_tf32_t<AMN, BMN, 1>(g, s, err, sc);
+}
+}  // namespace
+
+int gemm_tf32_prepare(GemmTF32 &g, GemmOperand A, GemmOperand B, float *C, int ldc, int M, int N, int K, int Mst,
+                      int Nst)
+{
+    g.ready = false;
+    int st;
+    if ((st = make_map(g.ta, A, M, K)) || (st = make_map(g.tb, B, N, K))) return st;
+    if ((uintptr_t)C % 16 || ldc % 4) {
+        set_error("TF32 GEMM output needs 16-byte aligned rows");
+        return IGA_ERR_ARG;
+    }
+    g.a_mn = A.mn_major;
+    g.b_mn = B.mn_major;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.Mst = Mst;
+    g.Nst = Nst;
+    g.C = C;
+    g.ldc = ldc;
+    g.ready = true;
+    return IGA_OK;
+}
+
+int gemm_tf32_launch(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter &sc)
+{
+    if (!g.ready) return IGA_ERR_ARG;
+    // the two operand layouts the preconditioner uses (both K-major, both MN-major)
+    if (g.a_mn && g.b_mn) return launch_tf32<true, true>(g, s, err, sc);
+    if (!g.a_mn && !g.b_mn) return launch_tf32<false, false>(g, s, err, sc);
+    set_error("TF32 GEMM: mixed operand layouts are not built");
+    return IGA_ERR_UNSUPPORTED;
+}
+
+// ------------------------------------------------------------ FP64 on DMMA
+// One CTA of 8 warps computes a 128 x 128 tile of C (warp tile 64 x 32 as
+// 4 x 4 blocks of the 16 x 8 x 8 FP64 MMA). K slices of 16 are staged by
+// 16-byte cp.async into a 3-deep ring: K-major operands as [row][k] with 20
+// doubles per row, MN-major ones as [k][row] with 132 per k, both of which
+// make a warp's fragment loads conflict-free. Rows and k past an operand's
+// extent are zero-filled (the matrices are zero-padded, so a 16-byte chunk
+// never straddles the end of the data).
+constexpr int kDM = 128, kDN = 128, kDK = 16, kDS = 3;
+constexpr int kDLK = 20, kDLR = 132;
+
+template <bool MN, int ROWS>
+struct DTile {
+    static constexpr int elems = MN ? kDK * kDLR : ROWS * kDLK;
+    __device__ static int at(int row, int k) { return MN ? k * kDLR + row : row * kDLK + k; }
+};
+
+// D (16 x 8) += A (16 x 8) B (8 x 8), FP64. Fragments (g = lane / 4,
+// t = lane % 4): a = A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4];
+// b = B[t][g], B[t+4][g]; d = D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1].
+__device__ __forceinline__ void dmma(double (&d)[4], const double (&a)[4], const double (&b)[2])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// Stages the slice k0 .. k0 + 15 of an operand tile (rows r0 .. r0 + ROWS - 1).
+template <bool MN, int ROWS>
+__device__ __forceinline__ void stage_f64(double *dst, const double *__restrict__ src, int ld, int rows, int K, int r0,
+                                          int k0, int tid)
+{
+    constexpr int CHUNKS = ROWS * kDK / 2;   // 16-byte chunks
+    for (int c = tid; c < CHUNKS; c += 256) {
+        int row, k;
+        if (MN) {   // [k][row] chunks along rows
+            k = c / (ROWS / 2);
+            row = 2 * (c % (ROWS / 2));
+        } else {    // [row][k] chunks along k
+            row = c / (kDK / 2);
+            k = 2 * (c % (kDK / 2));
+        }
+        const int gr = r0 + row, gk = k0 + k;
+        const bool v = gr < rows && gk < K;
+        const double *g = v ? (MN ? src + (size_t)gk * ld + gr : src + (size_t)gr * ld + gk) : src;
+        cp_async_zfill<16>(dst + DTile<MN, ROWS>::at(row, k), g, v);
+    }
+}
+
+template <bool AMN, bool BMN, bool SCATTER>
+__global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const double *__restrict__ A, int lda, const double *__restrict__ B,
+                                                          int ldb, double *__restrict__ C, int ldc, int M, int N, int K,
+                                                          int Mst, int Nst, GemmScatter sc)
+{
+    using TA = DTile<AMN, kDM>;
+    using TB = DTile<BMN, kDN>;
+    extern __shared__ __align__(16) double dsm[];
+    double *As = dsm, *Bs = dsm + kDS * TA::elems;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int wm = (w & 1) * 64, wn = (w >> 1) * 32;
+    const int m0 = blockIdx.x * kDM, n0 = blockIdx.y * kDN;
+    const int nk = (K + kDK - 1) / kDK;
+    double acc[4][4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[i][j][c] = 0.0;
+    for (int s = 0; s < kDS - 1; ++s) {
+        if (s < nk) {
+            stage_f64<AMN, kDM>(As + s * TA::elems, A, lda, M, K, m0, s * kDK, tid);
+            stage_f64<BMN, kDN>(Bs + s * TB::elems, B, ldb, N, K, n0, s * kDK, tid);
+        }
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < nk; ++kt) {
+        cp_async_wait<kDS - 2>();
+        __syncthreads();
+        {   // refill the stage consumed one iteration ago
+            const int nt = kt + kDS - 1, s = nt % kDS;
+            if (nt < nk) {
+                stage_f64<AMN, kDM>(As + s * TA::elems, A, lda, M, K, m0, nt * kDK, tid);
+                stage_f64<BMN, kDN>(Bs + s * TB::elems, B, ldb, N, K, n0, nt * kDK, tid);
+            }
+            cp_async_commit();
+        }
+        const double *a = As + (kt % kDS) * TA::elems, *b = Bs + (kt % kDS) * TB::elems;
+#pragma unroll
+        for (int kk = 0; kk < kDK; kk += 8) {
+            double av[4][4], bv[4][2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int r = wm + 16 * i + g;
+                av[i][0] = a[TA::at(r, kk + t4)];
+                av[i][1] = a[TA::at(r + 8, kk + t4)];
+                av[i][2] = a[TA::at(r, kk + t4 + 4)];
+                av[i][3] = a[TA::at(r + 8, kk + t4 + 4)];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                bv[j][0] = b[TB::at(wn + 8 * j + g, kk + t4)];
+                bv[j][1] = b[TB::at(wn + 8 * j + g, kk + t4 + 4)];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) dmma(acc[i][j], av[i], bv[j]);
+        }
+    }
+    cp_async_wait<0>();
+    // accumulator (i, j, c): row wm + 16 i + g + 8 (c / 2), column wn + 8 j + 2 t4 + c % 2
+    if constexpr (SCATTER) {
+        double f = 1.0;
+        if (sc.rr) {
+            const double rr = *sc.rr;
+            f = (rr > 0.0 && rr < 1e300) ? sqrt(rr) : 1.0;
+        }
+        double *out = static_cast<double *>(sc.out);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int row = m0 + wm + 16 * i + g + 8 * h;
+                if (row >= sc.rows) continue;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int c = 0; c < 2; ++c) {
+                        const int col = n0 + wn + 8 * j + 2 * t4 + c;
+                        if (col < sc.cols) out[(size_t)(row + 1) * sc.ld + col + 1] = f * acc[i][j][2 * h + c];
+                    }
+            }
+    } else {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int row = m0 + wm + 16 * i + g + 8 * h;
+            if (row >= Mst) continue;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int col = n0 + wn + 8 * j + 2 * t4;
+                double *dst = C + (size_t)row * ldc + col;
+                if (col + 1 < Nst) *reinterpret_cast<double2 *>(dst) = make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
+                else if (col < Nst) dst[0] = acc[i][j][2 * h];
+            }
+        }
+    }
+}
+
+namespace {
+template <bool AMN, bool BMN, bool SCATTER>
+int launch_f64(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst, cudaStream_t s,
+               const GemmScatter &sc)
+{
+    const size_t smem = (size_t)kDS * (DTile<AMN, kDM>::elems + DTile<BMN, kDN>::elems) * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(gemm_f64_kernel<AMN, BMN, SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return IGA_ERR_CUDA;
+        attr = true;
+    }
+    const dim3 grid((Mst + kDM - 1) / kDM, (Nst + kDN - 1) / kDN);
+    gemm_f64_kernel<AMN, BMN, SCATTER><<<grid, 256, smem, s>>>(static_cast<const double *>(A.ptr), A.ld,
+                                                               static_cast<const double *>(B.ptr), B.ld, C, ldc, M, N,
+                                                               K, Mst, Nst, sc);
+    return cudaPeekAtLastError() == cudaSuccess ? IGA_OK : IGA_ERR_CUDA;
+}
+}  // namespace
+
+int gemm_f64_launch(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst,
+                    cudaStream_t s, const GemmScatter &sc)
+{
+    if ((uintptr_t)A.ptr % 16 || (uintptr_t)B.ptr % 16 || A.ld % 2 || B.ld % 2 || (uintptr_t)C % 16 || ldc % 2 ||
+        (sc.out && !sc.f64)) {
+        set_error("FP64 GEMM operands need 16-byte aligned rows (and an FP64 scatter target)");
+        return IGA_ERR_ARG;
+    }
+    // the two operand layouts the preconditioner uses (both K-major, both MN-major)
+    if (!A.mn_major && !B.mn_major && !sc.out) return launch_f64<false, false, false>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+    if (A.mn_major && B.mn_major) {
+        if (sc.out) return launch_f64<true, true, true>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+        return launch_f64<true, true, false>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+    }
+    set_error("FP64 GEMM: this operand layout / output combination is not built");
+    return IGA_ERR_UNSUPPORTED;
+}
+
+}  // namespace iga

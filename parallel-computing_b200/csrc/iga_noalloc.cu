@@ -14,7 +14,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <mutex>
+#include <string>
 
 #include "iga_apply.cuh"
 #include "iga_plan.hpp"
@@ -106,19 +108,25 @@ __global__ void noalloc_tables_kernel(double *__restrict__ tabX, double *__restr
     }
 }
 
+// Scratch layout: a 256-byte head (the kernels' error slot at byte 0, the
+// IEN / ID check flags at byte 4), the words marking ID values already seen
+// (when d_ID is given), then the tables and the seam frames.
 struct Layout {
-    size_t off_err, off_wq, off_tabX, off_tabY, off_frame, total;
+    size_t off_err, off_flags, off_seen, off_wq, off_tabX, off_tabY, off_frame, total;
 };
 
 size_t up256(size_t v) { return (v + 255) & ~size_t(255); }
 
-Layout layout_for(int P, int nex, int ney, int TY)
+Layout layout_for(int P, int nex, int ney, int TY, bool with_id)
 {
     const int NB = P + 1, NQ = P + 1, QH = (NQ + 1) / 2;
     const long long NSX = (nex + iga::kSW - 1) / iga::kSW, NSY = (ney + TY - 1) / TY;
+    const long long N = (long long)(nex + P) * (ney + P);
     Layout L;
     L.off_err = 0;
-    L.off_wq = 256;
+    L.off_flags = 4;
+    L.off_seen = 256;
+    L.off_wq = L.off_seen + (with_id ? up256(sizeof(unsigned) * (size_t)((N + 31) / 32)) : 0);
     L.off_tabX = L.off_wq + up256(sizeof(double) * NQ * NQ);
     L.off_tabY = L.off_tabX + up256(sizeof(double) * NSX * 2 * QH * NB * 32);
     L.off_frame = L.off_tabY + up256(sizeof(double) * (size_t)ney * 2 * NQ * iga::tab_nbp(NB, (int)sizeof(double)));
@@ -128,7 +136,7 @@ Layout layout_for(int P, int nex, int ney, int TY)
 
 template <int P>
 int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int ney, const double *d_CP,
-           const double *d_in, double *d_out, cudaStream_t s)
+           const int *d_ID, const double *d_in, double *d_out, cudaStream_t s)
 {
     using namespace iga;
     int W = apply_max_threads<P, double, 1>() / 32;
@@ -138,8 +146,11 @@ int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int 
     {
         std::lock_guard<std::mutex> lk(g_mu);
         if (!g_attr[dev][P]) {
-            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) {
+                set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
                 return IGA_ERR_CUDA;
+            }
             g_attr[dev][P] = true;
         }
     }
@@ -165,15 +176,37 @@ int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int 
     a.frame = reinterpret_cast<double *>(base + Ly.off_frame);
     a.g = g;
     a.sign = -1.0;   // the reference operator A_ref = -K
-    a.bc = IGA_BC_REFERENCE;
+    // the reference's serial numbering: y[Dir] = 0; any other ID: rows through ID
+    a.bc = d_ID ? IGA_BC_NONE : IGA_BC_REFERENCE;
+    a.ID = d_ID;
     a.err = reinterpret_cast<int *>(base + Ly.off_err);
     dim3 grid(g.NSX, (g.NSY + W - 1) / W), block(32, W);
     kern<<<grid, block, smem, s>>>(a);
+    cudaError_t e = cudaPeekAtLastError();
     const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
-    if (nseam > 0)
+    if (e == cudaSuccess && nseam > 0) {
         seam_fixup_kernel<P, double><<<(int)std::min<long long>((nseam + 255) / 256, 592), 256, 0, s>>>(
-            a.frame, d_in, d_out, g, -1.0, IGA_BC_REFERENCE);
-    return cudaGetLastError() == cudaSuccess ? IGA_OK : IGA_ERR_CUDA;
+            a.frame, d_in, d_out, g, -1.0, a.bc, d_ID);
+        e = cudaPeekAtLastError();
+    }
+    if (e != cudaSuccess) {
+        set_error(std::string("iga_MatrixFreeMatMultCUDA_noalloc launch: ") + cudaGetErrorString(e));
+        return IGA_ERR_CUDA;
+    }
+    return IGA_OK;
+}
+
+// Reads one int of the scratch back to the host after the stream's work
+// (into a host variable: nothing is allocated).
+int read_back(const unsigned char *base, size_t off, cudaStream_t s, int &out)
+{
+    cudaError_t e = cudaMemcpyAsync(&out, base + off, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        iga::set_error(std::string("iga_MatrixFreeMatMultCUDA_noalloc: ") + cudaGetErrorString(e));
+        return IGA_ERR_CUDA;
+    }
+    return IGA_OK;
 }
 
 }  // namespace
@@ -181,19 +214,32 @@ int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int 
 extern "C" int iga_MatrixFreeMatMultCUDA_noalloc(int p, int q, int nex, int ney, const double *d_B1,
                                                  const double *d_B2, const double *d_dB1, const double *d_dB2,
                                                  const double *d_C1, const double *d_C2, const double *,
-                                                 const double *, const int *, const int *, const double *d_CP,
-                                                 const double *qw1, const double *qw2, const double *d_in,
-                                                 double *d_out, void *stream)
+                                                 const double *, const int *d_IEN, const int *d_ID,
+                                                 const double *d_CP, const double *qw1, const double *qw2,
+                                                 const double *d_in, double *d_out, void *stream)
 {
-    if (p < 1 || p > 5 || q != p || nex < 1 || ney < 1) return p == q ? IGA_ERR_ARG : IGA_ERR_UNSUPPORTED;
+    if (p < 1 || q < 1 || nex < 1 || ney < 1) return IGA_ERR_ARG;
+    if (p > 5 || q != p) {
+        iga::set_error("iga_MatrixFreeMatMultCUDA_noalloc handles p == q with 1 <= p <= 5");
+        return IGA_ERR_UNSUPPORTED;
+    }
     if (!d_B1 || !d_B2 || !d_dB1 || !d_dB2 || !d_C1 || !d_C2 || !d_CP || !qw1 || !qw2 || !d_in || !d_out)
         return IGA_ERR_ARG;
+    // d_CP is read as 16-byte (x, y) pairs, the double arrays as doubles, IEN/ID as ints.
+    bool aligned = (uintptr_t)d_CP % 16 == 0 && (uintptr_t)d_IEN % 4 == 0 && (uintptr_t)d_ID % 4 == 0;
+    for (const double *q8 : {d_B1, d_B2, d_dB1, d_dB2, d_C1, d_C2, qw1, qw2, d_in, (const double *)d_out})
+        aligned = aligned && (uintptr_t)q8 % 8 == 0;
+    if (!aligned) {
+        iga::set_error("iga_MatrixFreeMatMultCUDA_noalloc: d_CP must be 16-byte aligned, the other double "
+                       "arrays 8-byte and d_IEN / d_ID 4-byte aligned");
+        return IGA_ERR_ARG;
+    }
     // Strip height: the smallest of these whose tables and frames fit the scratch.
     int TY = 0;
     Layout Ly{};
     for (int cand : {32, 64, 128, 256, 512, 1024}) {
         if (cand < p) continue;
-        Ly = layout_for(p, nex, ney, cand);
+        Ly = layout_for(p, nex, ney, cand, d_ID != nullptr);
         if (Ly.total <= kScratchBytes) {
             TY = cand;
             break;
@@ -203,6 +249,7 @@ extern "C" int iga_MatrixFreeMatMultCUDA_noalloc(int p, int q, int nex, int ney,
         iga::set_error("mesh too large for the fixed 16 MiB scratch of iga_MatrixFreeMatMultCUDA_noalloc");
         return IGA_ERR_UNSUPPORTED;
     }
+    (void)cudaGetLastError();   // an earlier, unrelated launch error is not this call's
     int dev = 0;
     unsigned char *base = static_cast<unsigned char *>(scratch_on_current_device(dev));
     if (!base) {
@@ -210,16 +257,38 @@ extern "C" int iga_MatrixFreeMatMultCUDA_noalloc(int p, int q, int nex, int ney,
         return IGA_ERR_CUDA;
     }
     cudaStream_t s = (cudaStream_t)stream;
+    // IEN / ID first: a call they do not fit is refused before y is touched.
+    const int *id_rows = nullptr;
+    if (d_IEN || d_ID) {
+        int st = iga::refentry_check(d_IEN, d_ID, p, nex, ney, reinterpret_cast<unsigned *>(base + Ly.off_seen),
+                                     reinterpret_cast<int *>(base + Ly.off_flags), s);
+        int flags = 0;
+        if (st == IGA_OK) st = read_back(base, Ly.off_flags, s, flags);
+        if (st == IGA_OK) st = iga::refentry_status(flags);
+        if (st) return st;
+        if (flags & iga::kCheckIDOrder) id_rows = d_ID;
+    }
     const int NSX = (nex + iga::kSW - 1) / iga::kSW;
     noalloc_tables_kernel<<<148, 256, 0, s>>>(
         reinterpret_cast<double *>(base + Ly.off_tabX), reinterpret_cast<double *>(base + Ly.off_tabY),
         reinterpret_cast<double *>(base + Ly.off_wq), reinterpret_cast<int *>(base + Ly.off_err), d_B1, d_dB1, d_B2,
         d_dB2, d_C1, d_C2, qw1, qw2, p, nex, ney, NSX);
+    int st;
     switch (p) {
-    case 1: return launch<1>(dev, base, Ly, TY, nex, ney, d_CP, d_in, d_out, s);
-    case 2: return launch<2>(dev, base, Ly, TY, nex, ney, d_CP, d_in, d_out, s);
-    case 3: return launch<3>(dev, base, Ly, TY, nex, ney, d_CP, d_in, d_out, s);
-    case 4: return launch<4>(dev, base, Ly, TY, nex, ney, d_CP, d_in, d_out, s);
-    default: return launch<5>(dev, base, Ly, TY, nex, ney, d_CP, d_in, d_out, s);
+    case 1: st = launch<1>(dev, base, Ly, TY, nex, ney, d_CP, id_rows, d_in, d_out, s); break;
+    case 2: st = launch<2>(dev, base, Ly, TY, nex, ney, d_CP, id_rows, d_in, d_out, s); break;
+    case 3: st = launch<3>(dev, base, Ly, TY, nex, ney, d_CP, id_rows, d_in, d_out, s); break;
+    case 4: st = launch<4>(dev, base, Ly, TY, nex, ney, d_CP, id_rows, d_in, d_out, s); break;
+    default: st = launch<5>(dev, base, Ly, TY, nex, ney, d_CP, id_rows, d_in, d_out, s); break;
     }
+    if (st) return st;
+    // Synchronous, like the reference's entry: the kernels' own error slot
+    // (a bounded wait that gave up) is read back before returning.
+    int err = 0;
+    if ((st = read_back(base, Ly.off_err, s, err))) return st;
+    if (err) {
+        iga::set_error("iga_MatrixFreeMatMultCUDA_noalloc: a kernel recorded an error");
+        return err;
+    }
+    return IGA_OK;
 }

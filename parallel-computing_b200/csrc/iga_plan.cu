@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -128,6 +129,74 @@ __global__ void rhs_kernel(double *__restrict__ F, const double *__restrict__ ta
             }
         F[t] = v;
     }
+}
+
+// Checks the connectivity and equation numbers a reference-shaped call
+// passes (device arrays, either may be null) against what this library's
+// structured kernels compute: IEN must be the single-patch connectivity of
+// matrix_free/src/IENGenerator.cpp:68-103 (element e = ey nex + ex, local
+// function a = jl (p+1) + il at control point (ey + jl) m + ex + il); ID may
+// be any map into [0, m n) that names no equation twice (negative: no row),
+// and is flagged when it differs from the reference's serial numbering
+// (matrix_free/src/Partition.cpp:102-108: -1 on the boundary ring, the
+// control point's own index elsewhere). seen: (m n + 31) / 32 zeroed words.
+__global__ void refentry_check_kernel(const int *__restrict__ IEN, const int *__restrict__ ID, int p, int nex,
+                                      int ney, unsigned *__restrict__ seen, int *__restrict__ flags)
+{
+    const int NB = p + 1, m = nex + p, n = ney + p;
+    const long long N = (long long)m * n, nien = IEN ? (long long)nex * ney * NB * NB : 0, nid = ID ? N : 0;
+    const long long total = nien > nid ? nien : nid;
+    int f = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        if (t < nien) {
+            const long long e = t / (NB * NB);
+            const int a = (int)(t - e * NB * NB);
+            const int ex = (int)(e % nex), ey = (int)(e / nex);
+            if (IEN[t] != (long long)(ey + a / NB) * m + ex + a % NB) f |= kCheckIEN;
+        }
+        if (t < nid) {
+            const int e = ID[t];
+            const int R = (int)(t / m), C = (int)(t % m);
+            const bool ring = R == 0 || C == 0 || R == n - 1 || C == m - 1;
+            if (ring ? e >= 0 : e != t) f |= kCheckIDOrder;
+            if (e >= N) f |= kCheckIDRange;
+            else if (e >= 0) {
+                const unsigned bit = 1u << (e & 31);
+                if (atomicOr(&seen[e >> 5], bit) & bit) f |= kCheckIDTwice;
+            }
+        }
+    }
+    if (f) atomicOr(flags, f);
+}
+
+int refentry_check(const int *IEN, const int *ID, int p, int nex, int ney, unsigned *seen, int *flags,
+                   cudaStream_t s)
+{
+    const long long N = (long long)(nex + p) * (ney + p);
+    if (cudaMemsetAsync(flags, 0, sizeof(int), s) != cudaSuccess) return IGA_ERR_CUDA;
+    if (!IEN && !ID) return IGA_OK;
+    if (ID && cudaMemsetAsync(seen, 0, (size_t)((N + 31) / 32) * sizeof(unsigned), s) != cudaSuccess)
+        return IGA_ERR_CUDA;
+    refentry_check_kernel<<<4 * 148, 256, 0, s>>>(IEN, ID, p, nex, ney, seen, flags);
+    return cudaPeekAtLastError() == cudaSuccess ? IGA_OK : IGA_ERR_CUDA;
+}
+
+int refentry_status(int flags)
+{
+    if (flags & kCheckIEN) {
+        set_error("d_IEN is not the structured single-patch connectivity (IENGenerator::GenerateIEN2D order)");
+        return IGA_ERR_UNSUPPORTED;
+    }
+    if (flags & kCheckIDRange) {
+        set_error("d_ID maps a control point to an equation number >= (nElemX+p)*(nElemY+q)");
+        return IGA_ERR_UNSUPPORTED;
+    }
+    if (flags & kCheckIDTwice) {
+        set_error("d_ID gives two control points the same equation number");
+        return IGA_ERR_UNSUPPORTED;
+    }
+    return IGA_OK;
 }
 
 // ---------------------------------------------------------------- helpers
@@ -295,9 +364,11 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
 }
 
 // Win: a window of strip rows (gyn >= 0: strip rows gy0 .. gy0 + gyn - 1, and
-// the seams of control-point rows R0 .. R1 - 1 instead of all seams).
+// the seams of control-point rows R0 .. R1 - 1 instead of all seams); ID:
+// equation numbers of the rows (ApplyParams::ID), null for the natural order.
 struct Win {
     int gy0 = 0, gyn = -1, R0 = 0, R1 = 0;
+    const int *ID = nullptr;
 };
 
 template <int P, typename T, int GEOM, int NST>
@@ -318,6 +389,8 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
     a.sign = (T)sign;
     a.bc = bc;
     a.err = pl->d_err;
+    a.ID = win.ID;
+    if (pl->wait_polls >= 0) a.wait_polls = pl->wait_polls;
     const int W = op.warps;
     const size_t smem = apply_smem_bytes<P, T, GEOM, NST>(W);
     auto kern = apply_kernel<P, T, GEOM, NST>;
@@ -343,13 +416,13 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
             // (L2 hits) are all in flight at once (p=3 2048^2 FP64 MatMult:
             // 309.5 us with 7 points per thread, 306 us with one)
             const int blocks = (int)std::min<long long>((nseam + 255) / 256, 32 * 148);
-            seam_fixup_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)sign, bc);
+            seam_fixup_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)sign, bc, win.ID);
         }
     } else if (win.R1 > win.R0) {
         const long long nseam = (long long)(g.NSX - 1) * P * (win.R1 - win.R0) + (long long)2 * P * g.m * (rows + 1);
         const int blocks = (int)std::max<long long>(1, std::min<long long>((nseam + 255) / 256, 4 * 148));
         seam_fixup_rows_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)sign, bc, win.R0,
-                                                             win.R1);
+                                                             win.R1, win.ID);
     }
     IGA_CUDA_TRY(cudaGetLastError());
     return IGA_OK;
@@ -390,6 +463,12 @@ int iga_apply_internal_sb(iga_plan *pl, int prec, const void *x, void *y, cudaSt
 
 int iga_apply_internal(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s)
 {
+    if (pl->eq_id) {   // rows in the caller's equation numbering (reference-shaped entry)
+        if (prec != IGA_FP64 || !pl->op64.ready) return IGA_ERR_ARG;
+        Win w;
+        w.ID = pl->eq_id;
+        return launch_apply<double>(pl, pl->op64, (const double *)x, (double *)y, s, pl->sign, IGA_BC_NONE, w);
+    }
     return iga_apply_internal_sb(pl, prec, x, y, s, pl->sign, pl->bc);
 }
 
@@ -610,7 +689,7 @@ int iga_plan_destroy(iga_plan *pl)
     free_op(pl->op64);
     free_op(pl->op32);
     for (void *p : {(void *)pl->tabX64, (void *)pl->tabY64, (void *)pl->CP, (void *)pl->qw, (void *)pl->d_err,
-                    (void *)pl->kappa_dev,
+                    (void *)pl->kappa_dev, (void *)pl->eq_id,
                     (void *)pl->h_stage_x, (void *)pl->d_stage_x, (void *)pl->d_stage_y})
         if (p) cudaFree(p);
     if (pl->h_pinned) cudaFreeHost(pl->h_pinned);
@@ -676,16 +755,45 @@ int iga_plan_set_kappa(iga_plan *pl, const double *kappa, void *stream)
     return IGA_OK;
 }
 
+static bool aligned_vectors(int prec, const void *x, const void *y)
+{
+    const uintptr_t es = prec == IGA_FP32 ? 4 : 8;
+    if ((uintptr_t)x % es == 0 && (uintptr_t)y % es == 0) return true;
+    set_error("x and y must be aligned to their element size");
+    return false;
+}
+
 int iga_apply(iga_plan *pl, const void *x, void *y, void *stream)
 {
     if (!pl || !x || !y) return IGA_ERR_ARG;
-    return iga_apply_internal(pl, pl->precision == IGA_FP32 ? IGA_FP32 : IGA_FP64, x, y, (cudaStream_t)stream);
+    const int prec = pl->precision == IGA_FP32 ? IGA_FP32 : IGA_FP64;
+    if (!aligned_vectors(prec, x, y)) return IGA_ERR_ARG;
+    return iga_apply_internal(pl, prec, x, y, (cudaStream_t)stream);
 }
 
 int iga_apply_prec(iga_plan *pl, int prec, const void *x, void *y, void *stream)
 {
     if (!pl || !x || !y || (prec != IGA_FP64 && prec != IGA_FP32)) return IGA_ERR_ARG;
+    if (!aligned_vectors(prec, x, y)) return IGA_ERR_ARG;
     return iga_apply_internal(pl, prec, x, y, (cudaStream_t)stream);
+}
+
+int iga_plan_device_status(iga_plan *pl, void *stream)
+{
+    if (!pl) return IGA_ERR_ARG;
+    IGA_CUDA_TRY(cudaSetDevice(pl->device));
+    IGA_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    const int st = iga_check_error_flag(pl);
+    if (st == IGA_ERR_TIMEOUT) set_error("a bounded device wait of this plan's kernels gave up");
+    else if (st) set_error("this plan's kernels recorded an error");
+    return st;
+}
+
+int iga_plan_set_wait_limit(iga_plan *pl, long long polls)
+{
+    if (!pl) return IGA_ERR_ARG;
+    pl->wait_polls = polls < 0 ? -1 : polls;
+    return IGA_OK;
 }
 
 // Host buffers: the patch is applied in up to kHostSlabs slabs of strip rows
@@ -767,52 +875,143 @@ int iga_rhs(iga_plan *pl, int fkind, double *F, void *stream)
 
 // ------------------------------------------------- reference-shaped entry point
 namespace {
-struct CachedPlan {
-    iga_plan *plan;
-};
+// Cached plans, keyed by the device and every array pointer of the call; the
+// arrays' contents are assumed unchanged while a plan is cached (a caller
+// that rewrites them in place calls iga_MatrixFreeMatMultCUDA_release first).
+using CacheKey = std::array<long long, 16>;
 std::mutex g_cache_mu;
-std::map<std::tuple<int, int, int, int, const void *, const void *, const void *>, CachedPlan> g_cache;
+std::map<CacheKey, iga_plan *> g_cache;
+
+// The caller's Bernstein tables and Gauss weights (matrix_free_gpu/src/
+// GlobalAssemblyMF.cu:156-169: B[k][i] at quadrature point k) must be the
+// (p+1)-point Gauss rule this library integrates with.
+int check_rule(int p, const double *dB1, const double *dB2, const double *ddB1, const double *ddB2,
+               const double *dqw1, const double *dqw2)
+{
+    const double *ptrs[6] = {dB1, dB2, ddB1, ddB2, dqw1, dqw2};
+    int given = 0;
+    for (const double *q : ptrs) given += q != nullptr;
+    if (given == 0) return IGA_OK;   // not passed: the library's own rule
+    if (given != 6) {
+        set_error("d_B1, d_B2, d_dB1, d_dB2, qw1 and qw2 must be given together (or all NULL)");
+        return IGA_ERR_ARG;
+    }
+    const int NB = p + 1, NQ = p + 1;
+    std::vector<double> qx(NQ), qw(NQ), B((size_t)NQ * NB), dB((size_t)NQ * NB);
+    gauss01(NQ, qx.data(), qw.data());
+    for (int k = 0; k < NQ; ++k) bernstein(p, qx[k], B.data() + k * NB, dB.data() + k * NB);
+    const std::vector<double> *want[6] = {&B, &B, &dB, &dB, &qw, &qw};
+    for (int t = 0; t < 6; ++t) {
+        std::vector<double> got(want[t]->size());
+        IGA_CUDA_TRY(cudaMemcpy(got.data(), ptrs[t], got.size() * 8, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < got.size(); ++i)
+            if (!(std::fabs(got[i] - (*want[t])[i]) <= 1e-13 * (1.0 + std::fabs((*want[t])[i])))) {
+                set_error("the Bernstein tables / quadrature weights passed differ from the (p+1)-point "
+                          "Gauss rule this library integrates with");
+                return IGA_ERR_UNSUPPORTED;
+            }
+    }
+    return IGA_OK;
+}
+
+// Builds the cached plan of one reference-shaped call: mesh tables copied
+// once to the host, IEN / ID checked on the device, a plan with on-the-fly
+// geometry (the reference kernel recomputes geometry too) and, for an ID
+// other than the reference's serial numbering, a copy of ID for the rows.
+int build_cached(int p, int q, int nex, int ney, const double *d_C1, const double *d_C2, const int *d_IEN,
+                 const int *d_ID, const double *d_CP, iga_plan **out)
+{
+    const long long nf = (long long)(nex + p) * (ney + q);
+    std::vector<double> CP(2 * nf), C1((size_t)nex * (p + 1) * (p + 1)), C2((size_t)ney * (q + 1) * (q + 1));
+    IGA_CUDA_TRY(cudaMemcpy(CP.data(), d_CP, CP.size() * 8, cudaMemcpyDeviceToHost));
+    IGA_CUDA_TRY(cudaMemcpy(C1.data(), d_C1, C1.size() * 8, cudaMemcpyDeviceToHost));
+    IGA_CUDA_TRY(cudaMemcpy(C2.data(), d_C2, C2.size() * 8, cudaMemcpyDeviceToHost));
+    int flags = 0;
+    if (d_IEN || d_ID) {
+        unsigned *seen = nullptr;
+        int *dflags = nullptr;
+        IGA_CUDA_TRY(cudaMalloc((void **)&seen, (size_t)((nf + 31) / 32) * sizeof(unsigned) + 16));
+        cudaError_t e = cudaMalloc((void **)&dflags, sizeof(int));
+        int st = e == cudaSuccess ? refentry_check(d_IEN, d_ID, p, nex, ney, seen, dflags, 0) : IGA_ERR_NOMEM;
+        if (st == IGA_OK && cudaMemcpy(&flags, dflags, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+            st = IGA_ERR_CUDA;
+        cudaFree(seen);
+        if (dflags) cudaFree(dflags);
+        if (st) {
+            set_error("checking d_IEN / d_ID failed");
+            return st;
+        }
+        if ((st = refentry_status(flags))) return st;
+    }
+    iga_mesh_desc d{};
+    d.p = p;
+    d.q = q;
+    d.nElemX = nex;
+    d.nElemY = ney;
+    d.CP = CP.data();
+    d.C1 = C1.data();
+    d.C2 = C2.data();
+    iga_opts o;
+    iga_opts_default(&o);
+    IGA_CUDA_TRY(cudaGetDevice(&o.device));
+    o.geometry = IGA_GEOM_ON_THE_FLY;
+    iga_plan *pl = nullptr;
+    int st = iga_plan_create(&d, &o, &pl);
+    if (st) return st;
+    if (flags & kCheckIDOrder) {
+        cudaError_t e = cudaMalloc((void **)&pl->eq_id, nf * sizeof(int));
+        if (e == cudaSuccess) e = cudaMemcpy(pl->eq_id, d_ID, nf * sizeof(int), cudaMemcpyDeviceToDevice);
+        if (e != cudaSuccess) {
+            iga_plan_destroy(pl);
+            set_error(std::string("copying d_ID: ") + cudaGetErrorString(e));
+            return e == cudaErrorMemoryAllocation ? IGA_ERR_NOMEM : IGA_ERR_CUDA;
+        }
+    }
+    *out = pl;
+    return IGA_OK;
+}
 }  // namespace
 
-int iga_MatrixFreeMatMultCUDA(int p, int q, int nex, int ney, const double *, const double *, const double *,
-                              const double *, const double *d_C1, const double *d_C2, const double *,
-                              const double *, const int *, const int *, const double *d_CP, const double *,
-                              const double *, const double *d_in, double *d_out)
+int iga_MatrixFreeMatMultCUDA(int p, int q, int nex, int ney, const double *d_B1, const double *d_B2,
+                              const double *d_dB1, const double *d_dB2, const double *d_C1, const double *d_C2,
+                              const double *, const double *, const int *d_IEN, const int *d_ID, const double *d_CP,
+                              const double *qw1, const double *qw2, const double *d_in, double *d_out)
 {
-    if (!d_C1 || !d_C2 || !d_CP || !d_in || !d_out || nex < 1 || ney < 1) return IGA_ERR_ARG;
+    if (!d_C1 || !d_C2 || !d_CP || !d_in || !d_out || nex < 1 || ney < 1 || p < 1 || q < 1) return IGA_ERR_ARG;
+    if ((uintptr_t)d_in % 8 || (uintptr_t)d_out % 8) {
+        set_error("d_F_array_in / d_F_array_out must be 8-byte aligned");
+        return IGA_ERR_ARG;
+    }
+    int dev = 0;
+    IGA_CUDA_TRY(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lk(g_cache_mu);
-    auto key = std::make_tuple(p, q, nex, ney, (const void *)d_CP, (const void *)d_C1, (const void *)d_C2);
+    const void *ptrs[11] = {d_CP, d_C1, d_C2, d_IEN, d_ID, d_B1, d_B2, d_dB1, d_dB2, qw1, qw2};
+    CacheKey key{dev, p, q, nex, ney};
+    for (int k = 0; k < 11; ++k) key[5 + k] = (long long)(uintptr_t)ptrs[k];
     auto it = g_cache.find(key);
     if (it == g_cache.end()) {
-        const long long nf = (long long)(nex + p) * (ney + q);
-        std::vector<double> CP(2 * nf), C1((size_t)nex * (p + 1) * (p + 1)), C2((size_t)ney * (q + 1) * (q + 1));
-        IGA_CUDA_TRY(cudaMemcpy(CP.data(), d_CP, CP.size() * 8, cudaMemcpyDeviceToHost));
-        IGA_CUDA_TRY(cudaMemcpy(C1.data(), d_C1, C1.size() * 8, cudaMemcpyDeviceToHost));
-        IGA_CUDA_TRY(cudaMemcpy(C2.data(), d_C2, C2.size() * 8, cudaMemcpyDeviceToHost));
-        iga_mesh_desc d{};
-        d.p = p;
-        d.q = q;
-        d.nElemX = nex;
-        d.nElemY = ney;
-        d.CP = CP.data();
-        d.C1 = C1.data();
-        d.C2 = C2.data();
-        iga_opts o;
-        iga_opts_default(&o);
-        cudaGetDevice(&o.device);
-        o.geometry = IGA_GEOM_ON_THE_FLY;   // the reference kernel recomputes geometry too
-        iga_plan *pl = nullptr;
-        const int st = iga_plan_create(&d, &o, &pl);
+        if (p != q) {
+            set_error("this library requires p == q");
+            return IGA_ERR_UNSUPPORTED;
+        }
+        int st = check_rule(p, d_B1, d_B2, d_dB1, d_dB2, qw1, qw2);
         if (st) return st;
-        it = g_cache.emplace(key, CachedPlan{pl}).first;
+        iga_plan *pl = nullptr;
+        if ((st = build_cached(p, q, nex, ney, d_C1, d_C2, d_IEN, d_ID, d_CP, &pl))) return st;
+        it = g_cache.emplace(key, pl).first;
     }
-    return iga_apply_internal(it->second.plan, IGA_FP64, d_in, d_out, 0);
+    // Synchronous, as the reference's entry (cudaDeviceSynchronize after its
+    // kernel, matrix_free_gpu/src/mult.cu:550): the status covers the launch
+    // and every bounded wait of the kernels.
+    const int st = iga_apply_internal(it->second, IGA_FP64, d_in, d_out, 0);
+    if (st) return st;
+    return iga_plan_device_status(it->second, nullptr);
 }
 
 int iga_MatrixFreeMatMultCUDA_release(void)
 {
     std::lock_guard<std::mutex> lk(g_cache_mu);
-    for (auto &kv : g_cache) iga_plan_destroy(kv.second.plan);
+    for (auto &kv : g_cache) iga_plan_destroy(kv.second);
     g_cache.clear();
     return IGA_OK;
 }

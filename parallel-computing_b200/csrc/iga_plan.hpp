@@ -30,6 +30,15 @@ struct SolverState;   // defined by the solver translation unit
 void set_error(const std::string &s);
 const std::string &last_error();
 
+// Checks of a reference-shaped call's d_IEN / d_ID (refentry_check_kernel):
+// flag bits, the stream-ordered launcher (flags: one device int; seen:
+// (m n + 31) / 32 device words; nothing is allocated) and the status the
+// flags mean (IGA_OK when the call can run, kCheckIDOrder alone included).
+enum { kCheckIEN = 1, kCheckIDOrder = 2, kCheckIDRange = 4, kCheckIDTwice = 8 };
+int refentry_check(const int *IEN, const int *ID, int p, int nex, int ney, unsigned *seen, int *flags,
+                   cudaStream_t s);
+int refentry_status(int flags);
+
 // Largest warps per CTA of the apply kernel for degree P, precision
 // (IGA_FP64 / IGA_FP32) and geometry mode that fits the shared-memory budget.
 int warps_for(int P, int prec, int geom);
@@ -56,6 +65,12 @@ struct iga_plan {
     cudaEvent_t host_ev0 = nullptr;
     void *h_pinned = nullptr;
     iga::SolverState *solver = nullptr;
+    // Equation number of every control point (the reference's ID array) when
+    // the reference-shaped entry point was given one other than the natural
+    // order with -1 on the boundary ring; null otherwise.
+    int *eq_id = nullptr;
+    // Polls of the apply kernel's bounded waits (< 0: the default limit).
+    long long wait_polls = -1;
 };
 
 int iga_apply_internal(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s);

@@ -7,7 +7,6 @@
 // scalar (alpha, beta, dot products) and every convergence test lives on the
 // device; the host only reads one flag per outer iteration. All reductions
 // are deterministic (fixed-order block partials, summed by the last block).
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,13 +21,13 @@
 #include "../../include/iga_solve.h"
 #include "iga_fastdiag.hpp"
 #include "iga_fem.hpp"
+#include "iga_gemm.hpp"
 #include "iga_plan.hpp"
 
 namespace iga {
 
 constexpr int kRedBlocks = 592;   // fixed grid of every reduction kernel (4 x 148 SMs)
 constexpr int kThreads = 256;
-constexpr size_t kBlasWorkspace = size_t(256) << 20;   // cuBLAS workspace of a solver (bytes)
 constexpr int kChunk = 16;        // inner CG iterations per captured graph
 
 struct DevScalars {
@@ -751,25 +750,7 @@ __global__ void fd_gather_kernel(const V *__restrict__ r, T *__restrict__ U, V *
         }
 }
 
-template <typename T, typename V>
-__global__ void fd_scatter_kernel(const T *__restrict__ Z, V *__restrict__ z, int m, int nx, int ny, int nxp,
-                                  const DevScalars *sc)
-{
-    constexpr int VN = Pk<T>::n;
-    const double f = sc ? pc_scale(sc) : 1.0;
-    const int nv = (nx + VN - 1) / VN;
-    for (int b = blockIdx.y; b < ny; b += gridDim.y)
-        for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += gridDim.x * blockDim.x) {
-            const Pk<T> zv = ldp(Z, (long long)b * nxp + (long long)k * VN);
-#pragma unroll
-            for (int c = 0; c < VN; ++c) {
-                const int a = k * VN + c;
-                if (a < nx) z[(size_t)(b + 1) * m + (a + 1)] = (V)(f * (double)zv.v[c]);
-            }
-        }
-}
-
-// 2-D launch of the gather / scatter: 128-thread blocks over the 16-byte
+// 2-D launch of the gather: 128-thread blocks over the 16-byte
 // groups of a column, one block row per column (at most 65535).
 static dim3 grid2d(int ngroups, int ncols)
 {
@@ -831,6 +812,7 @@ struct PrecState {
     T *Vx = nullptr, *lx = nullptr, *W1 = nullptr, *W2 = nullptr, *Dv = nullptr;
     T *Lf = nullptr;   // LDL^T unit lower factor's subdiagonal per x mode (layout of Dv)
     int nxp = 0, nyp = 0;   // transform sizes padded to multiples of 16
+    GemmTF32 g1, g2;        // FP32: the two transforms' prepared tensor-core GEMMs
     int tri_w = 0;          // most warps per CTA of the staged tridiagonal kernel (0: in place)
     size_t tri_smem = 0;    // its shared memory at tri_w warps
     int nsm = 148;          // SMs of the plan's device
@@ -851,8 +833,6 @@ struct PrecState {
 struct SolverState {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cublasHandle_t blas = nullptr;
-    void *blas_ws = nullptr;   // fixed cuBLAS workspace (no allocation inside graph capture)
     bool fd_host = false;
     std::vector<double> lamx, Vx;             // host x eigenpairs (built once)
     std::vector<double> Dv, Lf;               // host LDL^T factors of the y systems, [a][b]
@@ -1011,8 +991,6 @@ void iga_solver_release(iga_plan *pl)
                     (void *)S->ks64, (void *)S->ks32})
         if (v) cudaFree(v);
     if (S->h) cudaFreeHost(S->h);
-    if (S->blas) cublasDestroy(S->blas);
-    if (S->blas_ws) cudaFree(S->blas_ws);
     if (S->stream) cudaStreamDestroy(S->stream);
     delete S;
     pl->solver = nullptr;
@@ -1108,6 +1086,17 @@ static int fd_setup(PrecState<double> &, const iga_plan *pl, SolverState *S)
     return IGA_OK;
 }
 
+static int prepare_gemms(PrecState<double> &) { return IGA_OK; }
+static int prepare_gemms(PrecState<float> &ps)
+{
+    const int nxp = ps.nxp, nyp = ps.nyp;
+    int st = gemm_tf32_prepare(ps.g1, GemmOperand{ps.Vx, nxp, false}, GemmOperand{ps.W2, nxp, false}, ps.W1, nyp, nxp,
+                               nyp, nxp, nxp, nyp);
+    if (st) return st;
+    return gemm_tf32_prepare(ps.g2, GemmOperand{ps.W1, nyp, true}, GemmOperand{ps.Vx, nxp, true}, ps.W2, nxp, nyp, nxp,
+                             nxp, nyp, nxp);
+}
+
 template <typename T>
 static int fd_upload(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
 {
@@ -1157,35 +1146,32 @@ static int fd_upload(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
                                        (int)ps.tri_smem));
     SOLVE_TRY(cudaMalloc((void **)&ps.W1, sizeof(T) * (size_t)nxp * nyp));
     SOLVE_TRY(cudaMalloc((void **)&ps.W2, sizeof(T) * (size_t)nxp * nyp));
-    if (!S->blas) {
-        if (cublasCreate(&S->blas) != CUBLAS_STATUS_SUCCESS) {
-            set_error("cublasCreate failed");
-            return IGA_ERR_CUDA;
-        }
-        SOLVE_TRY(cudaMalloc(&S->blas_ws, kBlasWorkspace));
-        if (cublasSetWorkspace(S->blas, S->blas_ws, kBlasWorkspace) != CUBLAS_STATUS_SUCCESS) {
-            set_error("cublasSetWorkspace failed");
-            return IGA_ERR_CUDA;
-        }
-    }
-    return IGA_OK;
+    return prepare_gemms(ps);
 }
 
-static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
-                           const double *A, int lda, const double *B, int ldb, double *C, int ldc)
+// The transforms' GEMMs in the row-major views of the work matrices:
+//   W1[a][b] = sum_k Vx[a][k] W2[b][k]   (both operands K-major),
+//   W2[b][i] = sum_a W1[a][b] Vx[a][i]   (both operands MN-major),
+// with Vx[a][k] = component k of eigenvector a (ld nxp), W1 [nxp][nyp],
+// W2 [nyp][nxp]. FP32: tcgen05 TF32 tiles fed by tensor maps built here once
+// (the preconditioner only has to be a close SPD approximation of K_fem^-1;
+// the flexible PCG and the FP64 refinement absorb the difference); FP64:
+// DMMA tiles.
+static int transform_gemm(PrecState<double> &ps, const iga_plan *, int which, cudaStream_t s,
+                          const GemmScatter &sc = GemmScatter())
 {
-    const double one = 1.0, zero = 0.0;
-    return cublasDgemm(h, ta, tb, m, n, k, &one, A, lda, B, ldb, &zero, C, ldc);
+    const int nxp = ps.nxp, nyp = ps.nyp;
+    if (which == 1)
+        return gemm_f64_launch(GemmOperand{ps.Vx, nxp, false}, GemmOperand{ps.W2, nxp, false}, ps.W1, nyp, nxp, nyp,
+                               nxp, nxp, nyp, s);
+    return gemm_f64_launch(GemmOperand{ps.W1, nyp, true}, GemmOperand{ps.Vx, nxp, true}, ps.W2, nxp, nyp, nxp, nxp, nyp,
+                           nxp, s, sc);
 }
 
-// FP32 preconditioner GEMMs run on the TF32 tensor cores: the preconditioner
-// only has to be a close SPD approximation of K_fem^-1.
-static cublasStatus_t gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
-                           const float *A, int lda, const float *B, int ldb, float *C, int ldc)
+static int transform_gemm(PrecState<float> &ps, const iga_plan *pl, int which, cudaStream_t s,
+                          const GemmScatter &sc = GemmScatter())
 {
-    const float one = 1.0f, zero = 0.0f;
-    return cublasGemmEx(h, ta, tb, m, n, k, &one, A, CUDA_R_32F, lda, B, CUDA_R_32F, ldb, &zero, C, CUDA_R_32F, ldc,
-                        CUBLAS_COMPUTE_32F_FAST_TF32, CUBLAS_GEMM_DEFAULT);
+    return gemm_tf32_launch(which == 1 ? ps.g1 : ps.g2, s, pl->d_err, sc);
 }
 
 // z = K_fem^-1 r on the free nodes (R, Z: the interior blocks of r, z,
@@ -1209,16 +1195,10 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
     const int nxp = ps.nxp, nyp = ps.nyp;
     int seg = (ny + 31) / 32;
     seg |= 1;   // odd: conflict-free shared-memory rows
-    // cublasSetStream puts the handle back on cuBLAS's own workspace pool;
-    // the fixed workspace goes back with it, or a GEMM captured into the
-    // solver's loop graph allocates (a memory-allocation node, which a
-    // conditional body may not hold)
-    cublasSetStream(S->blas, S->stream);
-    cublasSetWorkspace(S->blas, S->blas_ws, kBlasWorkspace);
     constexpr int VN = Pk<T>::n;
     fd_gather_kernel<T, V><<<grid2d(nxp / VN, nyp), 128, 0, S->stream>>>(r, ps.W2, z, m, n, nx, ny, nxp, nyp, sc);
-    cublasStatus_t e = gemm(S->blas, CUBLAS_OP_T, CUBLAS_OP_N, nyp, nxp, nxp, ps.W2, nxp, ps.Vx, nxp, ps.W1, nyp);
-    if (e == CUBLAS_STATUS_SUCCESS) {
+    int e = transform_gemm(ps, pl, 1, S->stream);
+    if (e == IGA_OK) {
         if (ps.tri_w) {
             // one mode per warp as long as the modes reach every SM, else the most
             // warps per CTA that shared memory allows (warps then loop over modes)
@@ -1229,13 +1209,20 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
         } else {
             fd_tri_kernel<T, false><<<(nx + 7) / 8, 256, 0, S->stream>>>(ps.W1, ps.Lf, ps.Dv, nx, ny, nyp, seg, S->s);
         }
-        e = gemm(S->blas, CUBLAS_OP_N, CUBLAS_OP_T, nxp, nyp, nxp, ps.Vx, nxp, ps.W1, nyp, ps.W2, nxp);
+        // the second GEMM's epilogue writes z's interior itself
+        GemmScatter gs;
+        gs.out = z;
+        gs.f64 = std::is_same<V, double>::value;
+        gs.ld = m;
+        gs.rows = ny;
+        gs.cols = nx;
+        gs.rr = sc ? &sc->rr : nullptr;
+        e = transform_gemm(ps, pl, 2, S->stream, gs);
     }
-    if (e != CUBLAS_STATUS_SUCCESS) {
-        set_error("cuBLAS GEMM failed in the FEM preconditioner");
-        return IGA_ERR_CUDA;
+    if (e != IGA_OK) {
+        set_error("GEMM launch failed in the FEM preconditioner: " + last_error());
+        return e;
     }
-    fd_scatter_kernel<T, V><<<grid2d((nx + VN - 1) / VN, ny), 128, 0, S->stream>>>(ps.W2, z, m, nx, ny, nxp, sc);
     return IGA_OK;
 }
 

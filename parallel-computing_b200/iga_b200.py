@@ -105,6 +105,8 @@ SIGNATURES = [
     ("iga_apply_prec", ctypes.c_int, [VP, ctypes.c_int, VP, VP, VP]),
     ("iga_apply_host", ctypes.c_int, [VP, VP, VP]),
     ("iga_rhs", ctypes.c_int, [VP, ctypes.c_int, VP, VP]),
+    ("iga_plan_device_status", ctypes.c_int, [VP, VP]),
+    ("iga_plan_set_wait_limit", ctypes.c_int, [VP, ctypes.c_longlong]),
     ("iga_MatrixFreeMatMultCUDA", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 15),
     ("iga_MatrixFreeMatMultCUDA_release", ctypes.c_int, []),
     ("iga_MatrixFreeMatMultCUDA_noalloc", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 16),
@@ -525,6 +527,15 @@ class Plan:
     def rhs(self, F, fkind=F_REFERENCE, stream=None):
         _check(_lib().iga_rhs(self.h, fkind, _ptr(F), _stream(stream)), "iga_rhs")
         return F
+
+    def device_status(self, stream=None):
+        """Synchronises the stream and returns (and clears) the status the
+        plan's kernels recorded (IGA_OK or e.g. IGA_ERR_TIMEOUT)."""
+        return _lib().iga_plan_device_status(self.h, _stream(stream))
+
+    def set_wait_limit(self, polls):
+        """Test hook: polls per bounded wait of the MatMult kernel (< 0: default)."""
+        _check(_lib().iga_plan_set_wait_limit(self.h, int(polls)), "iga_plan_set_wait_limit")
 
     def solve(self, b, x, stream=None, check=True, **kw):
         """Solve K x = b (SPD form) on the device; keyword arguments set iga_solve_opts fields."""

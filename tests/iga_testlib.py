@@ -390,8 +390,11 @@ class RefGpuKernel:
     def available():
         return os.path.exists(REF_GPU_LIB) and os.path.exists(REF_CPU_LIB)
 
-    def __init__(self, nex, ney, Lx=1.0, Ly=1.0):
+    def __init__(self, nex, ney, Lx=1.0, Ly=1.0, ID=None):
+        """ID: equation numbers to use instead of the reference's serial ones
+        (the kernel adds control point A's row into y[ID[A]] for ID[A] >= 0)."""
         p = self.P
+        ID_in = ID
         cpu = ctypes.CDLL(REF_CPU_LIB)
         self.L = ctypes.CDLL(REF_GPU_LIB)
         m, n = nex + p, ney + p
@@ -409,6 +412,11 @@ class RefGpuKernel:
         qp, qw = np.zeros(p + 1), np.zeros(p + 1)
         B, dB = np.zeros(nb), np.zeros(nb)
         cpu.ref_tables(p, _p(qp), _p(qw), _p(B), _p(dB))
+        if ID_in is not None:
+            ID = np.ascontiguousarray(ID_in, dtype=np.int32)
+            assert ID.shape == (m * n,)
+        # the reference's arrays of this mesh, for passing the same ones to other entry points
+        self.arrays = dict(CP=CP, IEN=IEN, ID=ID, C1=C1, C2=C2, h1=h1, h2=h2, B=B, dB=dB, qw=qw)
         h = VP()
         st = self.L.refgpu_create(p, nex, ney, _p(B), _p(dB), _p(qw), _p(C1), _p(C2), _p(h1), _p(h2), _p(IEN),
                                   _p(ID), _p(CP), ctypes.byref(h))

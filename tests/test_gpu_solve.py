@@ -197,6 +197,32 @@ def test_preconditioner_inverts_fem_matrix(torch_cuda, ib, pc, prec, tol):
     assert float((y - r).norm() / r.norm()) < tol
 
 
+@pytest.mark.parametrize("nex,ney", [(300, 260), (130, 517), (517, 130)])
+def test_exact_pc_multi_tile_transforms(torch_cuda, ib, nex, ney):
+    """The exact inverse's two transform GEMMs over many 128 x 128 output tiles
+    with ragged edges (the library's own DMMA tiles in FP64, the TMA-fed
+    tcgen05 TF32 tiles in FP32): FP64 K_fem z = r to 1e-10; the FP32 z close
+    to the FP64 one (TF32 operands: about 1e-3 relative)."""
+    torch = torch_cuda
+    mesh = distorted(ib.unit_square(3, nex, ney))
+    plan = ib.Plan(mesh, precision=ib.MIXED)
+    m, n = nex + 3, ney + 3
+    r = torch.from_numpy(splitmix_uniform(12, -1, 1, plan.nfunc)).cuda()
+    r[torch.from_numpy(boundary_mask(m, n)).cuda()] = 0
+    z = torch.empty_like(r)
+    plan.pc_apply(r, z, pc=ib.PC_FEM_EXACT, precision=ib.FP64)
+    y = torch.empty_like(r)
+    plan.fem_apply(z, y, precision=ib.FP64)
+    r32 = r.float()
+    z32 = torch.empty_like(r32)
+    plan.pc_apply(r32, z32, pc=ib.PC_FEM_EXACT, precision=ib.FP32)
+    torch.cuda.synchronize()
+    assert plan.device_status() == 0
+    assert float((y - r).norm() / r.norm()) < 1e-10
+    assert float((z32.double() - z).norm() / z.norm()) < 1e-2
+    plan.close()
+
+
 @pytest.mark.parametrize("ney", [9700, 19400, 95])
 def test_exact_pc_long_columns(torch_cuda, ib, ney):
     """Tall meshes: the y tridiagonal solves of the exact inverse run on columns of

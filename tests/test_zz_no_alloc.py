@@ -34,11 +34,15 @@ def bernstein_tables(orc, p):
 
 
 def device_args(torch, orc, mesh):
+    """Device copies of the reference-layout arrays; the x- and y-direction
+    tables (B1/B2, dB1/dB2, qw1/qw2) are separate buffers, so that a mix-up
+    of the two directions' arguments would show."""
     p = mesh["p"]
     B, dB, qw = bernstein_tables(orc, p)
     d = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64)).cuda()
-         for k, v in dict(B=B, dB=dB, qw=qw, C1=mesh["C1"], C2=mesh["C2"], CP=mesh["CP"],
-                          h1=np.full(mesh["nex"], 1.0 / mesh["nex"]), h2=np.full(mesh["ney"], 1.0 / mesh["ney"])).items()}
+         for k, v in dict(B1=B, dB1=dB, qw1=qw, B2=B.copy(), dB2=dB.copy(), qw2=qw.copy(), C1=mesh["C1"],
+                          C2=mesh["C2"], CP=mesh["CP"], h1=np.full(mesh["nex"], 1.0 / mesh["nex"]),
+                          h2=np.full(mesh["ney"], 1.0 / mesh["ney"])).items()}
     return d
 
 
@@ -49,13 +53,13 @@ def call_both(torch, ib, mesh, d, x_host):
     y_new = torch.full_like(x, float("nan"))
     y_old = torch.full_like(x, float("nan"))
     ptr = {k: v.data_ptr() for k, v in d.items()}
-    st = L.iga_MatrixFreeMatMultCUDA_noalloc(p, p, nex, ney, ptr["B"], ptr["B"], ptr["dB"], ptr["dB"], ptr["C1"],
-                                             ptr["C2"], ptr["h1"], ptr["h2"], None, None, ptr["CP"], ptr["qw"],
-                                             ptr["qw"], x.data_ptr(), y_new.data_ptr(), None)
+    st = L.iga_MatrixFreeMatMultCUDA_noalloc(p, p, nex, ney, ptr["B1"], ptr["B2"], ptr["dB1"], ptr["dB2"], ptr["C1"],
+                                             ptr["C2"], ptr["h1"], ptr["h2"], None, None, ptr["CP"], ptr["qw1"],
+                                             ptr["qw2"], x.data_ptr(), y_new.data_ptr(), None)
     assert st == 0, ib.lib().iga_last_error()
-    st = L.iga_MatrixFreeMatMultCUDA(p, p, nex, ney, ptr["B"], ptr["B"], ptr["dB"], ptr["dB"], ptr["C1"], ptr["C2"],
-                                     ptr["h1"], ptr["h2"], None, None, ptr["CP"], ptr["qw"], ptr["qw"], x.data_ptr(),
-                                     y_old.data_ptr())
+    st = L.iga_MatrixFreeMatMultCUDA(p, p, nex, ney, ptr["B1"], ptr["B2"], ptr["dB1"], ptr["dB2"], ptr["C1"],
+                                     ptr["C2"], ptr["h1"], ptr["h2"], None, None, ptr["CP"], ptr["qw1"], ptr["qw2"],
+                                     x.data_ptr(), y_old.data_ptr())
     assert st == 0, ib.lib().iga_last_error()
     torch.cuda.synchronize()
     return y_new.cpu().numpy(), y_old.cpu().numpy()
@@ -65,7 +69,7 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-@pytest.mark.parametrize("case", ["golden_p3_16", "p2_130x17", "p3_300x200", "p4_70x45"])
+@pytest.mark.parametrize("case", ["golden_p3_16", "p1_77x40", "p2_130x17", "p3_300x200", "p4_70x45", "p5_50x37"])
 def test_noalloc_matches_existing_entry_point_twice(torch_cuda, orc, gold, case):
     ib = load_binding()
     if case == "golden_p3_16":
@@ -81,7 +85,42 @@ def test_noalloc_matches_existing_entry_point_twice(torch_cuda, orc, gold, case)
         y_new, y_old = call_both(torch_cuda, ib, mesh, d, x)
         assert np.isfinite(y_new).all()
         assert rel(y_new, y_old) < TOL64
+    if case == "golden_p3_16":   # and against the compiled reference's own MatMult
+        x = np.asarray(gold["p3_16_x"])
+        y_new, _ = call_both(torch_cuda, ib, mesh, d, x)
+        assert rel(y_new, gold["p3_16_y_mf"]) < TOL64
     assert ib.lib().iga_MatrixFreeMatMultCUDA_release() == 0
+
+
+def test_noalloc_refuses_misaligned_arrays_before_any_launch(torch_cuda, orc):
+    """d_CP is read as 16-byte (x, y) pairs: an array 8 bytes into a larger
+    buffer is refused with IGA_ERR_ARG on the host (nothing is launched, y
+    keeps its contents); so are double arrays off an 8-byte boundary."""
+    torch = torch_cuda
+    ib = load_binding()
+    L = ib.lib()
+    mesh = ib.unit_square(3, 20, 12)
+    d = device_args(torch, orc, mesh)
+    n = (20 + 3) * (12 + 3)
+    cp_buf = torch.zeros(2 * n + 1, dtype=torch.float64, device="cuda")
+    cp_buf[1:] = d["CP"]
+    x = torch.from_numpy(splitmix_uniform(5, -1.0, 1.0, n)).cuda()
+    y = torch.full_like(x, 3.0)
+    ptr = {k: v.data_ptr() for k, v in d.items()}
+
+    def call(cp, xin):
+        return L.iga_MatrixFreeMatMultCUDA_noalloc(3, 3, 20, 12, ptr["B1"], ptr["B2"], ptr["dB1"], ptr["dB2"],
+                                                   ptr["C1"], ptr["C2"], None, None, None, None, cp, ptr["qw1"],
+                                                   ptr["qw2"], xin, y.data_ptr(), None)
+
+    assert call(cp_buf.data_ptr() + 8, x.data_ptr()) == 1
+    assert b"16-byte" in L.iga_last_error()
+    assert call(ptr["CP"], x.data_ptr() + 4) == 1
+    torch.cuda.synchronize()
+    assert bool((y == 3.0).all())
+    assert call(ptr["CP"], x.data_ptr()) == 0   # the aligned call still works
+    torch.cuda.synchronize()
+    assert np.isfinite(y.cpu().numpy()).all()
 
 
 def test_noalloc_rejects_meshes_beyond_its_scratch(torch_cuda):
@@ -96,3 +135,10 @@ def test_noalloc_rejects_meshes_beyond_its_scratch(torch_cuda):
     st = L.iga_MatrixFreeMatMultCUDA_noalloc(3, 2, 8, 8, *([dummy] * 8), None, None, dummy, dummy, dummy, dummy,
                                              dummy, None)
     assert st == 2
+    # a degree the entry point does not handle is "unsupported", not a bad argument
+    st = L.iga_MatrixFreeMatMultCUDA_noalloc(6, 6, 8, 8, *([dummy] * 8), None, None, dummy, dummy, dummy, dummy,
+                                             dummy, None)
+    assert st == 2
+    st = L.iga_MatrixFreeMatMultCUDA_noalloc(0, 0, 8, 8, *([dummy] * 8), None, None, dummy, dummy, dummy, dummy,
+                                             dummy, None)
+    assert st == 1
