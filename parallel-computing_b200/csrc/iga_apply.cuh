@@ -537,6 +537,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
 template <int P, typename T, int GEOM, int NST>
 __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kernel(ApplyParams<T> a)
 {
+    pdl_begin();
     const int rows = min(a.gyn, a.g.NSY - a.gy0);   // strip rows of the window
     if constexpr (apply_txreg<P, T, GEOM>()) {
         const int sid = blockIdx.x * blockDim.y + threadIdx.y;
@@ -663,6 +664,7 @@ template <int P, typename T>
 __global__ void seam_fixup_kernel(const T *__restrict__ frame, const T *__restrict__ x, T *__restrict__ y,
                                   StripGrid g, T sign, int bc, const int *__restrict__ ID)
 {
+    pdl_begin();
     const long long total = seam_count(g);
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x)

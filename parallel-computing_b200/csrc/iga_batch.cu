@@ -879,6 +879,7 @@ using namespace iga;
 struct iga_batch {
     int count = 0, precision = IGA_FP64, device = 0;
     std::vector<iga_plan *> plans;
+    PlanArena arena;   // device memory of the plans' tables and geometry
     std::vector<long long> off;   // count + 1
     long long ntot = 0;
     std::vector<BGroup> groups;
@@ -1540,7 +1541,9 @@ int create_batch(const iga_mesh_desc *meshes, int count, int precision, int devi
         if (ty <= 0) ty = default_rows(meshes[i].p, meshes[i].nElemY);
         o.rows_per_strip = std::max(ty, std::max(1, meshes[i].p));
         iga_plan *pl = nullptr;
+        plan_arena() = &B->arena;   // few large allocations, no synchronisation per plan
         const int st = iga_plan_create(&meshes[i], &o, &pl);
+        plan_arena() = nullptr;
         if (st) {
             set_error("iga_batch_create: problem " + std::to_string(i) + ": " + last_error());
             return fail(st);
@@ -1621,6 +1624,16 @@ int create_batch(const iga_mesh_desc *meshes, int count, int precision, int devi
         if ((st = bmalloc(&B->v32.x, N)) || (st = bmalloc(&B->v32.q, N))) return fail(st);
     }
     BT_TRY(cudaDeviceSynchronize());
+    // the plans' geometry set-up ran without a synchronisation each: check their flags now
+    for (int i = 0; i < count; ++i) {
+        int herr = 0;
+        BT_TRY(cudaMemcpy(&herr, B->plans[i]->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr) {
+            set_error("iga_batch_create: problem " + std::to_string(i) +
+                      ": geometry has a non-positive Jacobian determinant");
+            return fail(IGA_ERR_ARG);
+        }
+    }
     *out = B;
     return IGA_OK;
 }
@@ -1690,6 +1703,8 @@ int iga_batch_destroy(iga_batch *B)
     cudaDeviceSynchronize();
     if (B->graph) cudaGraphExecDestroy(B->graph);
     for (iga_plan *pl : B->plans) iga_plan_destroy(pl);
+    B->plans.clear();
+    B->arena.release();
     for (BGroup &G : B->groups)
         for (int pi = 0; pi < 2; ++pi)
             if (G.items[pi]) cudaFree(G.items[pi]);

@@ -5,7 +5,53 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <utility>
+
 namespace iga {
+
+// ---------------------------------------------------------------- dependent launches
+// Kernels that run inside the solver's captured loop start with pdl_begin():
+// griddepcontrol.wait blocks until the preceding grid has completed and its
+// memory is visible (a no-op when the kernel was launched without a
+// programmatic dependency), then launch_dependents lets the next grid be
+// scheduled while this one runs. A kernel whose CTAs all passed pdl_begin()
+// can therefore have its successor's CTAs resident and waiting, which hides
+// the launch gap between graph nodes.
+__device__ __forceinline__ void pdl_begin()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Host side: while pdl_capture() is true on this thread (the solver's loop
+// capture), launch_k() launches with a programmatic stream serialisation
+// attribute, so that stream capture records programmatic edges; otherwise
+// it is an ordinary launch. Only kernels that begin with pdl_begin() may be
+// launched through it.
+inline bool &pdl_capture()
+{
+    static thread_local bool on = false;
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                            Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    if (pdl_capture()) {
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+    }
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 // Upper bound on mbarrier polls before a wait gives up and reports
 // IGA_ERR_TIMEOUT; each try_wait suspends for a hardware-defined interval, so

@@ -17,10 +17,10 @@ namespace iga {
 // One CTA computes a 128 x 128 tile of C with the FP32 accumulator in 128
 // TMEM columns. Thread 0 of warp 0 feeds a ring of kGS stages with the
 // tensor-memory accelerator: per stage a 32-wide K slice of A (128 rows) and
-// of B (128 rows), 16 KiB each, in the canonical 128-byte-swizzled layouts of
-// the UMMA descriptors (K-major: 128-byte rows of 32 k values, 8-row groups
-// 1 KiB apart; MN-major: four 4 KiB boxes of 32 k rows x 32 values, one per
-// 32-wide MN atom). Thread 0 of warp 1 issues four 128 x 128 x 8 MMAs per
+// of B (128 rows), 16 KiB each, in the canonical swizzled layouts of the UMMA
+// descriptors (K-major: 128-byte rows of 32 k values, 8-row groups 1 KiB
+// apart; MN-major: four 4 KiB boxes of 32 k rows x 32 values, one per 32-wide
+// MN atom, in the 32-byte-atom swizzle). Thread 0 of warp 1 issues four 128 x 128 x 8 MMAs per
 // stage and commits them to the stage's "empty" barrier, which releases the
 // stage to the copy thread. After the last slice a commit to "done" hands
 // the accumulator to the epilogue: every warp reads its 32 TMEM lanes
@@ -40,11 +40,20 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
-// Descriptor of a 128-byte-swizzled operand tile (start 1 KiB aligned up to
-// the K-substep offset); layout type 2 = SWIZZLE_128B in bits [61, 64).
+// Descriptors of the operand tiles (layout type in bits [61, 64)):
+// K-major tiles use the 128-byte swizzle (type 2; 128-byte rows of 32 k
+// values, 8-row groups SBO apart); MN-major TF32 tiles must use the 128-byte
+// swizzle with 32-byte atoms (type 1: 128-byte K rows, 4-row groups SBO apart,
+// 32-value MN atoms LBO apart), the only MN-major layout the tensor cores
+// take for 32-bit operands; the copy engine writes it with
+// CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B.
 __device__ __forceinline__ uint64_t sw128_desc(const void *p, uint32_t lbo, uint32_t sbo)
 {
     return umma::smem_desc(p, lbo, sbo) | ((uint64_t)2 << 61);
+}
+__device__ __forceinline__ uint64_t sw128_32b_desc(const void *p, uint32_t lbo, uint32_t sbo)
+{
+    return umma::smem_desc(p, lbo, sbo) | ((uint64_t)1 << 61);
 }
 
 // OUT: 0 C, 1 scatter into an FP32 vector, 2 into an FP64 vector (GemmScatter).
@@ -62,6 +71,7 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
     uint64_t *empty = full + kGS, *done = empty + kGS;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 1);
     int *cnt = reinterpret_cast<int *>(tslot + 1);   // [0] slices loaded, [1] slices consumed, [2] failure
+    pdl_begin();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * kGM, n0 = blockIdx.y * kGN;
     const int nk = (K + kGK - 1) / kGK;
@@ -122,9 +132,9 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
 #pragma unroll
             for (int j = 0; j < kGK / 8; ++j) {
                 // K substep j: 8 k values = 32 bytes along a K-major row, or 8
-                // rows (one 1 KiB swizzle group) of an MN-major tile
-                const uint64_t ad = AMN ? sw128_desc(a + j * 1024, 4096, 1024) : sw128_desc(a + j * 32, 16, 1024);
-                const uint64_t bd = BMN ? sw128_desc(b + j * 1024, 4096, 1024) : sw128_desc(b + j * 32, 16, 1024);
+                // K rows (two 512-byte swizzle groups) of an MN-major tile
+                const uint64_t ad = AMN ? sw128_32b_desc(a + j * 1024, 4096, 512) : sw128_desc(a + j * 32, 16, 1024);
+                const uint64_t bd = BMN ? sw128_32b_desc(b + j * 1024, 4096, 512) : sw128_desc(b + j * 32, 16, 1024);
                 umma::mma_tf32(tmem, ad, bd, IDESC, (kt > 0 || j > 0) ? 1u : 0u);
             }
             umma::commit(&empty[s]);
@@ -200,9 +210,10 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder()
     return fn;
 }
 
-// Tensor map of one operand: K-major X[rows][k] (box 32 k x 128 rows) or
-// MN-major X[k][rows] (box 32 rows x 32 k), FP32, 128-byte swizzle, reads
-// outside [0, inner) x [0, outer) zero-filled.
+// Tensor map of one operand: K-major X[rows][k] (box 32 k x 128 rows,
+// 128-byte swizzle) or MN-major X[k][rows] (box 32 rows x 32 k, 128-byte
+// swizzle with 32-byte atoms), FP32, reads outside [0, inner) x [0, outer)
+// zero-filled.
 int make_map(CUtensorMap &map, const GemmOperand &op, int rows, int K)
 {
     auto enc = encoder();
@@ -220,7 +231,8 @@ int make_map(CUtensorMap &map, const GemmOperand &op, int rows, int K)
     const cuuint32_t box[2] = {32u, op.mn_major ? 32u : 128u};
     const cuuint32_t estr[2] = {1u, 1u};
     const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(op.ptr), dims, strides, box,
-                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           op.mn_major ? CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B : CU_TENSOR_MAP_SWIZZLE_128B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         set_error("cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
@@ -240,8 +252,10 @@ int launch_tf32_t(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter
         attr = true;
     }
     const dim3 grid((g.Mst + kGM - 1) / kGM, (g.Nst + kGN - 1) / kGN);
-    gemm_tf32_kernel<AMN, BMN, OUT><<<grid, 128, kGSmem, s>>>(g.ta, g.tb, g.K, g.Mst, g.Nst, g.C, g.ldc, err, sc);
-    return cudaPeekAtLastError() == cudaSuccess ? IGA_OK : IGA_ERR_CUDA;
+    return launch_k(gemm_tf32_kernel<AMN, BMN, OUT>, grid, dim3(128), kGSmem, s, g.ta, g.tb, g.K, g.Mst, g.Nst, g.C,
+                    g.ldc, err, sc) == cudaSuccess
+               ? IGA_OK
+               : IGA_ERR_CUDA;
 }
 
 template <bool AMN, bool BMN>
@@ -343,6 +357,7 @@ __global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const double *__restri
 {
     using TA = DTile<AMN, kDM>;
     using TB = DTile<BMN, kDN>;
+    pdl_begin();
     extern __shared__ __align__(16) double dsm[];
     double *As = dsm, *Bs = dsm + kDS * TA::elems;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -453,10 +468,10 @@ int launch_f64(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, i
         attr = true;
     }
     const dim3 grid((Mst + kDM - 1) / kDM, (Nst + kDN - 1) / kDN);
-    gemm_f64_kernel<AMN, BMN, SCATTER><<<grid, 256, smem, s>>>(static_cast<const double *>(A.ptr), A.ld,
-                                                               static_cast<const double *>(B.ptr), B.ld, C, ldc, M, N,
-                                                               K, Mst, Nst, sc);
-    return cudaPeekAtLastError() == cudaSuccess ? IGA_OK : IGA_ERR_CUDA;
+    return launch_k(gemm_f64_kernel<AMN, BMN, SCATTER>, grid, dim3(256), smem, s, static_cast<const double *>(A.ptr),
+                    A.ld, static_cast<const double *>(B.ptr), B.ld, C, ldc, M, N, K, Mst, Nst, sc) == cudaSuccess
+               ? IGA_OK
+               : IGA_ERR_CUDA;
 }
 }  // namespace
 

@@ -180,7 +180,11 @@ int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int 
     a.bc = d_ID ? IGA_BC_NONE : IGA_BC_REFERENCE;
     a.ID = d_ID;
     a.err = reinterpret_cast<int *>(base + Ly.off_err);
-    dim3 grid(g.NSX, (g.NSY + W - 1) / W), block(32, W);
+    // tables in registers: strips dealt to warps one by one; else a CTA per W strips of a column
+    const long long nstrips = (long long)g.NSX * g.NSY;
+    const dim3 grid = apply_txreg<P, double, 1>() ? dim3((unsigned)((nstrips + W - 1) / W))
+                                                  : dim3(g.NSX, (g.NSY + W - 1) / W),
+               block(32, W);
     kern<<<grid, block, smem, s>>>(a);
     cudaError_t e = cudaPeekAtLastError();
     const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;

@@ -213,12 +213,56 @@ static thread_local std::string g_last_error;
 void set_error(const std::string &s) { g_last_error = s; }
 const std::string &last_error() { return g_last_error; }
 
+PlanArena *&plan_arena()
+{
+    static thread_local PlanArena *a = nullptr;
+    return a;
+}
+
+cudaError_t PlanArena::alloc(void **p, size_t bytes)
+{
+    constexpr size_t kChunk = size_t(256) << 20;
+    bytes = (bytes + 255) & ~size_t(255);
+    if (chunks.empty() || used + bytes > chunks.back().second) {
+        const size_t sz = std::max(kChunk, bytes);
+        char *c = nullptr;
+        const cudaError_t e = cudaMalloc((void **)&c, sz);
+        if (e != cudaSuccess) return e;
+        chunks.emplace_back(c, sz);
+        used = 0;
+    }
+    *p = chunks.back().first + used;
+    used += bytes;
+    return cudaSuccess;
+}
+
+bool PlanArena::owns(const void *p) const
+{
+    for (const auto &c : chunks)
+        if (p >= (const void *)c.first && p < (const void *)(c.first + c.second)) return true;
+    return false;
+}
+
+void PlanArena::release()
+{
+    for (auto &c : chunks) cudaFree(c.first);
+    chunks.clear();
+    used = 0;
+}
+
 template <typename T>
 static int upload(T **dst, const void *src, size_t bytes)
 {
-    IGA_CUDA_TRY(cudaMalloc((void **)dst, std::max<size_t>(bytes, 16)));
+    if (PlanArena *a = plan_arena()) IGA_CUDA_TRY(a->alloc((void **)dst, std::max<size_t>(bytes, 16)));
+    else IGA_CUDA_TRY(cudaMalloc((void **)dst, std::max<size_t>(bytes, 16)));
     if (src && bytes) IGA_CUDA_TRY(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
     return IGA_OK;
+}
+
+// cudaFree unless the buffer belongs to the plan's arena.
+static void plan_free(const iga_plan *pl, void *p)
+{
+    if (p && !(pl->arena && pl->arena->owns(p))) cudaFree(p);
 }
 
 static constexpr size_t kSmemBudget = 220 * 1024;
@@ -353,7 +397,8 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
         if ((st = upload((T **)&op.G, nullptr, op.geom_bytes))) return st;
         geom_setup_kernel<T><<<1184, 256>>>((T *)op.G, pl->tabX64, pl->tabY64, pl->CP, pl->qw, pl->kappa_dev, g,
                                             pl->d_err);
-        cudaError_t e = cudaDeviceSynchronize();
+        // in an arena (a batch's set-up) the caller synchronises once for all plans
+        cudaError_t e = pl->arena ? cudaPeekAtLastError() : cudaDeviceSynchronize();
         if (e != cudaSuccess) {
             set_error(std::string("geometry setup: ") + cudaGetErrorString(e));
             return IGA_ERR_CUDA;
@@ -408,7 +453,7 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
     const long long nstrips = (long long)g.NSX * rows;
     dim3 grid = apply_txreg<P, T, GEOM>() ? dim3((unsigned)((nstrips + W - 1) / W)) : dim3(g.NSX, (rows + W - 1) / W);
     dim3 block(32, W);
-    if (rows > 0) kern<<<grid, block, smem, s>>>(a);
+    if (rows > 0) IGA_CUDA_TRY(launch_k(kern, grid, block, smem, s, a));
     if (win.gyn < 0) {
         const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
         if (nseam > 0) {
@@ -416,7 +461,8 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
             // (L2 hits) are all in flight at once (p=3 2048^2 FP64 MatMult:
             // 309.5 us with 7 points per thread, 306 us with one)
             const int blocks = (int)std::min<long long>((nseam + 255) / 256, 32 * 148);
-            seam_fixup_kernel<P, T><<<blocks, 256, 0, s>>>((const T *)op.frame, x, y, g, (T)sign, bc, win.ID);
+            IGA_CUDA_TRY(launch_k(seam_fixup_kernel<P, T>, dim3(blocks), dim3(256), 0, s, (const T *)op.frame, x, y,
+                                  g, (T)sign, bc, win.ID));
         }
     } else if (win.R1 > win.R0) {
         const long long nseam = (long long)(g.NSX - 1) * P * (win.R1 - win.R0) + (long long)2 * P * g.m * (rows + 1);
@@ -490,10 +536,9 @@ __global__ void kappa_convert_kernel(T *__restrict__ dst, const double *__restri
         dst[t] = (T)src[t];
 }
 
-static void free_op(OperatorData &op)
+static void free_op(const iga_plan *pl, OperatorData &op)
 {
-    for (void *p : {op.tabX, op.tabY, op.G, op.frame, op.wq, op.kappa, op.CP})
-        if (p) cudaFree(p);
+    for (void *p : {op.tabX, op.tabY, op.G, op.frame, op.wq, op.kappa, op.CP}) plan_free(pl, p);
     op = OperatorData{};
 }
 
@@ -596,6 +641,7 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     pl->sign = opts.sign;
     pl->bc = opts.bc;
     pl->device = opts.device;
+    pl->arena = plan_arena();
     pl->patch = P;
     // Rows per strip, per operator: a MIXED plan's FP64 and FP32 operators
     // have their own G layouts, so each gets the strip height that fills the
@@ -672,7 +718,7 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
         if ((st = build_operator<float>(pl, pl->op32, P, tx, ty))) return fail(st);
     }
     int herr = 0;
-    cudaMemcpy(&herr, pl->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (!pl->arena) cudaMemcpy(&herr, pl->d_err, sizeof(int), cudaMemcpyDeviceToHost);
     if (herr) {
         set_error("geometry has a non-positive Jacobian determinant");
         return fail(IGA_ERR_ARG);
@@ -686,12 +732,12 @@ int iga_plan_destroy(iga_plan *pl)
     if (!pl) return IGA_OK;
     cudaSetDevice(pl->device);
     cudaDeviceSynchronize();
-    free_op(pl->op64);
-    free_op(pl->op32);
+    free_op(pl, pl->op64);
+    free_op(pl, pl->op32);
     for (void *p : {(void *)pl->tabX64, (void *)pl->tabY64, (void *)pl->CP, (void *)pl->qw, (void *)pl->d_err,
                     (void *)pl->kappa_dev, (void *)pl->eq_id,
                     (void *)pl->h_stage_x, (void *)pl->d_stage_x, (void *)pl->d_stage_y})
-        if (p) cudaFree(p);
+        plan_free(pl, p);
     if (pl->h_pinned) cudaFreeHost(pl->h_pinned);
     for (cudaStream_t hs : pl->host_st)
         if (hs) cudaStreamDestroy(hs);

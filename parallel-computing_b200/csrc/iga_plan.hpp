@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "../../include/iga_mf.h"
 #include "iga_device.cuh"
@@ -26,6 +28,22 @@ struct OperatorData {
 };
 
 struct SolverState;   // defined by the solver translation unit
+
+// Device memory of many plans carved out of a few large allocations. A batch
+// creates hundreds of small plans; with one cudaMalloc per table and a device
+// synchronisation per plan their set-up cost far more than the solves.
+// While plan_arena() is set on a thread, plan creation allocates from that
+// arena and skips its synchronisations (the caller synchronises once and
+// checks every plan's error flag); the plans' destroy leaves arena memory
+// alone, and the arena's owner releases it after destroying the plans.
+struct PlanArena {
+    std::vector<std::pair<char *, size_t>> chunks;
+    size_t used = 0;   // bytes used in the last chunk
+    cudaError_t alloc(void **p, size_t bytes);
+    bool owns(const void *p) const;
+    void release();
+};
+PlanArena *&plan_arena();
 
 void set_error(const std::string &s);
 const std::string &last_error();
@@ -71,6 +89,8 @@ struct iga_plan {
     int *eq_id = nullptr;
     // Polls of the apply kernel's bounded waits (< 0: the default limit).
     long long wait_polls = -1;
+    // Arena the plan's creation-time buffers came from (not owned), or null.
+    iga::PlanArena *arena = nullptr;
 };
 
 int iga_apply_internal(iga_plan *pl, int prec, const void *x, void *y, cudaStream_t s);

@@ -347,6 +347,7 @@ template <typename T>
 __global__ void pcg_pq_kernel(const T *__restrict__ p, const T *__restrict__ q, long long N, DevScalars *s,
                               double *partials, unsigned *counter)
 {
+    pdl_begin();
     double v[1] = {0.0};
     vloop<T>(N, al16(p) && al16(q), [&](long long i, int c) {
         const Pk<T> a = ldc(p, i, c), b = ldc(q, i, c);
@@ -411,6 +412,7 @@ __global__ void pcg_xr_cond_kernel(T *__restrict__ x, T *__restrict__ r, const T
                                    const T *__restrict__ q, const T *__restrict__ z, long long N, DevScalars *s,
                                    double *partials, unsigned *counter, cudaGraphConditionalHandle h)
 {
+    pdl_begin();
     double tot[2];
     if (xr_update(x, r, p, q, z, N, s, partials, counter, tot) && threadIdx.x == 0) {
         s->rr = tot[0];
@@ -435,6 +437,7 @@ template <typename T>
 __global__ void pcg_beta_kernel(const T *__restrict__ r, const T *__restrict__ z, long long N, DevScalars *s,
                                 double *partials, unsigned *counter)
 {
+    pdl_begin();
     double v[1] = {0.0};
     vloop<T>(N, al16(r) && al16(z), [&](long long i, int c) {
         const Pk<T> a = ldc(r, i, c), b = ldc(z, i, c);
@@ -452,6 +455,7 @@ __global__ void pcg_beta_kernel(const T *__restrict__ r, const T *__restrict__ z
 template <typename T>
 __global__ void pcg_p_kernel(T *__restrict__ p, const T *__restrict__ z, long long N, const DevScalars *s, int first)
 {
+    pdl_begin();
     const T be = first ? T(0) : (T)s->beta;
     vloop<T>(N, al16(p) && al16(z), [&](long long i, int c) {
         const Pk<T> zv = ldc(z, i, c);
@@ -514,6 +518,7 @@ __global__ void sub_kernel(const T *__restrict__ b, const T *__restrict__ q, T *
 template <typename T>
 __global__ void copy_kernel(T *__restrict__ dst, const T *__restrict__ src, long long N)
 {
+    pdl_begin();
     vloop<T>(N, al16(dst) && al16(src), [&](long long i, int c) { stc(dst, i, c, ldc(src, i, c)); });
 }
 
@@ -553,6 +558,7 @@ __device__ __forceinline__ double pc_scale(const DevScalars *s)
 
 __global__ void to_fp32_kernel(const double *__restrict__ r, float *__restrict__ r32, long long N, const DevScalars *s)
 {
+    pdl_begin();
     const double inv = 1.0 / pc_scale(s);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
         r32[t] = (float)(r[t] * inv);
@@ -560,6 +566,7 @@ __global__ void to_fp32_kernel(const double *__restrict__ r, float *__restrict__
 
 __global__ void from_fp32_kernel(const float *__restrict__ z32, double *__restrict__ z, long long N, const DevScalars *s)
 {
+    pdl_begin();
     const double sc = pc_scale(s);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
         z[t] = sc * (double)z32[t];
@@ -603,6 +610,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32)
 fd_tri_kernel(T *__restrict__ W, const T *__restrict__ Lf, const T *__restrict__ Dv, int nx, int ny, int nyp, int seg,
               DevScalars *sc)
 {
+    pdl_begin();
     extern __shared__ __align__(16) unsigned char tri_smem[];
     __shared__ uint64_t bar[kTriMaxWarps];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -733,6 +741,7 @@ template <typename T, typename V>
 __global__ void fd_gather_kernel(const V *__restrict__ r, T *__restrict__ U, V *__restrict__ z, int m, int n, int nx,
                                  int ny, int nxp, int nyp, const DevScalars *sc)
 {
+    pdl_begin();
     ring_copy(z, r, m, n, ((long long)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x,
               (long long)gridDim.x * gridDim.y * blockDim.x);
     constexpr int VN = Pk<T>::n;
@@ -761,6 +770,7 @@ static dim3 grid2d(int ngroups, int ncols)
 template <typename T>
 __global__ void boundary_copy_kernel(T *__restrict__ z, const T *__restrict__ r, int m, int n)
 {
+    pdl_begin();
     ring_copy(z, r, m, n, blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 
@@ -792,6 +802,7 @@ __global__ void kappa_scale_kernel(const double *__restrict__ kappa, double *__r
 template <typename T>
 __global__ void mul_kernel(T *__restrict__ out, const T *__restrict__ a, const T *__restrict__ b, long long N)
 {
+    pdl_begin();
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < N; t += (long long)gridDim.x * blockDim.x)
         out[t] = a[t] * b[t];
 }
@@ -1189,14 +1200,15 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
 {
     const int m = pl->m, n = pl->n, nx = m - 2, ny = n - 2;
     if (nx <= 0 || ny <= 0) {   // no free nodes: the ring is everything
-        boundary_copy_kernel<V><<<kRedBlocks, kThreads, 0, S->stream>>>(z, r, m, n);
+        SOLVE_TRY(launch_k(boundary_copy_kernel<V>, dim3(kRedBlocks), dim3(kThreads), 0, S->stream, z, r, m, n));
         return IGA_OK;
     }
     const int nxp = ps.nxp, nyp = ps.nyp;
     int seg = (ny + 31) / 32;
     seg |= 1;   // odd: conflict-free shared-memory rows
     constexpr int VN = Pk<T>::n;
-    fd_gather_kernel<T, V><<<grid2d(nxp / VN, nyp), 128, 0, S->stream>>>(r, ps.W2, z, m, n, nx, ny, nxp, nyp, sc);
+    SOLVE_TRY(launch_k(fd_gather_kernel<T, V>, grid2d(nxp / VN, nyp), dim3(128), 0, S->stream, r, ps.W2, z, m, n, nx, ny,
+                       nxp, nyp, sc));
     int e = transform_gemm(ps, pl, 1, S->stream);
     if (e == IGA_OK) {
         if (ps.tri_w) {
@@ -1205,9 +1217,11 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
             const int w = std::max(1, std::min(ps.tri_w, (nx + ps.nsm - 1) / ps.nsm));
             const int grid = std::min((nx + w - 1) / w, ps.nsm);
             const size_t smem = ps.tri_smem / ps.tri_w * w;
-            fd_tri_kernel<T, true><<<grid, w * 32, smem, S->stream>>>(ps.W1, ps.Lf, ps.Dv, nx, ny, nyp, seg, S->s);
+            SOLVE_TRY(launch_k(fd_tri_kernel<T, true>, dim3(grid), dim3(w * 32), smem, S->stream, ps.W1,
+                               (const T *)ps.Lf, (const T *)ps.Dv, nx, ny, nyp, seg, S->s));
         } else {
-            fd_tri_kernel<T, false><<<(nx + 7) / 8, 256, 0, S->stream>>>(ps.W1, ps.Lf, ps.Dv, nx, ny, nyp, seg, S->s);
+            SOLVE_TRY(launch_k(fd_tri_kernel<T, false>, dim3((nx + 7) / 8), dim3(256), 0, S->stream, ps.W1,
+                               (const T *)ps.Lf, (const T *)ps.Dv, nx, ny, nyp, seg, S->s));
         }
         // the second GEMM's epilogue writes z's interior itself
         GemmScatter gs;
@@ -1268,11 +1282,15 @@ static int pc_apply_fp32(const iga_plan *pl, SolverState *S, const iga_solve_opt
         if ((st = fd_upload(f, pl, S))) return st;
         if ((st = fd_apply<float, double>(f, pl, S, rin, z, S->s))) return st;
     } else {
-        to_fp32_kernel<<<kRedBlocks, kThreads, 0, S->stream>>>(rin, f.sc, N, S->s);
+        SOLVE_TRY(launch_k(to_fp32_kernel, dim3(kRedBlocks), dim3(kThreads), 0, S->stream, rin, f.sc, N,
+                           (const DevScalars *)S->s));
         if ((st = pc_apply_core<float>(f, pl, S, o, f.sc, f.tz, pc_rtol, pc_iters))) return st;
-        from_fp32_kernel<<<kRedBlocks, kThreads, 0, S->stream>>>(f.tz, z, N, S->s);
+        SOLVE_TRY(launch_k(from_fp32_kernel, dim3(kRedBlocks), dim3(kThreads), 0, S->stream, (const float *)f.tz, z, N,
+                           (const DevScalars *)S->s));
     }
-    if (pl->kappa_dev) mul_kernel<double><<<kRedBlocks, kThreads, 0, S->stream>>>(z, z, S->ks64, N);
+    if (pl->kappa_dev)
+        SOLVE_TRY(launch_k(mul_kernel<double>, dim3(kRedBlocks), dim3(kThreads), 0, S->stream, z, (const double *)z,
+                           (const double *)S->ks64, N));
     return IGA_OK;
 }
 
@@ -1290,9 +1308,9 @@ static int pc_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
     int st;
     if ((st = update_kscale(pl, S))) return st;
     const T *sv = kscale(S, (T *)nullptr);
-    mul_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(ps.sc, r, sv, N);
+    SOLVE_TRY(launch_k(mul_kernel<T>, dim3(kRedBlocks), dim3(kThreads), 0, S->stream, ps.sc, r, sv, N));
     if ((st = pc_apply_core(ps, pl, S, o, ps.sc, z, pc_rtol, pc_iters))) return st;
-    mul_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(z, z, sv, N);
+    SOLVE_TRY(launch_k(mul_kernel<T>, dim3(kRedBlocks), dim3(kThreads), 0, S->stream, z, (const T *)z, sv, N));
     return IGA_OK;
 }
 
@@ -1302,7 +1320,7 @@ static int pc_apply_core(PrecState<T> &ps, const iga_plan *pl, SolverState *S, c
 {
     const long long N = pl->nfunc;
     if (o.pc == IGA_PC_NONE) {
-        copy_kernel<T><<<kRedBlocks, kThreads, 0, S->stream>>>(z, r, N);
+        SOLVE_TRY(launch_k(copy_kernel<T>, dim3(kRedBlocks), dim3(kThreads), 0, S->stream, z, r, N));
         return IGA_OK;
     }
     int st;
@@ -1408,17 +1426,30 @@ static int build_loop(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_
     cudaGraph_t body = np.conditional.phGraph_out[0];
     SOLVE_TRY(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
     int64_t dummy = 0;
+    // Programmatic dependencies between the body's kernels (the inner-CG
+    // preconditioner runs child graphs and keeps ordinary edges).
+    pdl_capture() = o.pc != IGA_PC_FEM_CG;
     int st = iga_apply_internal_sb(pl, prec, ps.p, ps.q, s, IGA_SIGN_SPD, IGA_BC_IDENTITY);
+    auto launched = [&](cudaError_t e) {
+        if (e != cudaSuccess && !st) {
+            set_error(std::string("PCG loop launch: ") + cudaGetErrorString(e));
+            st = IGA_ERR_CUDA;
+        }
+    };
     if (!st) {
-        pcg_pq_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.q, N, S->s, S->partials, S->counter);
-        pcg_xr_cond_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.x, ps.r, ps.p, ps.q, ps.z, N, S->s, S->partials,
-                                                             S->counter, h);
-        st = pc_apply(ps, pl, S, o, ps.r, ps.z, o.pc_rtol, dummy);
+        launched(launch_k(pcg_pq_kernel<T>, dim3(kRedBlocks), dim3(kThreads), 0, s, (const T *)ps.p, (const T *)ps.q,
+                          N, S->s, S->partials, S->counter));
+        launched(launch_k(pcg_xr_cond_kernel<T>, dim3(kRedBlocks), dim3(kThreads), 0, s, ps.x, ps.r, (const T *)ps.p,
+                          (const T *)ps.q, (const T *)ps.z, N, S->s, S->partials, S->counter, h));
+        if (!st) st = pc_apply(ps, pl, S, o, ps.r, ps.z, o.pc_rtol, dummy);
     }
     if (!st) {
-        pcg_beta_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, N, S->s, S->partials, S->counter);
-        pcg_p_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.z, N, S->s, 0);
+        launched(launch_k(pcg_beta_kernel<T>, dim3(kRedBlocks), dim3(kThreads), 0, s, (const T *)ps.r,
+                          (const T *)ps.z, N, S->s, S->partials, S->counter));
+        launched(launch_k(pcg_p_kernel<T>, dim3(kRedBlocks), dim3(kThreads), 0, s, ps.p, (const T *)ps.z, N,
+                          (const DevScalars *)S->s, 0));
     }
+    pdl_capture() = false;
     cudaGraph_t captured = body;
     const cudaError_t ce = cudaStreamEndCapture(s, &captured);
     if (st || ce != cudaSuccess) {

@@ -141,12 +141,13 @@ def test_reference_entry_checks_the_callers_rule_tables(torch_cuda, ib, gold):
     x = torch.from_numpy(gold[f"{name}_x"]).cuda()
     L = ib.lib()
     y = torch.zeros_like(x)
-    assert call_cached(L, 3, M["nex"], M["ney"], device(torch, base), x, y) == 0
+    d_base = device(torch, base)   # kept alive: a freed array's address may be reused by the next one
+    assert call_cached(L, 3, M["nex"], M["ney"], d_base, x, y) == 0
     torch.cuda.synchronize()
     assert rel(y.cpu().numpy(), gold[f"{name}_y_mf"]) < TOL64
-    other = dict(base)
-    other["qw"] = np.full(4, 0.25)   # a 4-point rule with equal weights is not Gauss
-    assert call_cached(L, 3, M["nex"], M["ney"], device(torch, other), x, y) == ERR_UNSUPPORTED
+    d_other = dict(d_base)
+    d_other["qw"] = torch.full((4,), 0.25, dtype=torch.float64, device="cuda")   # equal weights: not Gauss
+    assert call_cached(L, 3, M["nex"], M["ney"], d_other, x, y) == ERR_UNSUPPORTED
     assert L.iga_MatrixFreeMatMultCUDA_release() == 0
 
 
