@@ -275,7 +275,7 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
     both with the FEM preconditioner inverted exactly; plus the reference's
     preconditioner (inner Jacobi-CG to 1e-10) on the p=2 64x64 configuration."""
     out = {"problem": f"p=3 {ne}x{ne}, f=2pi^2 sin(pi x) sin(pi y), K u = F, rtol 1e-10 (true residual)",
-           "pc": "bilinear-FEM matrix, exact inverse (x eigenvectors by GEMM, y tridiagonal solves; FP64 DGEMM / FP32 TF32)"}
+           "pc": "bilinear-FEM matrix, exact inverse (x eigenvectors by GEMM, y tridiagonal solves; own FP64 DMMA / FP32 tcgen05 TF32 GEMMs)"}
     plan = ib.Plan(mesh, precision=ib.MIXED)
     b = torch.empty(plan.nfunc, dtype=torch.float64, device="cuda")
     plan.rhs(b, ib.F_SINSIN)
@@ -287,7 +287,7 @@ def time_solves(ib, torch, mesh, ne, barrier, max_over_ranks):
                      ("fp32_refine", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED, sweep_rtol=1e-3)),
                      ("fp64_pcg_fp32_pc", dict(pc=ib.PC_FEM_EXACT, precision=ib.MIXED_PC))):
         x = torch.zeros_like(b)
-        plan.solve(b, x, **kw)   # warm-up: eigen-decomposition, cuBLAS, allocations
+        plan.solve(b, x, **kw)   # warm-up: eigen-decomposition, tensor maps, loop graph, allocations
         times, st = [], None
         for _ in range(3):
             x.zero_()

@@ -133,19 +133,23 @@ template <int P, typename T, int GEOM>
 __host__ __device__ constexpr int apply_max_threads()
 {
     return sizeof(T) == 4 ? (P <= 3 ? 512 : (GEOM ? 384 : 512))
-                          : (P <= 2 ? (GEOM ? 384 : 512) : P == 3 ? (GEOM ? 320 : 384) : 256);
+                          : (P <= 2 ? (GEOM ? 384 : 512) : P == 3 ? (GEOM ? 256 : 384) : 256);
 }
 
 // Whether a lane keeps its x-direction tables in registers (16 values at
 // p = 3) or reads them from shared memory: registers except where they are
-// the scarcer resource (FP64 on-the-fly geometry, FP64 p >= 4). In registers
-// they save 32 shared loads per element row of a p=3 FP64 strip (12 instead
-// of 13 warps per SM: 1.12x faster), and the warps of a CTA need not share a
-// column strip.
+// the scarcer resource (FP64 p >= 4, FP64 on-the-fly geometry at p <= 2). In
+// registers they save 32 shared loads per element row of a p=3 FP64 strip
+// (12 instead of 13 warps per SM: 1.12x faster), and the warps of a CTA need
+// not share a column strip, so strips are dealt to warps one by one and every
+// SM gets work. The FP64 on-the-fly kernel at p = 3 keeps them in registers
+// at 8 warps per SM (244 registers, no spills; shared tables: 10 warps with
+// spills): 2048^2 673 -> 536 us, 1024^2 208 -> 149 us. At p = 2 the same
+// change was slower (2048^2 392 -> 435 us).
 template <int P, typename T, int GEOM>
 __host__ __device__ constexpr bool apply_txreg()
 {
-    return sizeof(T) == 4 || (GEOM == 0 && P <= 3);
+    return sizeof(T) == 4 || (GEOM == 0 ? P <= 3 : P == 3);
 }
 
 // One warp: strip (gx, gy). With tables in shared memory the CTA's warps

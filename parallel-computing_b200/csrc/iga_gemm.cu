@@ -300,20 +300,24 @@ int gemm_tf32_launch(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScat
 }
 
 // ------------------------------------------------------------ FP64 on DMMA
-// One CTA of 8 warps computes a 128 x 128 tile of C (warp tile 64 x 32 as
-// 4 x 4 blocks of the 16 x 8 x 8 FP64 MMA). K slices of 16 are staged by
-// 16-byte cp.async into a 3-deep ring: K-major operands as [row][k] with 20
-// doubles per row, MN-major ones as [k][row] with 132 per k, both of which
-// make a warp's fragment loads conflict-free. Rows and k past an operand's
-// extent are zero-filled (the matrices are zero-padded, so a 16-byte chunk
-// never straddles the end of the data).
-constexpr int kDM = 128, kDN = 128, kDK = 16, kDS = 3;
-constexpr int kDLK = 20, kDLR = 132;
+// A CTA of WMW x WNW warps computes a (16 WI WMW) x (32 WNW) tile of C; a
+// warp tile is WI x 4 blocks of the 16 x 8 x 8 FP64 MMA. K slices of 16 are
+// staged by 16-byte cp.async into a 3-deep ring: K-major operands as
+// [row][k] with 20 doubles per row, MN-major ones as [k][row] with ROWS + 4
+// per k, both of which make a warp's fragment loads conflict-free. Rows and k
+// past an operand's extent are zero-filled (the matrices are zero-padded, so
+// a 16-byte chunk never straddles the end of the data). Three shapes:
+//   0: 128 x 128, 8 warps of 64 x 32 (one CTA per SM), large products;
+//   1: 128 x 64, 8 warps of 32 x 32 (two CTAs per SM);
+//   2: 64 x 64, 4 warps of 32 x 32 (three CTAs per SM), small products.
+constexpr int kDK = 16, kDS = 3;
+constexpr int kDLK = 20;
 
 template <bool MN, int ROWS>
 struct DTile {
-    static constexpr int elems = MN ? kDK * kDLR : ROWS * kDLK;
-    __device__ static int at(int row, int k) { return MN ? k * kDLR + row : row * kDLK + k; }
+    static constexpr int LR = ROWS + 4;
+    static constexpr int elems = MN ? kDK * LR : ROWS * kDLK;
+    __device__ static int at(int row, int k) { return MN ? k * LR + row : row * kDLK + k; }
 };
 
 // D (16 x 8) += A (16 x 8) B (8 x 8), FP64. Fragments (g = lane / 4,
@@ -329,12 +333,13 @@ __device__ __forceinline__ void dmma(double (&d)[4], const double (&a)[4], const
 }
 
 // Stages the slice k0 .. k0 + 15 of an operand tile (rows r0 .. r0 + ROWS - 1).
-template <bool MN, int ROWS>
+template <bool MN, int ROWS, int NT>
 __device__ __forceinline__ void stage_f64(double *dst, const double *__restrict__ src, int ld, int rows, int K, int r0,
                                           int k0, int tid)
 {
     constexpr int CHUNKS = ROWS * kDK / 2;   // 16-byte chunks
-    for (int c = tid; c < CHUNKS; c += 256) {
+#pragma unroll
+    for (int c = tid; c < CHUNKS; c += NT) {
         int row, k;
         if (MN) {   // [k][row] chunks along rows
             k = c / (ROWS / 2);
@@ -350,32 +355,50 @@ __device__ __forceinline__ void stage_f64(double *dst, const double *__restrict_
     }
 }
 
-template <bool AMN, bool BMN, bool SCATTER>
-__global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const double *__restrict__ A, int lda, const double *__restrict__ B,
-                                                          int ldb, double *__restrict__ C, int ldc, int M, int N, int K,
-                                                          int Mst, int Nst, GemmScatter sc)
+template <int CFG>
+struct DCfg;
+template <>
+struct DCfg<0> {
+    static constexpr int WI = 4, WMW = 2, WNW = 4, MINB = 1;
+};
+template <>
+struct DCfg<1> {
+    static constexpr int WI = 2, WMW = 4, WNW = 2, MINB = 2;
+};
+template <>
+struct DCfg<2> {
+    static constexpr int WI = 2, WMW = 2, WNW = 2, MINB = 3;
+};
+
+template <int CFG, bool AMN, bool BMN, bool SCATTER>
+__global__ void __launch_bounds__(32 * DCfg<CFG>::WMW * DCfg<CFG>::WNW, DCfg<CFG>::MINB)
+    gemm_f64_kernel(const double *__restrict__ A, int lda, const double *__restrict__ B, int ldb,
+                    double *__restrict__ C, int ldc, int M, int N, int K, int Mst, int Nst, GemmScatter sc)
 {
-    using TA = DTile<AMN, kDM>;
-    using TB = DTile<BMN, kDN>;
+    using Cf = DCfg<CFG>;
+    constexpr int WI = Cf::WI, NT = 32 * Cf::WMW * Cf::WNW;
+    constexpr int TM = 16 * WI * Cf::WMW, TN = 32 * Cf::WNW;
+    using TA = DTile<AMN, TM>;
+    using TB = DTile<BMN, TN>;
     pdl_begin();
     extern __shared__ __align__(16) double dsm[];
     double *As = dsm, *Bs = dsm + kDS * TA::elems;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int g = lane >> 2, t4 = lane & 3;
-    const int wm = (w & 1) * 64, wn = (w >> 1) * 32;
-    const int m0 = blockIdx.x * kDM, n0 = blockIdx.y * kDN;
+    const int wm = (w % Cf::WMW) * 16 * WI, wn = (w / Cf::WMW) * 32;
+    const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
     const int nk = (K + kDK - 1) / kDK;
-    double acc[4][4][4];
+    double acc[WI][4][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < WI; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
 #pragma unroll
             for (int c = 0; c < 4; ++c) acc[i][j][c] = 0.0;
     for (int s = 0; s < kDS - 1; ++s) {
         if (s < nk) {
-            stage_f64<AMN, kDM>(As + s * TA::elems, A, lda, M, K, m0, s * kDK, tid);
-            stage_f64<BMN, kDN>(Bs + s * TB::elems, B, ldb, N, K, n0, s * kDK, tid);
+            stage_f64<AMN, TM, NT>(As + s * TA::elems, A, lda, M, K, m0, s * kDK, tid);
+            stage_f64<BMN, TN, NT>(Bs + s * TB::elems, B, ldb, N, K, n0, s * kDK, tid);
         }
         cp_async_commit();
     }
@@ -385,17 +408,17 @@ __global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const double *__restri
         {   // refill the stage consumed one iteration ago
             const int nt = kt + kDS - 1, s = nt % kDS;
             if (nt < nk) {
-                stage_f64<AMN, kDM>(As + s * TA::elems, A, lda, M, K, m0, nt * kDK, tid);
-                stage_f64<BMN, kDN>(Bs + s * TB::elems, B, ldb, N, K, n0, nt * kDK, tid);
+                stage_f64<AMN, TM, NT>(As + s * TA::elems, A, lda, M, K, m0, nt * kDK, tid);
+                stage_f64<BMN, TN, NT>(Bs + s * TB::elems, B, ldb, N, K, n0, nt * kDK, tid);
             }
             cp_async_commit();
         }
         const double *a = As + (kt % kDS) * TA::elems, *b = Bs + (kt % kDS) * TB::elems;
 #pragma unroll
         for (int kk = 0; kk < kDK; kk += 8) {
-            double av[4][4], bv[4][2];
+            double av[WI][4], bv[4][2];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
+            for (int i = 0; i < WI; ++i) {
                 const int r = wm + 16 * i + g;
                 av[i][0] = a[TA::at(r, kk + t4)];
                 av[i][1] = a[TA::at(r + 8, kk + t4)];
@@ -408,7 +431,7 @@ __global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const double *__restri
                 bv[j][1] = b[TB::at(wn + 8 * j + g, kk + t4 + 4)];
             }
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int i = 0; i < WI; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) dmma(acc[i][j], av[i], bv[j]);
         }
@@ -423,7 +446,7 @@ __global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const double *__restri
         }
         double *out = static_cast<double *>(sc.out);
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < WI; ++i)
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int row = m0 + wm + 16 * i + g + 8 * h;
@@ -438,42 +461,65 @@ __global__ void __launch_bounds__(256, 1) gemm_f64_kernel(const double *__restri
             }
     } else {
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < WI; ++i)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int row = m0 + wm + 16 * i + g + 8 * h;
-            if (row >= Mst) continue;
+            for (int h = 0; h < 2; ++h) {
+                const int row = m0 + wm + 16 * i + g + 8 * h;
+                if (row >= Mst) continue;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int col = n0 + wn + 8 * j + 2 * t4;
-                double *dst = C + (size_t)row * ldc + col;
-                if (col + 1 < Nst) *reinterpret_cast<double2 *>(dst) = make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
-                else if (col < Nst) dst[0] = acc[i][j][2 * h];
+                for (int j = 0; j < 4; ++j) {
+                    const int col = n0 + wn + 8 * j + 2 * t4;
+                    double *dst = C + (size_t)row * ldc + col;
+                    if (col + 1 < Nst)
+                        *reinterpret_cast<double2 *>(dst) = make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
+                    else if (col < Nst) dst[0] = acc[i][j][2 * h];
+                }
             }
-        }
     }
 }
 
 namespace {
-template <bool AMN, bool BMN, bool SCATTER>
+int g_f64_shape = -1;   // forced CTA shape (timing runs); -1: by the product's size
+
+template <int CFG, bool AMN, bool BMN, bool SCATTER>
 int launch_f64(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst, cudaStream_t s,
                const GemmScatter &sc)
 {
-    const size_t smem = (size_t)kDS * (DTile<AMN, kDM>::elems + DTile<BMN, kDN>::elems) * sizeof(double);
+    using Cf = DCfg<CFG>;
+    constexpr int TM = 16 * Cf::WI * Cf::WMW, TN = 32 * Cf::WNW, NT = 32 * Cf::WMW * Cf::WNW;
+    const size_t smem = (size_t)kDS * (DTile<AMN, TM>::elems + DTile<BMN, TN>::elems) * sizeof(double);
     static bool attr = false;
     if (!attr) {
-        if (cudaFuncSetAttribute(gemm_f64_kernel<AMN, BMN, SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(gemm_f64_kernel<CFG, AMN, BMN, SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return IGA_ERR_CUDA;
         attr = true;
     }
-    const dim3 grid((Mst + kDM - 1) / kDM, (Nst + kDN - 1) / kDN);
-    return launch_k(gemm_f64_kernel<AMN, BMN, SCATTER>, grid, dim3(256), smem, s, static_cast<const double *>(A.ptr),
-                    A.ld, static_cast<const double *>(B.ptr), B.ld, C, ldc, M, N, K, Mst, Nst, sc) == cudaSuccess
+    const dim3 grid((Mst + TM - 1) / TM, (Nst + TN - 1) / TN);
+    return launch_k(gemm_f64_kernel<CFG, AMN, BMN, SCATTER>, grid, dim3(NT), smem, s,
+                    static_cast<const double *>(A.ptr), A.ld, static_cast<const double *>(B.ptr), B.ld, C, ldc, M, N, K,
+                    Mst, Nst, sc) == cudaSuccess
                ? IGA_OK
                : IGA_ERR_CUDA;
 }
+
+template <int CFG>
+int launch_f64_layout(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst,
+                      cudaStream_t s, const GemmScatter &sc)
+{
+    // the two operand layouts the preconditioner uses (both K-major, both MN-major)
+    if (!A.mn_major && !B.mn_major && !sc.out)
+        return launch_f64<CFG, false, false, false>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+    if (A.mn_major && B.mn_major) {
+        if (sc.out) return launch_f64<CFG, true, true, true>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+        return launch_f64<CFG, true, true, false>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+    }
+    set_error("FP64 GEMM: this operand layout / output combination is not built");
+    return IGA_ERR_UNSUPPORTED;
+}
 }  // namespace
+
+void gemm_f64_force_shape(int shape) { g_f64_shape = shape; }
 
 int gemm_f64_launch(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst,
                     cudaStream_t s, const GemmScatter &sc)
@@ -483,14 +529,24 @@ int gemm_f64_launch(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int
         set_error("FP64 GEMM operands need 16-byte aligned rows (and an FP64 scatter target)");
         return IGA_ERR_ARG;
     }
-    // the two operand layouts the preconditioner uses (both K-major, both MN-major)
-    if (!A.mn_major && !B.mn_major && !sc.out) return launch_f64<false, false, false>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
-    if (A.mn_major && B.mn_major) {
-        if (sc.out) return launch_f64<true, true, true>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
-        return launch_f64<true, true, false>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+    int shape = g_f64_shape;
+    if (shape < 0) {
+        // the largest tile whose grid still fills the SMs (148 on a B200)
+        static int nsm = 0;
+        if (!nsm) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) nsm = 148;
+        }
+        const long long t0 = (long long)((Mst + 127) / 128) * ((Nst + 127) / 128);
+        const long long t1 = (long long)((Mst + 127) / 128) * ((Nst + 63) / 64);
+        shape = t0 >= 3 * nsm / 2 ? 0 : t1 >= 3 * nsm / 2 ? 1 : 2;
     }
-    set_error("FP64 GEMM: this operand layout / output combination is not built");
-    return IGA_ERR_UNSUPPORTED;
+    switch (shape) {
+    case 0: return launch_f64_layout<0>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+    case 1: return launch_f64_layout<1>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+    default: return launch_f64_layout<2>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+    }
 }
 
 }  // namespace iga

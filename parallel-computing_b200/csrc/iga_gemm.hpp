@@ -58,5 +58,8 @@ int gemm_tf32_launch(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScat
 // output only) the result is scattered instead of written to C.
 int gemm_f64_launch(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst,
                     cudaStream_t s, const GemmScatter &sc = GemmScatter());
+// CTA shape of the FP64 GEMM for every later launch (0: 128 x 128, 1: 128 x 64,
+// 2: 64 x 64; -1: chosen from the product's size). For timing the shapes.
+void gemm_f64_force_shape(int shape);
 
 }  // namespace iga

@@ -337,7 +337,7 @@ static int rows_for(int nex, int ney, const std::vector<WarpShape> &Ws, int nsm)
 
 static bool apply_flat(int P, int prec, int geom)
 {
-    return prec == IGA_FP32 || (geom == IGA_GEOM_PRECOMPUTED && P <= 3);
+    return prec == IGA_FP32 || (geom == IGA_GEOM_PRECOMPUTED ? P <= 3 : P == 3);
 }
 
 }  // namespace iga

@@ -145,6 +145,15 @@ SIGNATURES = [
     ("iga_part_mesh", ctypes.c_int, [VP, ctypes.POINTER(MeshDesc)]),
     ("iga_part_build", ctypes.c_int, [VP, ctypes.POINTER(Opts)]),
     ("iga_part_apply", ctypes.c_int, [VP, VP, VP, VP]),
+    ("iga_dist_unique_id", ctypes.c_int, [VP]),
+    ("iga_dist_comm_create", ctypes.c_int, [ctypes.c_int, ctypes.c_int, VP, ctypes.c_int, ctypes.POINTER(VP)]),
+    ("iga_dist_comm_destroy", ctypes.c_int, [VP]),
+    ("iga_dist_exchange_maps", ctypes.c_int, [ctypes.c_int, ctypes.c_int, VP, VP, VP, VP, VP, VP, VP,
+                                              ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
+    ("iga_dist_create", ctypes.c_int, [VP, VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(VP)]),
+    ("iga_dist_destroy", ctypes.c_int, [VP]),
+    ("iga_dist_apply", ctypes.c_int, [VP, VP, VP, VP]),
+    ("iga_dist_solve", ctypes.c_int, [VP, VP, VP, ctypes.POINTER(SolveOpts), ctypes.POINTER(SolveStats), VP]),
 ]
 
 
@@ -450,6 +459,89 @@ class Part:
     def close(self):
         if getattr(self, "h", None):
             _lib().iga_part_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def dist_exchange_maps(rank, offsets, ghost_lists):
+    """Exchange maps of one rank (host, include/iga_dist.h): returns
+    (recv_count[nranks], recv_pos, send_count[nranks], send_idx)."""
+    nranks = len(ghost_lists)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+    counts = np.array([len(g) for g in ghost_lists], dtype=np.int32)
+    ghosts = np.ascontiguousarray(np.concatenate([np.asarray(g, dtype=np.int64) for g in ghost_lists])
+                                  if counts.sum() else np.zeros(1, np.int64))
+    recv_count = np.zeros(nranks, np.int32)
+    send_count = np.zeros(nranks, np.int32)
+    recv_pos = np.zeros(max(1, counts[rank]), np.int32)
+    send_idx = np.zeros(max(1, int(counts.sum())), np.int32)
+    nsend = ctypes.c_int64()
+    _check(_lib().iga_dist_exchange_maps(nranks, rank, _ptr(offsets), _ptr(counts), _ptr(ghosts), _ptr(recv_count),
+                                         _ptr(recv_pos), _ptr(send_count), _ptr(send_idx), send_idx.size,
+                                         ctypes.byref(nsend)), "iga_dist_exchange_maps")
+    return recv_count, recv_pos[:counts[rank]], send_count, send_idx[:nsend.value]
+
+
+class NcclComm:
+    """An NCCL communicator made through the library (one rank per process and
+    GPU): rank 0 calls unique_id() and shares the 128 bytes; every rank then
+    constructs NcclComm(nranks, rank, uid, device)."""
+
+    @staticmethod
+    def unique_id():
+        buf = ctypes.create_string_buffer(128)
+        _check(_lib().iga_dist_unique_id(buf), "iga_dist_unique_id")
+        return buf.raw
+
+    def __init__(self, nranks, rank, uid, device=0):
+        buf = ctypes.create_string_buffer(bytes(uid), 128)
+        h = VP()
+        _check(_lib().iga_dist_comm_create(nranks, rank, buf, device, ctypes.byref(h)), "iga_dist_comm_create")
+        self.h, self.nranks, self.rank = h, nranks, rank
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().iga_dist_comm_destroy(self.h)
+            self.h = None
+
+
+class DistSolver:
+    """The device-resident multi-rank MatMult and PCG of include/iga_dist.h
+    over one opened (not yet built) Part per rank. comm: an NcclComm, or None
+    for a single rank."""
+
+    def __init__(self, part, comm=None, nranks=1, rank=0, device=0):
+        h = VP()
+        c = comm.h if comm is not None else None
+        if comm is not None:
+            nranks, rank = comm.nranks, comm.rank
+        _check(_lib().iga_dist_create(part.h, c, nranks, rank, device, ctypes.byref(h)), "iga_dist_create")
+        self.h, self.part = h, part
+        self.nowned = part.nowned
+
+    def apply(self, x_owned, y_owned, stream=None):
+        _check(_lib().iga_dist_apply(self.h, _ptr(x_owned), _ptr(y_owned), _stream(stream)), "iga_dist_apply")
+
+    def solve(self, b_owned, x_owned, stream=None, check=True, **kw):
+        o = SolveOpts()
+        _lib().iga_solve_opts_default(ctypes.byref(o))
+        for k, v in kw.items():
+            setattr(o, k, v)
+        st = SolveStats()
+        status = _lib().iga_dist_solve(self.h, _ptr(b_owned), _ptr(x_owned), ctypes.byref(o), ctypes.byref(st),
+                                       _stream(stream))
+        if check:
+            _check(status, "iga_dist_solve")
+        return st
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().iga_dist_destroy(self.h)
             self.h = None
 
     def __del__(self):

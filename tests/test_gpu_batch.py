@@ -4,7 +4,7 @@ graph launch.
 The batch has no reference implementation; it is checked against this
 library's single-problem path (the same strip kernel must give bit-identical
 operator results at the same tile shape), against the single-problem exact
-preconditioner (cuBLAS GEMMs), and against the oracle's CPU PCG and operator
+preconditioner (the single plan's own GEMMs), and against the oracle's CPU PCG and operator
 (every solution's residual is recomputed on the CPU).
 """
 import numpy as np
@@ -77,7 +77,7 @@ def test_batch_apply_matches_oracle(torch_cuda, ib, orc):
         assert rel(y[a:b], orc.apply_mf(m, x[a:b], sign=1.0, bc=1)) < 1e-12
 
 
-# FP64 GEMMs (DMMA) match the single-problem cuBLAS DGEMMs to rounding; the FP32
+# FP64 GEMMs (DMMA) match the single-problem DMMA GEMMs to rounding; the FP32
 # preconditioner runs its GEMMs on TF32 operands (10-bit mantissa).
 @pytest.mark.parametrize("prec,tol", [(0, 1e-12), (1, 1e-2)])
 def test_batch_preconditioner_matches_single(torch_cuda, ib, prec, tol):

@@ -268,9 +268,9 @@ def test_exact_pc_solve_matches_inner_cg_solve(torch_cuda, ib, orc, p, ne):
 
 @pytest.mark.parametrize("precision", [0, 2])
 def test_large_solve_runs_as_one_conditional_graph(torch_cuda, ib, precision):
-    """p=3 1536^2 (where cuBLAS's GEMMs would otherwise allocate inside the
-    captured loop): the PCG loop graph instantiates, so no fallback message
-    is left behind, and the solve converges."""
+    """p=3 1536^2: the PCG loop graph (with the preconditioner's tensor-core
+    GEMMs and programmatic dependencies between its kernels) instantiates, so
+    no fallback message is left behind, and the solve converges."""
     torch = torch_cuda
     plan = ib.Plan(ib.unit_square(3, 1536), precision=ib.MIXED)
     b = torch.empty(plan.nfunc, dtype=torch.float64, device="cuda")

@@ -423,3 +423,30 @@ def test_emulated_pcg_fem_cg_pc_matches_oracle_pcg(ib, orc, name):
     b = bp[new]
     _, it_ref, _ = orc.pcg(unit_square_mesh(orc, p, q, nex, ney), b, rtol=1e-11, maxit=500)
     assert it_ref > 0 and abs(its - it_ref) <= 2
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_native_exchange_maps_match_python_maps(ib, name):
+    """The device solver's exchange maps (iga_dist_exchange_maps, C++) equal
+    build_exchange's (the maps the gloo / NCCL torch.distributed path uses) on
+    the reference's own partition files: same peers, same ghost positions,
+    same owned-local indices in the peers' ghost-list order."""
+    from iga_dist import build_exchange
+    parts = open_parts(ib, name)
+    offsets = [pt.owned_offset for pt in parts] + [parts[-1].owned_offset + parts[-1].nowned]
+    ghosts = [pt.ghosts for pt in parts]
+    py = build_exchange(offsets, ghosts)
+    for r in range(len(parts)):
+        recv_count, recv_pos, send_count, send_idx = ib.dist_exchange_maps(r, offsets, ghosts)
+        py_recv, py_send = py[r]
+        want_pos = np.concatenate([py_recv[q] for q in sorted(py_recv)]) if py_recv else np.zeros(0, int)
+        want_idx = np.concatenate([py_send[q] for q in sorted(py_send)]) if py_send else np.zeros(0, int)
+        assert [int(recv_count[q]) for q in range(len(parts))] == [len(py_recv.get(q, [])) for q in range(len(parts))]
+        assert [int(send_count[q]) for q in range(len(parts))] == [len(py_send.get(q, [])) for q in range(len(parts))]
+        assert np.array_equal(recv_pos, want_pos)
+        assert np.array_equal(send_idx, want_idx)
+
+
+def test_native_exchange_maps_reject_unowned_ghosts(ib):
+    with pytest.raises(Exception):
+        ib.dist_exchange_maps(0, [0, 4, 8], [[9], []])   # entry 9 is nobody's
