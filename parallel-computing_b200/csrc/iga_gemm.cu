@@ -27,9 +27,13 @@ namespace iga {
 // (tcgen05.ld 32x32b) and stores its rows of C. No cluster multicast.
 // Two CTAs fit an SM (96 KiB of stages each), so a 2064 x 2064 product
 // (17 x 17 tiles) runs in one wave on 148 SMs.
-constexpr int kGM = 128, kGN = 128, kGK = 32, kGS = 3;
-constexpr int kGTile = kGM * kGK * 4;   // bytes of one operand slice (A and B alike, kGM == kGN)
-constexpr int kGSmem = 1024 + kGS * 2 * kGTile + 256;
+// The tile width BN is 128, or 64 where the 128-wide grid would leave SMs
+// idle (the 1040 x 1040 transforms of a 1024^2 patch: 81 tiles of 128 x 128
+// on 148 SMs, 153 of 128 x 64).
+constexpr int kGM = 128, kGK = 32, kGS = 3;
+constexpr int kGTileA = kGM * kGK * 4;   // bytes of one A slice
+template <int BN>
+constexpr int gemm_tf32_smem() { return 1024 + kGS * (kGTileA + BN * kGK * 4) + 256; }
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
 {
@@ -57,27 +61,28 @@ __device__ __forceinline__ uint64_t sw128_32b_desc(const void *p, uint32_t lbo, 
 }
 
 // OUT: 0 C, 1 scatter into an FP32 vector, 2 into an FP64 vector (GemmScatter).
-template <bool AMN, bool BMN, int OUT>
+template <bool AMN, bool BMN, int OUT, int BN>
 __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ CUtensorMap ta,
                                                         const __grid_constant__ CUtensorMap tb, int K, int Mst, int Nst,
                                                         float *__restrict__ C, int ldc, int *__restrict__ err,
                                                         GemmScatter sc)
 {
+    constexpr int kGTileB = BN * kGK * 4;
     extern __shared__ unsigned char smem_raw[];
     unsigned char *sm =
         reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    unsigned char *As = sm, *Bs = sm + kGS * kGTile;
-    uint64_t *full = reinterpret_cast<uint64_t *>(sm + 2 * kGS * kGTile);
+    unsigned char *As = sm, *Bs = sm + kGS * kGTileA;
+    uint64_t *full = reinterpret_cast<uint64_t *>(sm + kGS * (kGTileA + kGTileB));
     uint64_t *empty = full + kGS, *done = empty + kGS;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 1);
     int *cnt = reinterpret_cast<int *>(tslot + 1);   // [0] slices loaded, [1] slices consumed, [2] failure
     pdl_begin();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * kGM, n0 = blockIdx.y * kGN;
+    const int m0 = blockIdx.x * kGM, n0 = blockIdx.y * BN;
     const int nk = (K + kGK - 1) / kGK;
 
     if (warp == 0) {
-        umma::alloc(tslot, kGN);
+        umma::alloc(tslot, BN);
         umma::relinquish();
     }
     if (tid == 32) {
@@ -102,16 +107,16 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
                 cnt[2] = 1;
                 break;
             }
-            mbar_arrive_expect_tx(&full[s], 2 * kGTile);
+            mbar_arrive_expect_tx(&full[s], kGTileA + kGTileB);
             const int k0 = kt * kGK;
-            unsigned char *a = As + s * kGTile, *b = Bs + s * kGTile;
+            unsigned char *a = As + s * kGTileA, *b = Bs + s * kGTileB;
             if (AMN) {
                 for (int j = 0; j < kGM / 32; ++j) tma_load_2d(a + j * 4096, &ta, m0 + 32 * j, k0, &full[s]);
             } else {
                 tma_load_2d(a, &ta, k0, m0, &full[s]);
             }
             if (BMN) {
-                for (int j = 0; j < kGN / 32; ++j) tma_load_2d(b + j * 4096, &tb, n0 + 32 * j, k0, &full[s]);
+                for (int j = 0; j < BN / 32; ++j) tma_load_2d(b + j * 4096, &tb, n0 + 32 * j, k0, &full[s]);
             } else {
                 tma_load_2d(b, &tb, k0, n0, &full[s]);
             }
@@ -119,7 +124,7 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
         cnt[0] = kt;
     } else if (warp == 1 && lane == 0) {   // MMA thread
         constexpr uint32_t IDESC =
-            umma::idesc_tf32<kGM, kGN>() | ((uint32_t)AMN << 15) | ((uint32_t)BMN << 16);
+            umma::idesc_tf32<kGM, BN>() | ((uint32_t)AMN << 15) | ((uint32_t)BMN << 16);
         int kt = 0;
         for (; kt < nk; ++kt) {
             const int s = kt % kGS;
@@ -128,7 +133,7 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
                 break;
             }
             umma::fence_after_sync();
-            const unsigned char *a = As + s * kGTile, *b = Bs + s * kGTile;
+            const unsigned char *a = As + s * kGTileA, *b = Bs + s * kGTileB;
 #pragma unroll
             for (int j = 0; j < kGK / 8; ++j) {
                 // K substep j: 8 k values = 32 bytes along a K-major row, or 8
@@ -153,21 +158,32 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
             const double rr = *sc.rr;
             f = (rr > 0.0 && rr < 1e300) ? sqrt(rr) : 1.0;
         }
+        // scatter output: each warp's 32 x 16 chunk goes through shared memory
+        // (the drained A stages) so that a half-warp stores 16 consecutive
+        // entries of one row instead of each lane its own row
+        float *stage = reinterpret_cast<float *>(As) + warp * 32 * 17;
 #pragma unroll 1
-        for (int c0 = 0; c0 < kGN; c0 += 16) {
+        for (int c0 = 0; c0 < BN; c0 += 16) {
             float v[16];
             umma::ld16(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
             umma::wait_ld();
             const int col = n0 + c0;
-            if (OUT != 0) {   // interior block of a vector, unaligned: scalar stores
-                if (row >= sc.rows) continue;
-                const size_t base = (size_t)(row + 1) * sc.ld + col + 1;
+            if (OUT != 0) {
 #pragma unroll
-                for (int c = 0; c < 16; ++c) {
-                    if (col + c >= sc.cols) break;
-                    if (OUT == 1) static_cast<float *>(sc.out)[base + c] = (float)(f * (double)v[c]);
-                    else static_cast<double *>(sc.out)[base + c] = f * (double)v[c];
+                for (int c = 0; c < 16; ++c) stage[lane * 17 + c] = v[c];
+                __syncwarp();
+                const int cl = lane & 15, r0 = m0 + 32 * warp;
+#pragma unroll 4
+                for (int rr = 0; rr < 16; ++rr) {
+                    const int rl = 2 * rr + (lane >> 4), row_s = r0 + rl;
+                    if (row_s < sc.rows && col + cl < sc.cols) {
+                        const double val = f * (double)stage[rl * 17 + cl];
+                        const size_t at = (size_t)(row_s + 1) * sc.ld + col + cl + 1;
+                        if (OUT == 1) static_cast<float *>(sc.out)[at] = (float)val;
+                        else static_cast<double *>(sc.out)[at] = val;
+                    }
                 }
+                __syncwarp();
                 continue;
             }
             if (row >= Mst || col >= Nst) continue;
@@ -192,7 +208,7 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
     }
     umma::fence_before_sync();
     __syncthreads();
-    if (warp == 0) umma::dealloc(tmem, kGN);
+    if (warp == 0) umma::dealloc(tmem, BN);
 }
 
 namespace {
@@ -210,11 +226,11 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder()
     return fn;
 }
 
-// Tensor map of one operand: K-major X[rows][k] (box 32 k x 128 rows,
+// Tensor map of one operand: K-major X[rows][k] (box 32 k x box_rows rows,
 // 128-byte swizzle) or MN-major X[k][rows] (box 32 rows x 32 k, 128-byte
 // swizzle with 32-byte atoms), FP32, reads outside [0, inner) x [0, outer)
 // zero-filled.
-int make_map(CUtensorMap &map, const GemmOperand &op, int rows, int K)
+int make_map(CUtensorMap &map, const GemmOperand &op, int rows, int K, int box_rows)
 {
     auto enc = encoder();
     if (!enc) {
@@ -228,7 +244,7 @@ int make_map(CUtensorMap &map, const GemmOperand &op, int rows, int K)
     const cuuint64_t inner = op.mn_major ? rows : K, outer = op.mn_major ? K : rows;
     const cuuint64_t dims[2] = {inner, outer};
     const cuuint64_t strides[1] = {(cuuint64_t)op.ld * 4};
-    const cuuint32_t box[2] = {32u, op.mn_major ? 32u : 128u};
+    const cuuint32_t box[2] = {32u, op.mn_major ? 32u : (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1u, 1u};
     const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(op.ptr), dims, strides, box,
                            estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -241,28 +257,35 @@ int make_map(CUtensorMap &map, const GemmOperand &op, int rows, int K)
     return IGA_OK;
 }
 
-template <bool AMN, bool BMN, int OUT>
+template <bool AMN, bool BMN, int OUT, int BN>
 int launch_tf32_t(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter &sc)
 {
+    constexpr int smem = gemm_tf32_smem<BN>();
     static bool attr = false;   // per instantiation
     if (!attr) {
-        if (cudaFuncSetAttribute(gemm_tf32_kernel<AMN, BMN, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kGSmem) != cudaSuccess)
+        if (cudaFuncSetAttribute(gemm_tf32_kernel<AMN, BMN, OUT, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem) != cudaSuccess)
             return IGA_ERR_CUDA;
         attr = true;
     }
-    const dim3 grid((g.Mst + kGM - 1) / kGM, (g.Nst + kGN - 1) / kGN);
-    return launch_k(gemm_tf32_kernel<AMN, BMN, OUT>, grid, dim3(128), kGSmem, s, g.ta, g.tb, g.K, g.Mst, g.Nst, g.C,
+    const dim3 grid((g.Mst + kGM - 1) / kGM, (g.Nst + BN - 1) / BN);
+    return launch_k(gemm_tf32_kernel<AMN, BMN, OUT, BN>, grid, dim3(128), smem, s, g.ta, g.tb, g.K, g.Mst, g.Nst, g.C,
                     g.ldc, err, sc) == cudaSuccess
                ? IGA_OK
                : IGA_ERR_CUDA;
 }
 
+template <bool AMN, bool BMN, int BN>
+int launch_tf32_bn(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter &sc)
+{
+    if (!sc.out) return launch_tf32_t<AMN, BMN, 0, BN>(g, s, err, sc);
+    return sc.f64 ? launch_tf32_t<AMN, BMN, 2, BN>(g, s, err, sc) : launch_tf32_t<AMN, BMN, 1, BN>(g, s, err, sc);
+}
+
 template <bool AMN, bool BMN>
 int launch_tf32(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter &sc)
 {
-    if (!sc.out) return launch_tf32_t<AMN, BMN, 0>(g, s, err, sc);
-    return sc.f64 ? launch_tf32_t<AMN, BMN, 2>(g, s, err, sc) : launch_tf32_t<AMN, BMN, 1>(g, s, err, sc);
+    return g.bn == 64 ? launch_tf32_bn<AMN, BMN, 64>(g, s, err, sc) : launch_tf32_bn<AMN, BMN, 128>(g, s, err, sc);
 }
 }  // namespace
 
@@ -270,8 +293,14 @@ int gemm_tf32_prepare(GemmTF32 &g, GemmOperand A, GemmOperand B, float *C, int l
                       int Nst)
 {
     g.ready = false;
+    // 128-wide tiles when they fill the SMs about one and a half times over, else 64-wide
+    int nsm = 148, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        nsm = 148;
+    const long long tiles128 = (long long)((Mst + kGM - 1) / kGM) * ((Nst + 127) / 128);
+    g.bn = tiles128 >= 3LL * nsm / 2 ? 128 : 64;
     int st;
-    if ((st = make_map(g.ta, A, M, K)) || (st = make_map(g.tb, B, N, K))) return st;
+    if ((st = make_map(g.ta, A, M, K, kGM)) || (st = make_map(g.tb, B, N, K, g.bn))) return st;
     if ((uintptr_t)C % 16 || ldc % 4) {
         set_error("TF32 GEMM output needs 16-byte aligned rows");
         return IGA_ERR_ARG;
@@ -307,9 +336,9 @@ int gemm_tf32_launch(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScat
 // per k, both of which make a warp's fragment loads conflict-free. Rows and k
 // past an operand's extent are zero-filled (the matrices are zero-padded, so
 // a 16-byte chunk never straddles the end of the data). Three shapes:
-//   0: 128 x 128, 8 warps of 64 x 32 (one CTA per SM), large products;
+//   0: 128 x 128, 8 warps of 64 x 32 (one CTA per SM);
 //   1: 128 x 64, 8 warps of 32 x 32 (two CTAs per SM);
-//   2: 64 x 64, 4 warps of 32 x 32 (three CTAs per SM), small products.
+//   2: 64 x 64, 4 warps of 32 x 32 (three CTAs per SM), the default.
 constexpr int kDK = 16, kDS = 3;
 constexpr int kDLK = 20;
 
@@ -479,7 +508,7 @@ __global__ void __launch_bounds__(32 * DCfg<CFG>::WMW * DCfg<CFG>::WNW, DCfg<CFG
 }
 
 namespace {
-int g_f64_shape = -1;   // forced CTA shape (timing runs); -1: by the product's size
+int g_f64_shape = -1;   // forced CTA shape (timing runs); -1: the default 64 x 64 shape
 
 template <int CFG, bool AMN, bool BMN, bool SCATTER>
 int launch_f64(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst, cudaStream_t s,
@@ -529,19 +558,10 @@ int gemm_f64_launch(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int
         set_error("FP64 GEMM operands need 16-byte aligned rows (and an FP64 scatter target)");
         return IGA_ERR_ARG;
     }
-    int shape = g_f64_shape;
-    if (shape < 0) {
-        // the largest tile whose grid still fills the SMs (148 on a B200)
-        static int nsm = 0;
-        if (!nsm) {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm <= 0) nsm = 148;
-        }
-        const long long t0 = (long long)((Mst + 127) / 128) * ((Nst + 127) / 128);
-        const long long t1 = (long long)((Mst + 127) / 128) * ((Nst + 63) / 64);
-        shape = t0 >= 3 * nsm / 2 ? 0 : t1 >= 3 * nsm / 2 ? 1 : 2;
-    }
+    // 64 x 64 tiles, three CTAs per SM, measured fastest at every size the
+    // preconditioner meets (2064^2: 586 us = 30.0 TFLOP/s against 614 us with
+    // 128 x 128; 1040^2: 78 us against 158 us; 528^2: 27 against 84 us)
+    const int shape = g_f64_shape >= 0 ? g_f64_shape : 2;
     switch (shape) {
     case 0: return launch_f64_layout<0>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
     case 1: return launch_f64_layout<1>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);

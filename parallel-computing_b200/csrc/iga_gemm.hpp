@@ -28,6 +28,7 @@ struct GemmTF32 {
     int Mst = 0, Nst = 0;          // rows / columns of C written (>= M, N: padding written as zeros)
     float *C = nullptr;
     int ldc = 0;
+    int bn = 128;                  // output tile width (128, or 64 for small products)
     bool ready = false;
 };
 
@@ -59,7 +60,7 @@ int gemm_tf32_launch(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScat
 int gemm_f64_launch(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst,
                     cudaStream_t s, const GemmScatter &sc = GemmScatter());
 // CTA shape of the FP64 GEMM for every later launch (0: 128 x 128, 1: 128 x 64,
-// 2: 64 x 64; -1: chosen from the product's size). For timing the shapes.
+// 2: 64 x 64; -1: the default, 2). For timing the shapes.
 void gemm_f64_force_shape(int shape);
 
 }  // namespace iga
