@@ -507,7 +507,8 @@ def our_arm(args):
 
     if args.profile_pc:
         # the exact FEM preconditioner of the p=3 patch (FP32 and FP64) and the
-        # FP32 operator, a few applies outside any graph
+        # FP32 operator, a few applies outside any graph; then the same
+        # preconditioner with the full (not parity-split) x transforms
         plan = ib.Plan(ib.unit_square(P, args.ne, args.ne), precision=ib.MIXED)
         r = torch.from_numpy(splitmix_uniform(SEED, -1.0, 1.0, plan.nfunc)).cuda()
         z = torch.empty_like(r)
@@ -516,6 +517,11 @@ def our_arm(args):
             plan.pc_apply(r32, z32, pc=ib.PC_FEM_EXACT, precision=ib.FP32)
             plan.pc_apply(r, z, pc=ib.PC_FEM_EXACT, precision=ib.FP64)
             plan.apply(r32, z32, precision=ib.FP32)
+        torch.cuda.synchronize()
+        plan.set_pc_split(0)
+        for _ in range(3):
+            plan.pc_apply(r32, z32, pc=ib.PC_FEM_EXACT, precision=ib.FP32)
+            plan.pc_apply(r, z, pc=ib.PC_FEM_EXACT, precision=ib.FP64)
         torch.cuda.synchronize()
         plan.close()
         if dist is not None:
@@ -725,7 +731,8 @@ def main():
                     help="time only the 256-problem batched solves (prints their JSON object)")
     ap.add_argument("--profile-pc", action="store_true",
                     help="run the exact FEM preconditioner (FP32, FP64) and the FP32 operator of the p=3 patch "
-                         "(--ne) a few times outside any graph (a target for ncu; prints nothing else)")
+                         "(--ne) a few times outside any graph, then the preconditioner with full x transforms "
+                         "(a target for ncu; prints nothing else)")
     ap.add_argument("--profile-annulus", action="store_true",
                     help="run the FP32 and FP64 operators of the p=4 1024x1024 NURBS annulus a few times "
                          "outside any graph (a target for ncu; prints nothing else)")

@@ -78,6 +78,15 @@ int iga_solve(iga_plan *plan, const double *b_dev, double *x_dev, const iga_solv
 int iga_pc_apply(iga_plan *plan, int pc, int precision, const void *r_dev, void *z_dev, double pc_rtol,
                  int pc_max_it, void *stream);
 
+/* IGA_PC_FEM_EXACT splits its x transforms by parity (the FEM nodes of a
+ * patch side are symmetric about its middle, so every x eigenvector is
+ * symmetric or antisymmetric and each transform costs half the flops).
+ * enable = 0 makes the plan's solver use the full transforms instead, 1
+ * restores the default; either drops the plan's solver state (rebuilt on
+ * the next solve). A test hook: the two forms give the same z to rounding.
+ * No counterpart in the reference. */
+int iga_plan_set_pc_split(iga_plan *plan, int enable);
+
 /* y = K_fem x, the SPD bilinear-FEM matrix of the preconditioner (boundary
  * rows identity), matrix-free from its 1-D tensor factors; precision of x/y
  * as for iga_apply_prec. */

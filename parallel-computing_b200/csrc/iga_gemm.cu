@@ -65,7 +65,7 @@ template <bool AMN, bool BMN, int OUT, int BN>
 __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ CUtensorMap ta,
                                                         const __grid_constant__ CUtensorMap tb, int K, int Mst, int Nst,
                                                         float *__restrict__ C, int ldc, int *__restrict__ err,
-                                                        GemmScatter sc)
+                                                        GemmScatter sc, GemmSplit split)
 {
     constexpr int kGTileB = BN * kGK * 4;
     extern __shared__ unsigned char smem_raw[];
@@ -79,7 +79,13 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
     pdl_begin();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * kGM, n0 = blockIdx.y * BN;
-    const int nk = (K + kGK - 1) / kGK;
+    int klo = 0, khi = K;   // this tile's k range (one block of a block-diagonal operand)
+    if (split.kb > 0) {
+        const int t0 = split.on_n ? n0 : m0, t1 = t0 + (split.on_n ? BN : kGM);
+        if (t0 >= split.kb) klo = split.kb;
+        else if (t1 <= split.kb) khi = split.kb;
+    }
+    const int nk = (khi - klo + kGK - 1) / kGK;
 
     if (warp == 0) {
         umma::alloc(tslot, BN);
@@ -108,7 +114,7 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
                 break;
             }
             mbar_arrive_expect_tx(&full[s], kGTileA + kGTileB);
-            const int k0 = kt * kGK;
+            const int k0 = klo + kt * kGK;
             unsigned char *a = As + s * kGTileA, *b = Bs + s * kGTileB;
             if (AMN) {
                 for (int j = 0; j < kGM / 32; ++j) tma_load_2d(a + j * 4096, &ta, m0 + 32 * j, k0, &full[s]);
@@ -270,7 +276,7 @@ int launch_tf32_t(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter
     }
     const dim3 grid((g.Mst + kGM - 1) / kGM, (g.Nst + BN - 1) / BN);
     return launch_k(gemm_tf32_kernel<AMN, BMN, OUT, BN>, grid, dim3(128), smem, s, g.ta, g.tb, g.K, g.Mst, g.Nst, g.C,
-                    g.ldc, err, sc) == cudaSuccess
+                    g.ldc, err, sc, g.split) == cudaSuccess
                ? IGA_OK
                : IGA_ERR_CUDA;
 }
@@ -290,7 +296,7 @@ int launch_tf32(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter &
 }  // namespace
 
 int gemm_tf32_prepare(GemmTF32 &g, GemmOperand A, GemmOperand B, float *C, int ldc, int M, int N, int K, int Mst,
-                      int Nst)
+                      int Nst, GemmSplit split)
 {
     g.ready = false;
     // 128-wide tiles when they fill the SMs about one and a half times over, else 64-wide
@@ -314,6 +320,7 @@ int gemm_tf32_prepare(GemmTF32 &g, GemmOperand A, GemmOperand B, float *C, int l
     g.Nst = Nst;
     g.C = C;
     g.ldc = ldc;
+    g.split = split.kb > 0 && split.kb < K ? split : GemmSplit();
     g.ready = true;
     return IGA_OK;
 }
@@ -402,7 +409,8 @@ struct DCfg<2> {
 template <int CFG, bool AMN, bool BMN, bool SCATTER>
 __global__ void __launch_bounds__(32 * DCfg<CFG>::WMW * DCfg<CFG>::WNW, DCfg<CFG>::MINB)
     gemm_f64_kernel(const double *__restrict__ A, int lda, const double *__restrict__ B, int ldb,
-                    double *__restrict__ C, int ldc, int M, int N, int K, int Mst, int Nst, GemmScatter sc)
+                    double *__restrict__ C, int ldc, int M, int N, int K, int Mst, int Nst, GemmScatter sc,
+                    GemmSplit split)
 {
     using Cf = DCfg<CFG>;
     constexpr int WI = Cf::WI, NT = 32 * Cf::WMW * Cf::WNW;
@@ -416,7 +424,13 @@ __global__ void __launch_bounds__(32 * DCfg<CFG>::WMW * DCfg<CFG>::WNW, DCfg<CFG
     const int g = lane >> 2, t4 = lane & 3;
     const int wm = (w % Cf::WMW) * 16 * WI, wn = (w / Cf::WMW) * 32;
     const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
-    const int nk = (K + kDK - 1) / kDK;
+    int klo = 0, khi = K;   // this tile's k range (one block of a block-diagonal operand)
+    if (split.kb > 0) {
+        const int t0 = split.on_n ? n0 : m0, t1 = t0 + (split.on_n ? TN : TM);
+        if (t0 >= split.kb) klo = split.kb;
+        else if (t1 <= split.kb) khi = split.kb;
+    }
+    const int nk = (khi - klo + kDK - 1) / kDK;
     double acc[WI][4][4];
 #pragma unroll
     for (int i = 0; i < WI; ++i)
@@ -426,8 +440,8 @@ __global__ void __launch_bounds__(32 * DCfg<CFG>::WMW * DCfg<CFG>::WNW, DCfg<CFG
             for (int c = 0; c < 4; ++c) acc[i][j][c] = 0.0;
     for (int s = 0; s < kDS - 1; ++s) {
         if (s < nk) {
-            stage_f64<AMN, TM, NT>(As + s * TA::elems, A, lda, M, K, m0, s * kDK, tid);
-            stage_f64<BMN, TN, NT>(Bs + s * TB::elems, B, ldb, N, K, n0, s * kDK, tid);
+            stage_f64<AMN, TM, NT>(As + s * TA::elems, A, lda, M, K, m0, klo + s * kDK, tid);
+            stage_f64<BMN, TN, NT>(Bs + s * TB::elems, B, ldb, N, K, n0, klo + s * kDK, tid);
         }
         cp_async_commit();
     }
@@ -437,8 +451,8 @@ __global__ void __launch_bounds__(32 * DCfg<CFG>::WMW * DCfg<CFG>::WNW, DCfg<CFG
         {   // refill the stage consumed one iteration ago
             const int nt = kt + kDS - 1, s = nt % kDS;
             if (nt < nk) {
-                stage_f64<AMN, TM, NT>(As + s * TA::elems, A, lda, M, K, m0, nt * kDK, tid);
-                stage_f64<BMN, TN, NT>(Bs + s * TB::elems, B, ldb, N, K, n0, nt * kDK, tid);
+                stage_f64<AMN, TM, NT>(As + s * TA::elems, A, lda, M, K, m0, klo + nt * kDK, tid);
+                stage_f64<BMN, TN, NT>(Bs + s * TB::elems, B, ldb, N, K, n0, klo + nt * kDK, tid);
             }
             cp_async_commit();
         }
@@ -512,7 +526,7 @@ int g_f64_shape = -1;   // forced CTA shape (timing runs); -1: the default 64 x 
 
 template <int CFG, bool AMN, bool BMN, bool SCATTER>
 int launch_f64(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst, cudaStream_t s,
-               const GemmScatter &sc)
+               const GemmScatter &sc, GemmSplit split)
 {
     using Cf = DCfg<CFG>;
     constexpr int TM = 16 * Cf::WI * Cf::WMW, TN = 32 * Cf::WNW, NT = 32 * Cf::WMW * Cf::WNW;
@@ -527,21 +541,21 @@ int launch_f64(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, i
     const dim3 grid((Mst + TM - 1) / TM, (Nst + TN - 1) / TN);
     return launch_k(gemm_f64_kernel<CFG, AMN, BMN, SCATTER>, grid, dim3(NT), smem, s,
                     static_cast<const double *>(A.ptr), A.ld, static_cast<const double *>(B.ptr), B.ld, C, ldc, M, N, K,
-                    Mst, Nst, sc) == cudaSuccess
+                    Mst, Nst, sc, split) == cudaSuccess
                ? IGA_OK
                : IGA_ERR_CUDA;
 }
 
 template <int CFG>
 int launch_f64_layout(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst,
-                      cudaStream_t s, const GemmScatter &sc)
+                      cudaStream_t s, const GemmScatter &sc, GemmSplit split)
 {
     // the two operand layouts the preconditioner uses (both K-major, both MN-major)
     if (!A.mn_major && !B.mn_major && !sc.out)
-        return launch_f64<CFG, false, false, false>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+        return launch_f64<CFG, false, false, false>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc, split);
     if (A.mn_major && B.mn_major) {
-        if (sc.out) return launch_f64<CFG, true, true, true>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
-        return launch_f64<CFG, true, true, false>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+        if (sc.out) return launch_f64<CFG, true, true, true>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc, split);
+        return launch_f64<CFG, true, true, false>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc, split);
     }
     set_error("FP64 GEMM: this operand layout / output combination is not built");
     return IGA_ERR_UNSUPPORTED;
@@ -551,8 +565,9 @@ int launch_f64_layout(GemmOperand A, GemmOperand B, double *C, int ldc, int M, i
 void gemm_f64_force_shape(int shape) { g_f64_shape = shape; }
 
 int gemm_f64_launch(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst,
-                    cudaStream_t s, const GemmScatter &sc)
+                    cudaStream_t s, const GemmScatter &sc, GemmSplit split)
 {
+    if (!(split.kb > 0 && split.kb < K)) split = GemmSplit();
     if ((uintptr_t)A.ptr % 16 || (uintptr_t)B.ptr % 16 || A.ld % 2 || B.ld % 2 || (uintptr_t)C % 16 || ldc % 2 ||
         (sc.out && !sc.f64)) {
         set_error("FP64 GEMM operands need 16-byte aligned rows (and an FP64 scatter target)");
@@ -563,9 +578,9 @@ int gemm_f64_launch(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int
     // 128 x 128; 1040^2: 78 us against 158 us; 528^2: 27 against 84 us)
     const int shape = g_f64_shape >= 0 ? g_f64_shape : 2;
     switch (shape) {
-    case 0: return launch_f64_layout<0>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
-    case 1: return launch_f64_layout<1>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
-    default: return launch_f64_layout<2>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc);
+    case 0: return launch_f64_layout<0>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc, split);
+    case 1: return launch_f64_layout<1>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc, split);
+    default: return launch_f64_layout<2>(A, B, C, ldc, M, N, K, Mst, Nst, s, sc, split);
     }
 }
 

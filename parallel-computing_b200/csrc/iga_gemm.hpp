@@ -13,6 +13,16 @@
 
 namespace iga {
 
+// A block-diagonal operand split at kb (> 0): the operand indexed by the
+// split dimension (M with on_n false, N with on_n true) has nonzeros only in
+// the blocks [0, kb) x [0, kb) and [kb, K) x [kb, K) of (that index, k). A
+// tile lying inside one block then runs its k loop over that block's range
+// only; a tile straddling kb runs the full range (the zeros keep it exact).
+struct GemmSplit {
+    int kb = 0;
+    bool on_n = false;
+};
+
 struct GemmOperand {
     const void *ptr = nullptr;
     int ld = 0;           // elements between consecutive outer-index entries
@@ -29,6 +39,7 @@ struct GemmTF32 {
     float *C = nullptr;
     int ldc = 0;
     int bn = 128;                  // output tile width (128, or 64 for small products)
+    GemmSplit split;               // block-diagonal operand, if any
     bool ready = false;
 };
 
@@ -37,7 +48,7 @@ struct GemmTF32 {
 // extents: rows = M (or N) and K for the logical problem; reads past them
 // are zero-filled by the copy engine.
 int gemm_tf32_prepare(GemmTF32 &g, GemmOperand A, GemmOperand B, float *C, int ldc, int M, int N, int K, int Mst,
-                      int Nst);
+                      int Nst, GemmSplit split = GemmSplit());
 // Where a GEMM's result goes instead of C: element (r, c) with r < rows,
 // c < cols is stored at out[(r + 1) ld + c + 1] (the interior block of a
 // vector on an (rows + 2) x ld grid of control points), in FP32 or FP64,
@@ -58,7 +69,7 @@ int gemm_tf32_launch(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScat
 // tiles are staged by cp.async). Mst/Nst as above; with sc.out set (FP64
 // output only) the result is scattered instead of written to C.
 int gemm_f64_launch(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, int K, int Mst, int Nst,
-                    cudaStream_t s, const GemmScatter &sc = GemmScatter());
+                    cudaStream_t s, const GemmScatter &sc = GemmScatter(), GemmSplit split = GemmSplit());
 // CTA shape of the FP64 GEMM for every later launch (0: 128 x 128, 1: 128 x 64,
 // 2: 64 x 64; -1: the default, 2). For timing the shapes.
 void gemm_f64_force_shape(int shape);

@@ -89,6 +89,8 @@ struct iga_plan {
     int *eq_id = nullptr;
     // Polls of the apply kernel's bounded waits (< 0: the default limit).
     long long wait_polls = -1;
+    // The exact FEM preconditioner may split its x transforms by parity.
+    bool pc_split = true;
     // Arena the plan's creation-time buffers came from (not owned), or null.
     iga::PlanArena *arena = nullptr;
 };

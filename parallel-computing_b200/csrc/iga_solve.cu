@@ -737,9 +737,12 @@ __device__ __forceinline__ void ring_copy(T *__restrict__ z, const T *__restrict
 }
 
 // The gather also copies the boundary ring of r into z (one launch fewer).
+// With the parity split (kb > 0) column c of U is, for c < kb, the even fold
+// r[c] + r[nx-1-c] (c < fo; the middle entry r[fo] alone when nx is odd) and,
+// for c >= kb, the odd fold r[j] - r[nx-1-j] with j = c - kb < fo.
 template <typename T, typename V>
 __global__ void fd_gather_kernel(const V *__restrict__ r, T *__restrict__ U, V *__restrict__ z, int m, int n, int nx,
-                                 int ny, int nxp, int nyp, const DevScalars *sc)
+                                 int ny, int nxp, int nyp, int kb, int fo, const DevScalars *sc)
 {
     pdl_begin();
     ring_copy(z, r, m, n, ((long long)blockIdx.y * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x,
@@ -747,16 +750,59 @@ __global__ void fd_gather_kernel(const V *__restrict__ r, T *__restrict__ U, V *
     constexpr int VN = Pk<T>::n;
     const double inv = sc ? 1.0 / pc_scale(sc) : 1.0;
     const int nv = nxp / VN;
-    for (int b = blockIdx.y; b < nyp; b += gridDim.y)
+    for (int b = blockIdx.y; b < nyp; b += gridDim.y) {
+        const V *rb = r + (size_t)(b + 1) * m + 1;
         for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += gridDim.x * blockDim.x) {
             Pk<T> o;
 #pragma unroll
             for (int c = 0; c < VN; ++c) {
                 const int a = k * VN + c;
-                o.v[c] = (a < nx && b < ny) ? (T)((double)r[(size_t)(b + 1) * m + (a + 1)] * inv) : T(0);
+                double v = 0.0;
+                if (b < ny) {
+                    if (kb == 0) {
+                        if (a < nx) v = (double)rb[a];
+                    } else if (a < kb) {
+                        if (a < fo) v = (double)rb[a] + (double)rb[nx - 1 - a];
+                        else if (a == fo && (nx & 1)) v = (double)rb[a];
+                    } else if (a - kb < fo) {
+                        v = (double)rb[a - kb] - (double)rb[nx - 1 - (a - kb)];
+                    }
+                }
+                o.v[c] = (T)(v * inv);
             }
             stp(U, (long long)b * nxp + (long long)k * VN, o);
         }
+    }
+}
+
+// z's interior from the parity-split transform W [nyp][nxp] (even block
+// Ze = columns 0 .. fe-1, odd block Zo = columns kb .. kb+fo-1):
+// z[j] = Ze[j] + Zo[j], z[nx-1-j] = Ze[j] - Zo[j] (j < fo), and the middle
+// entry z[fo] = Ze[fo] when nx is odd; times sqrt(*rr) when rr is set.
+template <typename T, typename V>
+__global__ void fd_unfold_kernel(const T *__restrict__ W, V *__restrict__ z, int m, int nx, int ny, int nxp, int kb,
+                                 int fe, int fo, const double *rr)
+{
+    pdl_begin();
+    double f = 1.0;
+    if (rr) {
+        const double v = *rr;
+        f = (v > 0.0 && v < 1e300) ? sqrt(v) : 1.0;
+    }
+    for (int b = blockIdx.y; b < ny; b += gridDim.y) {
+        const T *wb = W + (size_t)b * nxp;
+        V *zb = z + (size_t)(b + 1) * m + 1;
+        for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < fe; j += gridDim.x * blockDim.x) {
+            const double e = (double)wb[j];
+            if (j < fo) {
+                const double o = (double)wb[kb + j];
+                zb[j] = (V)(f * (e + o));
+                zb[nx - 1 - j] = (V)(f * (e - o));
+            } else {
+                zb[j] = (V)(f * e);
+            }
+        }
+    }
 }
 
 // 2-D launch of the gather: 128-thread blocks over the 16-byte
@@ -823,6 +869,10 @@ struct PrecState {
     T *Vx = nullptr, *lx = nullptr, *W1 = nullptr, *W2 = nullptr, *Dv = nullptr;
     T *Lf = nullptr;   // LDL^T unit lower factor's subdiagonal per x mode (layout of Dv)
     int nxp = 0, nyp = 0;   // transform sizes padded to multiples of 16
+    // parity split of the x transform (centrosymmetric x pencil): kb = the
+    // padded even block (0: no split), fe / fo the even / odd mode counts;
+    // nmodes = rows of the mode-major work matrix the y solves walk
+    int kb = 0, fe = 0, fo = 0, nmodes = 0;
     GemmTF32 g1, g2;        // FP32: the two transforms' prepared tensor-core GEMMs
     int tri_w = 0;          // most warps per CTA of the staged tridiagonal kernel (0: in place)
     size_t tri_smem = 0;    // its shared memory at tri_w warps
@@ -845,7 +895,12 @@ struct SolverState {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool fd_host = false;
-    std::vector<double> lamx, Vx;             // host x eigenpairs (built once)
+    // host x eigenpairs (built once). Split by parity (fold): even modes
+    // 0 .. fe-1 then odd modes, Vx = the fe x fe even block followed by the
+    // fo x fo odd block, each row one mode's half vector; else n x n.
+    bool fold = false;
+    int fe = 0, fo = 0;
+    std::vector<double> lamx, Vx;
     std::vector<double> Dv, Lf;               // host LDL^T factors of the y systems, [a][b]
     double *ks64 = nullptr;                   // kappa scaling of the preconditioner
     float *ks32 = nullptr;
@@ -1065,18 +1120,91 @@ void interior_pencil(const std::vector<double> &g, std::vector<double> &Kd, std:
 }
 }  // namespace iga
 
+// True when the tridiagonal pencil is centrosymmetric (entry i equals entry
+// n-1-i) to rounding: the FEM nodes of a patch side are symmetric about its
+// middle.
+static bool centrosymmetric(const std::vector<double> &Kd, const std::vector<double> &Ko,
+                            const std::vector<double> &Md, const std::vector<double> &Mo)
+{
+    const int n = (int)Kd.size();
+    if (n < 2) return false;
+    auto sym = [](const std::vector<double> &v) {
+        double mx = 0.0, dif = 0.0;
+        for (size_t i = 0; i < v.size(); ++i) {
+            mx = std::max(mx, std::fabs(v[i]));
+            dif = std::max(dif, std::fabs(v[i] - v[v.size() - 1 - i]));
+        }
+        return dif <= 1e-12 * mx;
+    };
+    return sym(Kd) && sym(Md) && sym(std::vector<double>(Ko.begin(), Ko.begin() + (n - 1))) &&
+           sym(std::vector<double>(Mo.begin(), Mo.begin() + (n - 1)));
+}
+
+// Eigenpairs of a centrosymmetric tridiagonal pencil of size n by parity.
+// Every eigenvector is symmetric (v[i] = v[n-1-i]) or antisymmetric, and each
+// class is the eigenproblem of a half-size symmetric tridiagonal pencil in
+// the half vector u = v[0 .. fe-1] (fe = ceil(n/2)) or v[0 .. fo-1] (fo =
+// floor(n/2)):
+//   n = 2h:   rows 0 .. h-1, the last diagonal entry plus (symmetric) or
+//             minus (antisymmetric) the coupling (h-1, h);
+//   n = 2h+1: symmetric: rows 0 .. h with the middle row's diagonal halved
+//             (the row equation of the middle entry divided by 2, which makes
+//             the half pencil symmetric); antisymmetric: rows 0 .. h-1 (the
+//             middle entry is zero).
+// v^T M v = 2 u^T M_half u, so the half vectors (M_half-normalised by
+// pencil_eig) are divided by sqrt 2. Then for a vector r,
+//   v . r = u . (r[i] + r[n-1-i])_i  (the middle entry taken once)  or
+//   u . (r[i] - r[n-1-i])_i,
+// which halves the flops of both transforms (the even-odd decomposition of
+// spectral and fast-diagonalisation methods).
+static void fold_eig(const std::vector<double> &Kd, const std::vector<double> &Ko, const std::vector<double> &Md,
+                     const std::vector<double> &Mo, SolverState *S)
+{
+    const int n = (int)Kd.size(), fo = n / 2, fe = n - fo;
+    S->fold = true;
+    S->fe = fe;
+    S->fo = fo;
+    S->lamx.assign(n, 0.0);
+    S->Vx.assign((size_t)fe * fe + (size_t)fo * fo, 0.0);
+    for (int parity = 0; parity < 2; ++parity) {
+        const int h = parity == 0 ? fe : fo;
+        if (h == 0) continue;
+        std::vector<double> kd(Kd.begin(), Kd.begin() + h), md(Md.begin(), Md.begin() + h);
+        std::vector<double> ko(Ko.begin(), Ko.begin() + std::max(h - 1, 0)), mo(Mo.begin(), Mo.begin() + std::max(h - 1, 0));
+        ko.resize(h, 0.0);
+        mo.resize(h, 0.0);
+        if (n % 2 == 0) {
+            const double sg = parity == 0 ? 1.0 : -1.0;
+            kd[h - 1] += sg * Ko[h - 1];
+            md[h - 1] += sg * Mo[h - 1];
+        } else if (parity == 0) {
+            kd[h - 1] *= 0.5;
+            md[h - 1] *= 0.5;
+        }
+        double *lam = S->lamx.data() + (parity == 0 ? 0 : fe);
+        double *V = S->Vx.data() + (parity == 0 ? 0 : (size_t)fe * fe);
+        pencil_eig(h, kd.data(), ko.data(), md.data(), mo.data(), lam, V);
+        const double s = 1.0 / std::sqrt(2.0);
+        for (size_t i = 0; i < (size_t)h * h; ++i) V[i] *= s;
+    }
+}
+
 // The x pencil's eigenpairs and, for every x mode a, the LDL^T factors of the
 // y system lx[a] My + Ky on the free nodes, built once per plan on the host.
 static int fd_setup(PrecState<double> &, const iga_plan *pl, SolverState *S)
 {
-    (void)pl;
     if (S->fd_host) return IGA_OK;
     std::vector<double> Kd, Ko, Md, Mo;
     interior_pencil(S->gx, Kd, Ko, Md, Mo);
     const int nx = (int)Kd.size();
-    S->lamx.assign(nx, 0.0);
-    S->Vx.assign((size_t)nx * nx, 0.0);
-    pencil_eig(nx, Kd.data(), Ko.data(), Md.data(), Mo.data(), S->lamx.data(), S->Vx.data());
+    if (pl->pc_split && centrosymmetric(Kd, Ko, Md, Mo)) {
+        fold_eig(Kd, Ko, Md, Mo, S);
+    } else {
+        S->fold = false;
+        S->lamx.assign(nx, 0.0);
+        S->Vx.assign((size_t)nx * nx, 0.0);
+        pencil_eig(nx, Kd.data(), Ko.data(), Md.data(), Mo.data(), S->lamx.data(), S->Vx.data());
+    }
     interior_pencil(S->gy, Kd, Ko, Md, Mo);
     const int ny = (int)Kd.size();
     S->Dv.assign((size_t)nx * ny, 0.0);
@@ -1102,10 +1230,10 @@ static int prepare_gemms(PrecState<float> &ps)
 {
     const int nxp = ps.nxp, nyp = ps.nyp;
     int st = gemm_tf32_prepare(ps.g1, GemmOperand{ps.Vx, nxp, false}, GemmOperand{ps.W2, nxp, false}, ps.W1, nyp, nxp,
-                               nyp, nxp, nxp, nyp);
+                               nyp, nxp, nxp, nyp, GemmSplit{ps.kb, false});
     if (st) return st;
     return gemm_tf32_prepare(ps.g2, GemmOperand{ps.W1, nyp, true}, GemmOperand{ps.Vx, nxp, true}, ps.W2, nxp, nyp, nxp,
-                             nxp, nyp, nxp);
+                             nxp, nyp, nxp, GemmSplit{ps.kb, true});
 }
 
 template <typename T>
@@ -1117,37 +1245,53 @@ static int fd_upload(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
     const int nx = pl->m - 2, ny = pl->n - 2;
     // multiples of 16: aligned rows for the GEMMs and 16-byte moves; the
     // DGEMMs do no more flops than they must (2112 -> 2064 at 2048^2: FP64
-    // PCG 114 -> 111 ms; TF32 GEMMs inside the solver's graph unchanged)
-    const int nxp = (nx + 15) / 16 * 16, nyp = (ny + 15) / 16 * 16;
+    // PCG 114 -> 111 ms; TF32 GEMMs inside the solver's graph unchanged).
+    // With the parity split the x index runs over the even block (fe values,
+    // padded to kb) and then the odd block (fo values, padded).
+    const int fe = S->fold ? S->fe : nx, fo = S->fold ? S->fo : 0;
+    const int kb = (fe + 15) / 16 * 16, kob = (fo + 15) / 16 * 16;
+    const int nxp = S->fold ? kb + kob : kb, nyp = (ny + 15) / 16 * 16;
     ps.nxp = nxp;
     ps.nyp = nyp;
-    // zero-padded eigenvector matrices; padded eigenvalues 1 keep the scaling finite
-    auto up_mat = [&](T **dst, const std::vector<double> &V, int n, int np) -> int {
-        std::vector<T> h((size_t)np * np, T(0));
-        for (int k = 0; k < n; ++k)
-            for (int i = 0; i < n; ++i) h[(size_t)k * np + i] = (T)V[(size_t)k * n + i];
+    ps.kb = S->fold ? kb : 0;
+    ps.fe = fe;
+    ps.fo = fo;
+    ps.nmodes = S->fold ? nxp : nx;
+    // device row of host mode a (even modes, then odd ones from row kb)
+    auto row_of = [&](int a) { return a < fe ? a : kb + (a - fe); };
+    // zero-padded eigenvector matrix, block diagonal with the split: row
+    // row_of(a) holds mode a's (half) vector from column 0 (even) or kb (odd)
+    auto up_mat = [&](T **dst) -> int {
+        std::vector<T> h((size_t)nxp * nxp, T(0));
+        for (int a = 0; a < fe; ++a)
+            for (int i = 0; i < fe; ++i) h[(size_t)a * nxp + i] = (T)S->Vx[(size_t)a * fe + i];
+        const double *Vo = S->Vx.data() + (size_t)fe * fe;
+        for (int a = 0; a < fo; ++a)
+            for (int i = 0; i < fo; ++i) h[(size_t)(kb + a) * nxp + kb + i] = (T)Vo[(size_t)a * fo + i];
         SOLVE_TRY(cudaMalloc((void **)dst, sizeof(T) * h.size()));
         SOLVE_TRY(cudaMemcpy(*dst, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
         return IGA_OK;
     };
+    // padded eigenvalues 1 keep the scaling finite
     auto up_vec = [&](T **dst, const std::vector<double> &v, int np) -> int {
         std::vector<T> h(np, T(1));
-        for (size_t i = 0; i < v.size(); ++i) h[i] = (T)v[i];
+        for (size_t i = 0; i < v.size(); ++i) h[row_of((int)i)] = (T)v[i];
         SOLVE_TRY(cudaMalloc((void **)dst, sizeof(T) * h.size()));
         SOLVE_TRY(cudaMemcpy(*dst, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
         return IGA_OK;
     };
-    // y factors in the layout of Wt: element (b, a) at b + a nyp
+    // y factors in the layout of Wt: element (b, row_of(a)) at b + row_of(a) nyp
+    // (padded modes: zero factors, so their solves return zeros)
     auto up_fac = [&](T **dst, const std::vector<double> &F) -> int {
         std::vector<T> h((size_t)nxp * nyp, T(0));
         for (int a = 0; a < nx; ++a)
-            for (int b = 0; b < ny; ++b) h[(size_t)a * nyp + b] = (T)F[(size_t)a * ny + b];
+            for (int b = 0; b < ny; ++b) h[(size_t)row_of(a) * nyp + b] = (T)F[(size_t)a * ny + b];
         SOLVE_TRY(cudaMalloc((void **)dst, sizeof(T) * h.size()));
         SOLVE_TRY(cudaMemcpy(*dst, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
         return IGA_OK;
     };
     int st;
-    if ((st = up_mat(&ps.Vx, S->Vx, nx, nxp)) || (st = up_vec(&ps.lx, S->lamx, nxp)) || (st = up_fac(&ps.Dv, S->Dv)) ||
+    if ((st = up_mat(&ps.Vx)) || (st = up_vec(&ps.lx, S->lamx, nxp)) || (st = up_fac(&ps.Dv, S->Dv)) ||
         (st = up_fac(&ps.Lf, S->Lf)))
         return st;
     ps.tri_w = tri_warps(nyp, sizeof(T), ps.tri_smem);
@@ -1164,7 +1308,11 @@ static int fd_upload(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
 //   W1[a][b] = sum_k Vx[a][k] W2[b][k]   (both operands K-major),
 //   W2[b][i] = sum_a W1[a][b] Vx[a][i]   (both operands MN-major),
 // with Vx[a][k] = component k of eigenvector a (ld nxp), W1 [nxp][nyp],
-// W2 [nyp][nxp]. FP32: tcgen05 TF32 tiles fed by tensor maps built here once
+// W2 [nyp][nxp]. With the parity split, W2's columns (the GEMMs' k for the
+// first, their n for the second) are the even folds then the odd folds, and
+// Vx is block diagonal at kb (even modes' half vectors, odd modes' half
+// vectors): each output tile runs over its own block's k range only, half
+// the flops of the full transforms. FP32: tcgen05 TF32 tiles fed by tensor maps built here once
 // (the preconditioner only has to be a close SPD approximation of K_fem^-1;
 // the flexible PCG and the FP64 refinement absorb the difference); FP64:
 // DMMA tiles.
@@ -1174,9 +1322,9 @@ static int transform_gemm(PrecState<double> &ps, const iga_plan *, int which, cu
     const int nxp = ps.nxp, nyp = ps.nyp;
     if (which == 1)
         return gemm_f64_launch(GemmOperand{ps.Vx, nxp, false}, GemmOperand{ps.W2, nxp, false}, ps.W1, nyp, nxp, nyp,
-                               nxp, nxp, nyp, s);
+                               nxp, nxp, nyp, s, GemmScatter(), GemmSplit{ps.kb, false});
     return gemm_f64_launch(GemmOperand{ps.W1, nyp, true}, GemmOperand{ps.Vx, nxp, true}, ps.W2, nxp, nyp, nxp, nxp, nyp,
-                           nxp, s, sc);
+                           nxp, s, sc, GemmSplit{ps.kb, true});
 }
 
 static int transform_gemm(PrecState<float> &ps, const iga_plan *pl, int which, cudaStream_t s,
@@ -1192,7 +1340,8 @@ static int transform_gemm(PrecState<float> &ps, const iga_plan *pl, int which, c
 // lx[a] My + Ky: Wt = R^T Vx (so that each mode's y values are contiguous),
 // column a of Wt solved along y, Z = Vx Wt^T. Two GEMMs and one pass of
 // tridiagonal solves (the fast diagonalisation in both directions would take
-// four GEMMs).
+// four GEMMs). With the parity split the gather folds r (r[i] +- r[nx-1-i]),
+// the GEMMs work on the two half blocks, and the unfold kernel forms z.
 // V is the vectors' type; an FP32 transform of FP64 vectors (T = float,
 // V = double) passes sc, the device scalars whose rr scales the data.
 template <typename T, typename V>
@@ -1208,30 +1357,41 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
     seg |= 1;   // odd: conflict-free shared-memory rows
     constexpr int VN = Pk<T>::n;
     SOLVE_TRY(launch_k(fd_gather_kernel<T, V>, grid2d(nxp / VN, nyp), dim3(128), 0, S->stream, r, ps.W2, z, m, n, nx, ny,
-                       nxp, nyp, sc));
+                       nxp, nyp, ps.kb, ps.fo, sc));
     int e = transform_gemm(ps, pl, 1, S->stream);
     if (e == IGA_OK) {
         if (ps.tri_w) {
             // one mode per warp as long as the modes reach every SM, else the most
             // warps per CTA that shared memory allows (warps then loop over modes)
-            const int w = std::max(1, std::min(ps.tri_w, (nx + ps.nsm - 1) / ps.nsm));
-            const int grid = std::min((nx + w - 1) / w, ps.nsm);
+            const int nm = ps.nmodes;
+            const int w = std::max(1, std::min(ps.tri_w, (nm + ps.nsm - 1) / ps.nsm));
+            const int grid = std::min((nm + w - 1) / w, ps.nsm);
             const size_t smem = ps.tri_smem / ps.tri_w * w;
             SOLVE_TRY(launch_k(fd_tri_kernel<T, true>, dim3(grid), dim3(w * 32), smem, S->stream, ps.W1,
-                               (const T *)ps.Lf, (const T *)ps.Dv, nx, ny, nyp, seg, S->s));
+                               (const T *)ps.Lf, (const T *)ps.Dv, nm, ny, nyp, seg, S->s));
         } else {
-            SOLVE_TRY(launch_k(fd_tri_kernel<T, false>, dim3((nx + 7) / 8), dim3(256), 0, S->stream, ps.W1,
-                               (const T *)ps.Lf, (const T *)ps.Dv, nx, ny, nyp, seg, S->s));
+            SOLVE_TRY(launch_k(fd_tri_kernel<T, false>, dim3((ps.nmodes + 7) / 8), dim3(256), 0, S->stream, ps.W1,
+                               (const T *)ps.Lf, (const T *)ps.Dv, ps.nmodes, ny, nyp, seg, S->s));
         }
-        // the second GEMM's epilogue writes z's interior itself
-        GemmScatter gs;
-        gs.out = z;
-        gs.f64 = std::is_same<V, double>::value;
-        gs.ld = m;
-        gs.rows = ny;
-        gs.cols = nx;
-        gs.rr = sc ? &sc->rr : nullptr;
-        e = transform_gemm(ps, pl, 2, S->stream, gs);
+        if (ps.kb > 0) {
+            // parity split: the second GEMM writes both halves' products, the
+            // unfold kernel combines them into z's interior
+            e = transform_gemm(ps, pl, 2, S->stream);
+            if (e == IGA_OK)
+                SOLVE_TRY(launch_k(fd_unfold_kernel<T, V>, grid2d(ps.fe, ny), dim3(128), 0, S->stream,
+                                   (const T *)ps.W2, z, m, nx, ny, nxp, ps.kb, ps.fe, ps.fo,
+                                   sc ? &sc->rr : (const double *)nullptr));
+        } else {
+            // the second GEMM's epilogue writes z's interior itself
+            GemmScatter gs;
+            gs.out = z;
+            gs.f64 = std::is_same<V, double>::value;
+            gs.ld = m;
+            gs.rows = ny;
+            gs.cols = nx;
+            gs.rr = sc ? &sc->rr : nullptr;
+            e = transform_gemm(ps, pl, 2, S->stream, gs);
+        }
     }
     if (e != IGA_OK) {
         set_error("GEMM launch failed in the FEM preconditioner: " + last_error());
@@ -1604,6 +1764,18 @@ int iga_pc_apply(iga_plan *pl, int pc, int prec, const void *r, void *z, double 
     SOLVE_TRY(cudaStreamWaitEvent((cudaStream_t)stream, ev, 0));
     cudaEventDestroy(ev);
     return st;
+}
+
+int iga_plan_set_pc_split(iga_plan *pl, int enable)
+{
+    if (!pl || (enable != 0 && enable != 1)) return IGA_ERR_ARG;
+    if (pl->solver) {
+        cudaSetDevice(pl->device);
+        cudaDeviceSynchronize();
+        iga_solver_release(pl);
+    }
+    pl->pc_split = enable != 0;
+    return IGA_OK;
 }
 
 int iga_fem_apply(iga_plan *pl, int prec, const void *x, void *y, void *stream)

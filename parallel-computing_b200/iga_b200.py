@@ -107,6 +107,7 @@ SIGNATURES = [
     ("iga_rhs", ctypes.c_int, [VP, ctypes.c_int, VP, VP]),
     ("iga_plan_device_status", ctypes.c_int, [VP, VP]),
     ("iga_plan_set_wait_limit", ctypes.c_int, [VP, ctypes.c_longlong]),
+    ("iga_plan_set_pc_split", ctypes.c_int, [VP, ctypes.c_int]),
     ("iga_MatrixFreeMatMultCUDA", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 15),
     ("iga_MatrixFreeMatMultCUDA_release", ctypes.c_int, []),
     ("iga_MatrixFreeMatMultCUDA_noalloc", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 16),
@@ -628,6 +629,11 @@ class Plan:
     def set_wait_limit(self, polls):
         """Test hook: polls per bounded wait of the MatMult kernel (< 0: default)."""
         _check(_lib().iga_plan_set_wait_limit(self.h, int(polls)), "iga_plan_set_wait_limit")
+
+    def set_pc_split(self, enable):
+        """Test hook: 0 makes the exact FEM preconditioner use full x
+        transforms instead of the parity-split ones (drops the solver state)."""
+        _check(_lib().iga_plan_set_pc_split(self.h, int(enable)), "iga_plan_set_pc_split")
 
     def solve(self, b, x, stream=None, check=True, **kw):
         """Solve K x = b (SPD form) on the device; keyword arguments set iga_solve_opts fields."""

@@ -223,6 +223,41 @@ def test_exact_pc_multi_tile_transforms(torch_cuda, ib, nex, ney):
     plan.close()
 
 
+@pytest.mark.parametrize("p,nex,ney", [(3, 300, 260), (3, 517, 130), (2, 16, 20), (4, 5, 7), (2, 1, 9)])
+def test_exact_pc_parity_split_equals_full_transforms(torch_cuda, ib, p, nex, ney):
+    """The exact inverse's x transforms split by parity (the FEM nodes are
+    symmetric about the patch middle: even/odd folds of r, half-size
+    eigenvector blocks, GEMM tiles over one block's k range, unfold into z)
+    give the same z as the full transforms: FP64 to 1e-12, and the FP32 (TF32)
+    forms both within 1e-2 of the FP64 z. Odd and even numbers of free x
+    nodes (301, 518, 16, 7) and one free x node (no split possible)."""
+    torch = torch_cuda
+    mesh = distorted(ib.unit_square(p, nex, ney)) if nex > 1 else ib.unit_square(p, nex, ney)
+    plan = ib.Plan(mesh, precision=ib.MIXED)
+    m, n = nex + p, ney + p
+    r = torch.from_numpy(splitmix_uniform(21, -1, 1, plan.nfunc)).cuda()
+    r[torch.from_numpy(boundary_mask(m, n)).cuda()] = 0
+    out = {}
+    for split in (1, 0):
+        plan.set_pc_split(split)
+        z = torch.empty_like(r)
+        plan.pc_apply(r, z, pc=ib.PC_FEM_EXACT, precision=ib.FP64)
+        z32 = torch.empty_like(r.float())
+        plan.pc_apply(r.float(), z32, pc=ib.PC_FEM_EXACT, precision=ib.FP32)
+        torch.cuda.synchronize()
+        assert plan.device_status() == 0
+        out[split] = (z.clone(), z32.double())
+    y = torch.empty_like(r)
+    plan.fem_apply(out[1][0], y, precision=ib.FP64)
+    torch.cuda.synchronize()
+    assert float((y - r).norm() / r.norm()) < 1e-10
+    z1, z0 = out[1][0], out[0][0]
+    assert float((z1 - z0).norm() / z0.norm()) < 1e-12
+    for s in (1, 0):
+        assert float((out[s][1] - z0).norm() / z0.norm()) < 1e-2
+    plan.close()
+
+
 @pytest.mark.parametrize("ney", [9700, 19400, 95])
 def test_exact_pc_long_columns(torch_cuda, ib, ney):
     """Tall meshes: the y tridiagonal solves of the exact inverse run on columns of
