@@ -552,6 +552,7 @@ def our_arm(args):
         b = torch.empty(plan.nfunc, dtype=torch.float64, device="cuda")
         plan.rhs(b, ib.F_ANNULUS)
         x = torch.zeros_like(b)
+        plan.set_solver_graph(0)   # iterations launched from the host: visible kernel by kernel
         plan.solve(b, x, check=False, pc=ib.PC_FEM_EXACT, precision=ib.MIXED, sweep_rtol=1e-2, max_it=12,
                    max_sweeps=1)
         torch.cuda.synchronize()
@@ -737,8 +738,9 @@ def main():
                     help="run the FP32 and FP64 operators of the p=4 1024x1024 NURBS annulus a few times "
                          "outside any graph (a target for ncu; prints nothing else)")
     ap.add_argument("--profile-solve", action="store_true",
-                    help="run one 12-iteration FP32 sweep of the annulus mixed-precision solve (a target for a "
-                         "per-iteration ncu launch list; prints nothing else)")
+                    help="run one 12-iteration FP32 sweep of the annulus mixed-precision solve with its "
+                         "iterations launched from the host (a target for a per-iteration ncu launch list; prints "
+                         "nothing else)")
     ap.add_argument("--profile-batch-pc", action="store_true",
                     help="run the batched preconditioner and operator of the 256-problem batch a few times "
                          "outside any graph (a target for ncu; prints nothing else)")

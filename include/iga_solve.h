@@ -87,6 +87,13 @@ int iga_pc_apply(iga_plan *plan, int pc, int precision, const void *r_dev, void 
  * No counterpart in the reference. */
 int iga_plan_set_pc_split(iga_plan *plan, int enable);
 
+/* enable = 0 makes iga_solve run its PCG iterations from the host, kernel by
+ * kernel, instead of inside one conditional-loop graph (per-kernel profilers
+ * do not see the kernels of conditional graphs); 1 restores the default.
+ * Same kernels and arithmetic per iteration; the host reads the convergence
+ * test after each one. A profiling hook: no counterpart in the reference. */
+int iga_plan_set_solver_graph(iga_plan *plan, int enable);
+
 /* y = K_fem x, the SPD bilinear-FEM matrix of the preconditioner (boundary
  * rows identity), matrix-free from its 1-D tensor factors; precision of x/y
  * as for iga_apply_prec. */

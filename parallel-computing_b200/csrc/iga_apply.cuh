@@ -117,10 +117,26 @@ __device__ __forceinline__ T shfl_idx(T v, int src)
     return __shfl_sync(0xffffffffu, v, src);
 }
 
+// 1 / v for the Jacobian determinant of the on-the-fly geometry (v > 0 and
+// far from the extremes of the exponent range). FP64: the hardware's
+// approximate reciprocal (rcp.approx.ftz.f64) refined by two Newton-Raphson
+// steps y <- y + y (1 - v y), each of which squares the relative error, so
+// the result is within a few units in the last place of 1 / v; five FP64
+// instructions in place of the correctly rounded reciprocal's longer
+// sequence with its special-case branch. The operator is checked against
+// the oracle at 1e-12 relative.
 template <typename T>
 __device__ __forceinline__ T recip(T v);
 template <>
-__device__ __forceinline__ double recip<double>(double v) { return __drcp_rn(v); }
+__device__ __forceinline__ double recip<double>(double v)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(v));
+    double e = fma(-v, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-v, y, 1.0);
+    return fma(y, e, y);
+}
 template <>
 __device__ __forceinline__ float recip<float>(float v) { return __frcp_rn(v); }
 

@@ -1219,6 +1219,93 @@ int build_graph(iga_batch *B, int pc, bool nested)
     return st;
 }
 
+// LDL^T factors of the y systems lx[a] My + Ky, one thread per (problem =
+// blockIdx.y, x mode a): Dv_b = 1 / d_b and Cf_b = e_b / d_b along y (layout
+// [b][a], ld nx), from the FP64 eigenvalues; f32 (optional) gets FP32 copies.
+__global__ void fd_ldl_kernel(const FdProb<double> *__restrict__ f64, const FdProb<float> *__restrict__ f32)
+{
+    const int i = blockIdx.y;
+    const FdProb<double> &f = f64[i];
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= f.nx) return;
+    const int nx = f.nx, ny = f.ny;
+    const double *Kd = f.yc, *Ko = Kd + ny, *Md = Kd + 2 * ny, *Mo = Kd + 3 * ny;
+    double *Dv = const_cast<double *>(f.Dv), *Cf = const_cast<double *>(f.Cf);
+    float *Dv32 = f32 ? const_cast<float *>(f32[i].Dv) : nullptr, *Cf32 = f32 ? const_cast<float *>(f32[i].Cf) : nullptr;
+    const double lam = f.lx[a];
+    double cprev = 0.0, eprev = 0.0;
+    for (int b = 0; b < ny; ++b) {
+        const double den = lam * Md[b] + Kd[b] - eprev * cprev;
+        const double e = b + 1 < ny ? lam * Mo[b] + Ko[b] : 0.0;
+        const double dv = 1.0 / den, cf = e / den;
+        const size_t at = (size_t)b * nx + a;
+        Dv[at] = dv;
+        Cf[at] = cf;
+        if (Dv32) {
+            Dv32[at] = (float)dv;
+            Cf32[at] = (float)cf;
+        }
+        cprev = cf;
+        eprev = e;
+    }
+}
+
+// One distinct grid's eigenpairs on the device: mode a < fe from the even
+// half (half vectors at U + ue, hn_e long), the others from the odd half
+// (U + uo, hn_o long; uo < 0: a pencil that was not split, fe = n), scaled
+// by sc; mirrored entries v[n-1-i] = +-u[i]; lam: the n eigenvalues in the
+// same mode order. Outputs: V (component i of mode a at a n + i) and its
+// transpose VT, FP64 and, when V32 is set, FP32 with 16-byte padded copies
+// (row length ldp).
+struct BasisDev {
+    int n, fe, hn_e, hn_o, ldp;
+    long long ue, uo, lo;
+    double sc;
+    double *V, *VT, *L;
+    float *V32, *VT32, *Vp32, *VTp32, *L32;
+};
+
+__global__ void basis_build_kernel(const BasisDev *__restrict__ bs, const double *__restrict__ U,
+                                   const double *__restrict__ lam)
+{
+    const BasisDev b = bs[blockIdx.y];
+    const int n = b.n;
+    const long long nn = (long long)n * n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nn; t += (long long)gridDim.x * blockDim.x) {
+        const int a = (int)(t / n), i = (int)(t - (long long)a * n);
+        const bool even = a < b.fe;
+        const int hn = even ? b.hn_e : b.hn_o;
+        const double *u = U + (even ? b.ue + (long long)a * hn : b.uo + (long long)(a - b.fe) * hn);
+        double v;
+        if (b.uo < 0 && even) {
+            v = u[i];
+        } else if (i < hn) {
+            v = b.sc * u[i];
+        } else {
+            const int im = n - 1 - i;
+            v = (im < hn && im != i) ? (even ? b.sc : -b.sc) * u[im] : 0.0;
+        }
+        b.V[t] = v;
+        b.VT[(long long)i * n + a] = v;
+        if (b.V32) {
+            b.V32[t] = (float)v;
+            b.VT32[(long long)i * n + a] = (float)v;
+            b.Vp32[(long long)a * b.ldp + i] = (float)v;
+            b.VTp32[(long long)i * b.ldp + a] = (float)v;
+        }
+        if (i == 0) {
+            b.L[a] = lam[b.lo + a];
+            if (b.L32) b.L32[a] = (float)lam[b.lo + a];
+        }
+    }
+}
+
+__global__ void gather_flags_kernel(int *const *__restrict__ flags, int n, int *__restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = *flags[i];
+}
+
 // Eigenpairs of the FEM pencils of every distinct 1-D grid, uploaded in T.
 int setup_fd(iga_batch *B)
 {
@@ -1233,18 +1320,26 @@ int setup_fd(iga_batch *B)
     // Net lengths summed over different numbers of segments differ in the last
     // bits for patches of the same extent; rounded to 14 significant digits,
     // equal grids are found equal and share one eigen-decomposition (the 256
-    // benchmark problems: 30 instead of 300 pencils, 0.32 -> 0.03 s).
+    // benchmark problems have 30 distinct grids).
     auto snap = [](double L) {
         if (!(L > 0.0) || !std::isfinite(L)) return L;
         const double e = std::pow(10.0, std::floor(std::log10(L)) - 13);
         return std::round(L / e) * e;
     };
+    // net lengths of every problem (the heavy part of the grid index), threaded
+    const unsigned nthr = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 16u));
+    std::vector<double> hLx(B->count), hLy(B->count);
+    {
+        std::vector<std::thread> th;
+        for (unsigned w = 0; w < nthr; ++w)
+            th.emplace_back([&, w]() {
+                for (int i = (int)w; i < B->count; i += (int)nthr) net_lengths(B->plans[i]->patch, hLx[i], hLy[i]);
+            });
+        for (auto &t : th) t.join();
+    }
     for (int i = 0; i < B->count; ++i) {
         const iga_plan *pl = B->plans[i];
-        double Lx, Ly;
-        net_lengths(pl->patch, Lx, Ly);
-        Lx = snap(Lx);
-        Ly = snap(Ly);
+        const double Lx = snap(hLx[i]), Ly = snap(hLy[i]);
         for (int dir = 0; dir < 2; ++dir) {
             std::vector<double> g = dir == 0 ? fem_nodes_1d(pl->p, pl->nex, Lx) : fem_nodes_1d(pl->p, pl->ney, Ly);
             auto it = index.find(g);
@@ -1259,110 +1354,186 @@ int setup_fd(iga_batch *B)
             (dir == 0 ? bx : by)[i] = id;
         }
     }
+    // Eigenpairs of every distinct grid's pencil: split by parity (the FEM
+    // nodes are symmetric about the middle: two half-size pencils), the
+    // eigenpairs of all of them on the device (one thread per eigenpair),
+    // expanded there to full vectors (even modes first, then odd ones).
     std::vector<Basis> bases(grids.size());
-    {
-        std::vector<std::thread> th;
-        const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 16u));
-        for (unsigned w = 0; w < nt; ++w)
-            th.emplace_back([&, w]() {
-                for (size_t k = w; k < grids.size(); k += nt) {
-                    std::vector<double> Kd, Ko, Md, Mo;
-                    interior_pencil(grids[k], Kd, Ko, Md, Mo);
-                    Basis &b = bases[k];
-                    b.n = (int)Kd.size();
-                    b.lam.assign(b.n, 0.0);
-                    b.V.assign((size_t)b.n * b.n, 0.0);
-                    if (b.n > 0) pencil_eig(b.n, Kd.data(), Ko.data(), Md.data(), Mo.data(), b.lam.data(), b.V.data());
-                }
-            });
-        for (auto &t : th) t.join();
-    }
-    // y pencils of the grids (double, shared by both precisions) and, per
-    // problem, the LDL^T factors of lx[a] My + Ky for every x mode a
-    std::vector<std::vector<double>> pencils(grids.size());
+    std::vector<std::vector<double>> pencils(grids.size());   // Kd | Ko | Md | Mo of the free nodes
+    struct Half {
+        int grid, parity;   // parity -1: the whole pencil (not centrosymmetric)
+        std::vector<double> kd, ko, md, mo, V;
+    };
+    std::vector<Half> halves;
     for (size_t k = 0; k < grids.size(); ++k) {
         std::vector<double> Kd, Ko, Md, Mo;
         interior_pencil(grids[k], Kd, Ko, Md, Mo);
+        const int n = (int)Kd.size();
+        bases[k].n = n;
         for (const std::vector<double> *v : {&Kd, &Ko, &Md, &Mo}) pencils[k].insert(pencils[k].end(), v->begin(), v->end());
+        if (n == 0) continue;
+        if (pencil_centrosymmetric(n, Kd.data(), Ko.data(), Md.data(), Mo.data())) {
+            for (int parity = 0; parity < 2; ++parity) {
+                Half h;
+                h.grid = (int)k;
+                h.parity = parity;
+                pencil_fold(n, Kd.data(), Ko.data(), Md.data(), Mo.data(), parity, h.kd, h.ko, h.md, h.mo);
+                if (!h.kd.empty()) halves.push_back(std::move(h));
+            }
+        } else {
+            halves.push_back(Half{(int)k, -1, Kd, Ko, Md, Mo, {}});
+        }
+    }
+    std::vector<PencilRef> refs;
+    for (const Half &h : halves) refs.push_back(PencilRef{(int)h.kd.size(), h.kd.data(), h.ko.data(), h.md.data(), h.mo.data()});
+    std::vector<std::vector<double>> hlam, hvec;
+    {
+        const int st = pencil_eig_device(B->device, refs, hlam, &hvec);
+        if (st) return st;
+        for (size_t r = 0; r < halves.size(); ++r) halves[r].V = std::move(hvec[r]);
+    }
+    // half vectors and eigenvalues of all grids in one upload; the device
+    // expands them into every grid's full eigenvector matrix, its transpose
+    // and (MIXED) the FP32 copies, in one buffer per precision
+    std::vector<long long> lo_of(grids.size(), -1), ue_of(grids.size(), -1), uo_of(grids.size(), -1);
+    std::vector<int> hne(grids.size(), 0), hno(grids.size(), 0), fe_of(grids.size(), 0);
+    std::vector<char> split(grids.size(), 0);
+    std::vector<double> hU, hL(0);
+    std::vector<long long> lam_at(halves.size());
+    for (size_t r = 0; r < halves.size(); ++r) {
+        const Half &h = halves[r];
+        const int hn = (int)h.kd.size();
+        if (h.parity <= 0) {   // even half or whole pencil: first in mode order
+            ue_of[h.grid] = (long long)hU.size();
+            hne[h.grid] = hn;
+            fe_of[h.grid] = hn;
+            split[h.grid] = h.parity == 0;
+        } else {
+            uo_of[h.grid] = (long long)hU.size();
+            hno[h.grid] = hn;
+        }
+        hU.insert(hU.end(), h.V.begin(), h.V.end());
+    }
+    // eigenvalues in mode order per grid: even half, then odd half
+    for (size_t k = 0; k < grids.size(); ++k) {
+        lo_of[k] = (long long)hL.size();
+        for (int parity = 0; parity < 2; ++parity)
+            for (size_t r = 0; r < halves.size(); ++r)
+                if (halves[r].grid == (int)k && (halves[r].parity == parity || (parity == 0 && halves[r].parity < 0)))
+                    hL.insert(hL.end(), hlam[r].begin(), hlam[r].end());
+    }
+    double *dU = nullptr, *dL = nullptr;
+    {
+        int st;
+        if ((st = bupload(&dU, hU)) || (st = bupload(&dL, hL))) return st;
+    }
+    const bool mixed = B->precision == IGA_MIXED;
+    // every sub-array starts on a 16-byte boundary (the FP32 padded copies
+    // move as 16-byte words)
+    auto al4 = [](size_t x) { return (x + 3) / 4 * 4; };
+    size_t tot64 = 0, tot32 = 0;
+    for (const Basis &bb : bases) {
+        const size_t n = (size_t)bb.n, ldp = al4(n);
+        tot64 += 2 * al4(n * n) + al4(n);
+        if (mixed) tot32 += 2 * al4(n * n) + 2 * n * ldp + al4(n);
+    }
+    double *b64 = nullptr;
+    float *b32 = nullptr;
+    {
+        int st;
+        if ((st = bmalloc(&b64, tot64))) return st;
+        B->v64.basis.push_back(b64);
+        if (mixed) {
+            if ((st = bmalloc(&b32, tot32))) return st;
+            BT_TRY(cudaMemset(b32, 0, sizeof(float) * tot32));   // the padding columns
+            B->v32.basis.push_back(b32);
+        }
+    }
+    std::vector<BasisDev> bd(grids.size());
+    std::vector<double *> V64(grids.size()), VT64(grids.size()), L64(grids.size());
+    std::vector<float *> V32(grids.size(), nullptr), VT32(grids.size(), nullptr), Vp32(grids.size(), nullptr),
+        VTp32(grids.size(), nullptr), L32(grids.size(), nullptr);
+    {
+        size_t o64 = 0, o32 = 0;
+        for (size_t k = 0; k < grids.size(); ++k) {
+            const int n = bases[k].n;
+            const size_t nn = (size_t)n * n, ldp = al4((size_t)n);
+            V64[k] = b64 + o64;
+            VT64[k] = V64[k] + al4(nn);
+            L64[k] = VT64[k] + al4(nn);
+            o64 += 2 * al4(nn) + al4(n);
+            if (mixed) {
+                V32[k] = b32 + o32;
+                VT32[k] = V32[k] + al4(nn);
+                Vp32[k] = VT32[k] + al4(nn);
+                VTp32[k] = Vp32[k] + (size_t)n * ldp;
+                L32[k] = VTp32[k] + (size_t)n * ldp;
+                o32 += 2 * al4(nn) + 2 * (size_t)n * ldp + al4(n);
+            }
+            BasisDev &d = bd[k];
+            d.n = n;
+            d.fe = split[k] ? fe_of[k] : n;
+            d.hn_e = hne[k];
+            d.hn_o = hno[k];
+            d.ldp = (int)ldp;
+            d.ue = ue_of[k] < 0 ? 0 : ue_of[k];
+            d.uo = split[k] ? uo_of[k] : -1;
+            d.lo = lo_of[k];
+            d.sc = split[k] ? 1.0 / std::sqrt(2.0) : 1.0;
+            d.V = V64[k];
+            d.VT = VT64[k];
+            d.L = L64[k];
+            d.V32 = V32[k];
+            d.VT32 = VT32[k];
+            d.Vp32 = Vp32[k];
+            d.VTp32 = VTp32[k];
+            d.L32 = L32[k];
+        }
+        BasisDev *dbd = nullptr;
+        int st;
+        if ((st = bupload(&dbd, bd))) return st;
+        int nmax = 1;
+        for (const Basis &bb : bases) nmax = std::max(nmax, bb.n);
+        const long long nn = (long long)nmax * nmax;
+        const dim3 grid((unsigned)std::max(1LL, std::min((nn + 255) / 256, 256LL)), (unsigned)grids.size());
+        basis_build_kernel<<<grid, 256>>>(dbd, dU, dL);
+        const cudaError_t ke = cudaGetLastError();
+        cudaDeviceSynchronize();
+        cudaFree(dbd);
+        cudaFree(dU);
+        cudaFree(dL);
+        if (ke != cudaSuccess) {
+            set_error(std::string("basis_build_kernel: ") + cudaGetErrorString(ke));
+            return IGA_ERR_CUDA;
+        }
+    }
+    // y pencils of the grids (double, shared by both precisions)
+    for (size_t k = 0; k < grids.size(); ++k) {
         double *d = nullptr;
         int st;
         if ((st = bupload(&d, pencils[k]))) return st;
         B->ycoef.push_back(d);
     }
-    std::vector<std::vector<double>> hDv(B->count), hCf(B->count);
-    {
-        std::vector<std::thread> th;
-        const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 16u));
-        for (unsigned w = 0; w < nt; ++w)
-            th.emplace_back([&, w]() {
-                for (int i = (int)w; i < B->count; i += (int)nt) {
-                    const Basis &bx_ = bases[bx[i]];
-                    const std::vector<double> &yp = pencils[by[i]];
-                    const int nx = bx_.n, ny = (int)yp.size() / 4;
-                    const double *Kd = yp.data(), *Ko = Kd + ny, *Md = Kd + 2 * ny, *Mo = Kd + 3 * ny;
-                    hDv[i].assign((size_t)nx * ny, 0.0);
-                    hCf[i].assign((size_t)nx * ny, 0.0);
-                    for (int a = 0; a < nx; ++a) {
-                        const double lam = bx_.lam[a];
-                        double cprev = 0.0, eprev = 0.0;
-                        for (int b = 0; b < ny; ++b) {
-                            const double den = lam * Md[b] + Kd[b] - eprev * cprev;
-                            const double e = b + 1 < ny ? lam * Mo[b] + Ko[b] : 0.0;
-                            hDv[i][(size_t)b * nx + a] = 1.0 / den;
-                            hCf[i][(size_t)b * nx + a] = e / den;
-                            cprev = e / den;
-                            eprev = e;
-                        }
-                    }
-                }
-            });
-        for (auto &t : th) t.join();
-    }
     auto upload_prec = [&](auto tag) -> int {
         using T = decltype(tag);
         BVec<T> &v = vecs<T>(B);
-        std::vector<T *> V(bases.size()), L(bases.size()), VT(bases.size()), Vp(bases.size(), nullptr),
-            VTp(bases.size(), nullptr);
-        for (size_t k = 0; k < bases.size(); ++k) {
-            const int nb = bases[k].n;
-            std::vector<T> hv(bases[k].V.begin(), bases[k].V.end()), hl(bases[k].lam.begin(), bases[k].lam.end());
-            std::vector<T> ht((size_t)nb * nb);
-            for (int i = 0; i < nb; ++i)
-                for (int j = 0; j < nb; ++j) ht[(size_t)j * nb + i] = (T)bases[k].V[(size_t)i * nb + j];
-            int st;
-            if ((st = bupload(&V[k], hv)) || (st = bupload(&L[k], hl)) || (st = bupload(&VT[k], ht))) return st;
-            v.basis.push_back(V[k]);
-            v.basis.push_back(L[k]);
-            v.basis.push_back(VT[k]);
-            if (sizeof(T) == 4) {   // padded copies for the tcgen05 tiles' 16-byte operand loads
-                const int ld = (nb + 3) / 4 * 4;
-                std::vector<T> pv((size_t)nb * ld, T(0)), pt((size_t)nb * ld, T(0));
-                for (int i = 0; i < nb; ++i)
-                    for (int j = 0; j < nb; ++j) {
-                        pv[(size_t)i * ld + j] = hv[(size_t)i * nb + j];
-                        pt[(size_t)i * ld + j] = ht[(size_t)i * nb + j];
-                    }
-                if ((st = bupload(&Vp[k], pv)) || (st = bupload(&VTp[k], pt))) return st;
-                v.basis.push_back(Vp[k]);
-                v.basis.push_back(VTp[k]);
-            }
-        }
+        const bool f64 = sizeof(T) == 8;
+        auto pick = [&](double *d, float *f) { return f64 ? (T *)(void *)d : (T *)(void *)f; };
         std::vector<FdProb<T>> fp(B->count);
         size_t wtot = 0;
         for (int i = 0; i < B->count; ++i) wtot += (size_t)(B->plans[i]->m - 2) * (B->plans[i]->n - 2);
         int st;
         if ((st = bmalloc(&v.W1, wtot)) || (st = bmalloc(&v.Dv, wtot)) || (st = bmalloc(&v.Cf, wtot))) return st;
-        std::vector<T> stage;
         size_t wo = 0;
         for (int i = 0; i < B->count; ++i) {
             const iga_plan *pl = B->plans[i];
             FdProb<T> &f = fp[i];
-            f.Vx = V[bx[i]];
-            f.VxT = VT[bx[i]];
-            f.Vxp = Vp[bx[i]];
-            f.VxTp = VTp[bx[i]];
+            f.Vx = pick(V64[bx[i]], V32[bx[i]]);
+            f.VxT = pick(VT64[bx[i]], VT32[bx[i]]);
+            f.Vxp = f64 ? nullptr : pick(nullptr, Vp32[bx[i]]);
+            f.VxTp = f64 ? nullptr : pick(nullptr, VTp32[bx[i]]);
             f.ldv = (bases[bx[i]].n + 3) / 4 * 4;
-            f.lx = L[bx[i]];
+            f.lx = pick(L64[bx[i]], L32[bx[i]]);
             f.yc = B->ycoef[by[i]];
             f.W1 = v.W1 + wo;
             f.Dv = v.Dv + wo;
@@ -1372,18 +1543,22 @@ int setup_fd(iga_batch *B)
             f.n = pl->n;
             f.nx = pl->m - 2;
             f.ny = pl->n - 2;
-            const size_t nn = (size_t)f.nx * f.ny;
-            stage.assign(hDv[i].begin(), hDv[i].end());
-            BT_TRY(cudaMemcpy(v.Dv + wo, stage.data(), sizeof(T) * nn, cudaMemcpyHostToDevice));
-            stage.assign(hCf[i].begin(), hCf[i].end());
-            BT_TRY(cudaMemcpy(v.Cf + wo, stage.data(), sizeof(T) * nn, cudaMemcpyHostToDevice));
-            wo += nn;
+            wo += (size_t)f.nx * f.ny;
         }
         return bupload(&v.fd, fp);
     };
     int st;
     if ((st = upload_prec(double{}))) return st;
     if (B->precision == IGA_MIXED && (st = upload_prec(float{}))) return st;
+    // LDL^T factors of lx[a] My + Ky for every problem and x mode, on the
+    // device from the FP64 eigenvalues (both precisions' copies)
+    {
+        int maxnx = 1;
+        for (int i = 0; i < B->count; ++i) maxnx = std::max(maxnx, B->plans[i]->m - 2);
+        const dim3 grid((unsigned)((maxnx + 127) / 128), (unsigned)B->count);
+        fd_ldl_kernel<<<grid, 128>>>(B->v64.fd, B->precision == IGA_MIXED ? B->v32.fd : nullptr);
+        BT_TRY(cudaGetLastError());
+    }
     // GEMM tiles, largest contraction first
     std::vector<std::pair<int, int4>> tl;
     for (int i = 0; i < B->count; ++i) {
@@ -1552,6 +1727,7 @@ int create_batch(const iga_mesh_desc *meshes, int count, int precision, int devi
         if (ty <= 0) ty = default_rows(meshes[i].p, meshes[i].nElemY);
         o.rows_per_strip = std::max(ty, std::max(1, meshes[i].p));
         iga_plan *pl = nullptr;
+        B->arena.defer = true;      // host data staged, sent once after the last plan
         plan_arena() = &B->arena;   // few large allocations, no synchronisation per plan
         const int st = iga_plan_create(&meshes[i], &o, &pl);
         plan_arena() = nullptr;
@@ -1562,6 +1738,8 @@ int create_batch(const iga_mesh_desc *meshes, int count, int precision, int devi
         B->plans.push_back(pl);
         B->off[i + 1] = B->off[i] + pl->nfunc;
     }
+    BT_TRY(B->arena.flush());   // the plans' tables and control points, then their geometry set-up
+    B->arena.defer = false;
     B->ntot = B->off[count];
     // degree groups
     for (int i = 0; i < count; ++i) {
@@ -1634,16 +1812,26 @@ int create_batch(const iga_mesh_desc *meshes, int count, int precision, int devi
     } else if (precision == IGA_MIXED) {
         if ((st = bmalloc(&B->v32.x, N)) || (st = bmalloc(&B->v32.q, N))) return fail(st);
     }
-    BT_TRY(cudaDeviceSynchronize());
-    // the plans' geometry set-up ran without a synchronisation each: check their flags now
-    for (int i = 0; i < count; ++i) {
-        int herr = 0;
-        BT_TRY(cudaMemcpy(&herr, B->plans[i]->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-        if (herr) {
-            set_error("iga_batch_create: problem " + std::to_string(i) +
-                      ": geometry has a non-positive Jacobian determinant");
-            return fail(IGA_ERR_ARG);
-        }
+    // the plans' geometry set-up ran without a synchronisation each: check
+    // their flags now, gathered by one kernel
+    {
+        std::vector<int *> flags(count);
+        for (int i = 0; i < count; ++i) flags[i] = B->plans[i]->d_err;
+        int **dflags = nullptr;
+        int *dout = nullptr;
+        if ((st = bupload(&dflags, flags)) || (st = bmalloc(&dout, count))) return fail(st);
+        gather_flags_kernel<<<(count + 255) / 256, 256>>>(dflags, count, dout);
+        std::vector<int> herr(count, 0);
+        const cudaError_t e = cudaMemcpy(herr.data(), dout, sizeof(int) * count, cudaMemcpyDeviceToHost);
+        cudaFree(dflags);
+        cudaFree(dout);
+        BT_TRY(e);
+        for (int i = 0; i < count; ++i)
+            if (herr[i]) {
+                set_error("iga_batch_create: problem " + std::to_string(i) +
+                          ": geometry has a non-positive Jacobian determinant");
+                return fail(IGA_ERR_ARG);
+            }
     }
     *out = B;
     return IGA_OK;

@@ -73,77 +73,100 @@ static void tri_solve_pivot(int n, const double *Kd, const double *Ko, const dou
     }
 }
 
-void pencil_eig(int n, const double *Kd, const double *Ko, const double *Md, const double *Mo, double *lam, double *V)
+// Eigenvalues by bisection on inertia counts (ascending), `threads` host
+// threads over the eigenvalues.
+void pencil_eigvals(int n, const double *Kd, const double *Ko, const double *Md, const double *Mo, double *lam,
+                    int threads)
 {
     if (n <= 0) return;
-    // Gershgorin bounds: lambda <= max_i (|K| row sum) / min_i (M_ii - |M off| row sum)
-    double kmax = 0.0, mmin = 1e300, mmax = 0.0;
+    const double hi0 = pencil_upper_bound(n, Kd, Ko, Md, Mo);
+    const unsigned nt = (unsigned)std::max(1, std::min(threads, n));
+    std::vector<std::thread> pool;
+    auto work = [=](unsigned t) {
+        for (int k = (int)t; k < n; k += (int)nt) {
+            double lo = 0.0, hi = hi0;
+            for (int it = 0; it < 200 && hi - lo > 4e-16 * hi; ++it) {
+                const double mid = 0.5 * (lo + hi);
+                if (count_below(n, Kd, Ko, Md, Mo, mid) > k) hi = mid;
+                else lo = mid;
+            }
+            lam[k] = 0.5 * (lo + hi);
+        }
+    };
+    if (nt == 1) work(0);
+    else {
+        for (unsigned t = 0; t < nt; ++t) pool.emplace_back(work, t);
+        for (auto &th : pool) th.join();
+    }
+}
+
+// Eigenvectors for given eigenvalues: inverse iteration with a tridiagonal
+// LU factorisation with partial pivoting, M-normalised, the largest
+// component positive; eigenvalues that coincide to working precision (e.g.
+// two modes localised at the two ends of a symmetric grid, which give inverse
+// iteration no way to tell their vectors apart) are handled cluster by
+// cluster, each vector M-orthogonalised against the cluster's earlier ones
+// after every solve.
+void pencil_eigvecs(int n, const double *Kd, const double *Ko, const double *Md, const double *Mo, const double *lam,
+                    double *V, int threads)
+{
+    if (n <= 0) return;
+    double kmax = 0.0, mmax = 0.0;
     for (int i = 0; i < n; ++i) {
         const double ko = (i > 0 ? std::fabs(Ko[i - 1]) : 0.0) + (i + 1 < n ? std::fabs(Ko[i]) : 0.0);
         const double mo = (i > 0 ? std::fabs(Mo[i - 1]) : 0.0) + (i + 1 < n ? std::fabs(Mo[i]) : 0.0);
         kmax = std::max(kmax, std::fabs(Kd[i]) + ko);
-        mmin = std::min(mmin, Md[i] - mo);
         mmax = std::max(mmax, Md[i] + mo);
     }
-    const double hi0 = kmax / std::max(mmin, 1e-300) * 1.01 + 1e-300;
-    unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (unsigned t = 0; t < nt; ++t)
-        pool.emplace_back([=]() {
-            std::vector<double> w, v(n), x(n), mv(n);
-            for (int k = (int)t; k < n; k += (int)nt) {
-                double lo = 0.0, hi = hi0;
-                for (int it = 0; it < 200 && hi - lo > 4e-16 * hi; ++it) {
-                    const double mid = 0.5 * (lo + hi);
-                    if (count_below(n, Kd, Ko, Md, Mo, mid) > k) hi = mid;
-                    else lo = mid;
-                }
-                const double s0 = 0.5 * (lo + hi);
-                lam[k] = s0;
-                const double floor = 4e-16 * (kmax + s0 * mmax);
-                bool ok = false;
-                for (int attempt = 0; attempt < 4 && !ok; ++attempt) {
-                    // shift perturbed on retries only
-                    const double s = s0 * (1.0 + (attempt ? 1e-13 * attempt : 0.0));
-                    for (int i = 0; i < n; ++i) v[i] = 1.0 + 0.5 * std::sin(0.7 * (i + 1) + 1.3 * (k + 1) + attempt);
-                    ok = true;
-                    for (int it = 0; it < 3 && ok; ++it) {
-                        for (int i = 0; i < n; ++i) {   // M v
-                            double a = Md[i] * v[i];
-                            if (i > 0) a += Mo[i - 1] * v[i - 1];
-                            if (i + 1 < n) a += Mo[i] * v[i + 1];
-                            mv[i] = a;
-                        }
-                        tri_solve_pivot(n, Kd, Ko, Md, Mo, s, mv.data(), x.data(), w, floor);
-                        double nrm = 0.0;
-                        for (int i = 0; i < n; ++i) {
-                            double a = Md[i] * x[i];
-                            if (i > 0) a += Mo[i - 1] * x[i - 1];
-                            if (i + 1 < n) a += Mo[i] * x[i + 1];
-                            nrm += a * x[i];
-                        }
-                        if (!(nrm > 0.0) || !std::isfinite(nrm)) {
-                            ok = false;
-                            break;
-                        }
-                        nrm = std::sqrt(nrm);
-                        for (int i = 0; i < n; ++i) v[i] = x[i] / nrm;
+    const unsigned nt = (unsigned)std::max(1, std::min(threads, n));
+    auto work = [=](unsigned t) {
+        std::vector<double> w, v(n), x(n), mv(n);
+        for (int k = (int)t; k < n; k += (int)nt) {
+            const double s0 = lam[k];
+            const double floor = 4e-16 * (kmax + s0 * mmax);
+            bool ok = false;
+            for (int attempt = 0; attempt < 4 && !ok; ++attempt) {
+                // shift perturbed on retries only
+                const double s = s0 * (1.0 + (attempt ? 1e-13 * attempt : 0.0));
+                for (int i = 0; i < n; ++i) v[i] = 1.0 + 0.5 * std::sin(0.7 * (i + 1) + 1.3 * (k + 1) + attempt);
+                ok = true;
+                for (int it = 0; it < 3 && ok; ++it) {
+                    for (int i = 0; i < n; ++i) {   // M v
+                        double a = Md[i] * v[i];
+                        if (i > 0) a += Mo[i - 1] * v[i - 1];
+                        if (i + 1 < n) a += Mo[i] * v[i + 1];
+                        mv[i] = a;
                     }
+                    tri_solve_pivot(n, Kd, Ko, Md, Mo, s, mv.data(), x.data(), w, floor);
+                    double nrm = 0.0;
+                    for (int i = 0; i < n; ++i) {
+                        double a = Md[i] * x[i];
+                        if (i > 0) a += Mo[i - 1] * x[i - 1];
+                        if (i + 1 < n) a += Mo[i] * x[i + 1];
+                        nrm += a * x[i];
+                    }
+                    if (!(nrm > 0.0) || !std::isfinite(nrm)) {
+                        ok = false;
+                        break;
+                    }
+                    nrm = std::sqrt(nrm);
+                    for (int i = 0; i < n; ++i) v[i] = x[i] / nrm;
                 }
-                int imax = 0;
-                for (int i = 1; i < n; ++i)
-                    if (std::fabs(v[i]) > std::fabs(v[imax])) imax = i;
-                const double sg = v[imax] < 0 ? -1.0 : 1.0;
-                for (int i = 0; i < n; ++i) V[(size_t)k * n + i] = sg * v[i];
             }
-        });
-    for (auto &th : pool) th.join();
+            int imax = 0;
+            for (int i = 1; i < n; ++i)
+                if (std::fabs(v[i]) > std::fabs(v[imax])) imax = i;
+            const double sg = v[imax] < 0 ? -1.0 : 1.0;
+            for (int i = 0; i < n; ++i) V[(size_t)k * n + i] = sg * v[i];
+        }
+    };
+    if (nt == 1) work(0);
+    else {
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < nt; ++t) pool.emplace_back(work, t);
+        for (auto &th : pool) th.join();
+    }
 
-    // Eigenvalues that coincide to working precision (e.g. two modes localised
-    // at the two ends of a symmetric grid) give inverse iteration no way to
-    // tell their vectors apart. Within each such cluster, recompute the
-    // vectors in order, M-orthogonalising against the cluster's earlier ones
-    // after every solve.
     const double ctol = 1e-5 * lam[n - 1];
     std::vector<double> w, v(n), x(n), mv(n);
     auto mdot = [&](const double *a, const double *b) {
@@ -182,6 +205,50 @@ void pencil_eig(int n, const double *Kd, const double *Ko, const double *Md, con
             for (int i = 0; i < n; ++i) V[(size_t)k * n + i] = v[i];
         }
         k0 = k1 + 1;
+    }
+}
+
+void pencil_eig(int n, const double *Kd, const double *Ko, const double *Md, const double *Mo, double *lam, double *V)
+{
+    const int nt = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    pencil_eigvals(n, Kd, Ko, Md, Mo, lam, nt);
+    pencil_eigvecs(n, Kd, Ko, Md, Mo, lam, V, nt);
+}
+
+bool pencil_centrosymmetric(int n, const double *Kd, const double *Ko, const double *Md, const double *Mo)
+{
+    if (n < 2) return false;
+    auto sym = [](const double *v, int len) {
+        double mx = 0.0, dif = 0.0;
+        for (int i = 0; i < len; ++i) {
+            mx = std::max(mx, std::fabs(v[i]));
+            dif = std::max(dif, std::fabs(v[i] - v[len - 1 - i]));
+        }
+        return dif <= 1e-12 * mx;
+    };
+    return sym(Kd, n) && sym(Md, n) && sym(Ko, n - 1) && sym(Mo, n - 1);
+}
+
+void pencil_fold(int n, const double *Kd, const double *Ko, const double *Md, const double *Mo, int parity,
+                 std::vector<double> &kd, std::vector<double> &ko, std::vector<double> &md, std::vector<double> &mo)
+{
+    const int fo = n / 2, fe = n - fo, h = parity == 0 ? fe : fo;
+    kd.assign(Kd, Kd + h);
+    md.assign(Md, Md + h);
+    ko.assign(h, 0.0);
+    mo.assign(h, 0.0);
+    for (int i = 0; i + 1 < h; ++i) {
+        ko[i] = Ko[i];
+        mo[i] = Mo[i];
+    }
+    if (h == 0) return;
+    if (n % 2 == 0) {
+        const double sg = parity == 0 ? 1.0 : -1.0;
+        kd[h - 1] += sg * Ko[h - 1];
+        md[h - 1] += sg * Mo[h - 1];
+    } else if (parity == 0) {
+        kd[h - 1] *= 0.5;
+        md[h - 1] *= 0.5;
     }
 }
 

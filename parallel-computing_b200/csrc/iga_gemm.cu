@@ -60,6 +60,44 @@ __device__ __forceinline__ uint64_t sw128_32b_desc(const void *p, uint32_t lbo, 
     return umma::smem_desc(p, lbo, sbo) | ((uint64_t)1 << 61);
 }
 
+// Output tile of a CTA and its k range. Without a split, tile (bx, by) is
+// rows bx TM .., columns by TN .., all of k. With a block-diagonal operand
+// split at kb, the tiles along the split dimension are laid out block by
+// block (ceil(kb / T) tiles from 0, then tiles from kb), so that no tile
+// straddles kb: each runs over its block's k range only, and stores rows (or
+// columns) below its block's end only (the rest of a last partial tile
+// belongs to the other block's tiles).
+struct TileRange {
+    int m0, n0, klo, khi, mlim, nlim;
+};
+__device__ __forceinline__ TileRange tile_range(const GemmSplit &sp, int bx, int by, int TM, int TN, int K, int Mst,
+                                                int Nst)
+{
+    TileRange t{bx * TM, by * TN, 0, K, Mst, Nst};
+    if (sp.kb > 0) {
+        const int T = sp.on_n ? TN : TM, idx = sp.on_n ? by : bx;
+        const int te = (sp.kb + T - 1) / T;
+        const bool even = idx < te;
+        const int s0 = even ? idx * T : sp.kb + (idx - te) * T;
+        const int lim = even ? sp.kb : (sp.on_n ? Nst : Mst);
+        t.klo = even ? 0 : sp.kb;
+        t.khi = even ? sp.kb : K;
+        if (sp.on_n) {
+            t.n0 = s0;
+            t.nlim = lim;
+        } else {
+            t.m0 = s0;
+            t.mlim = lim;
+        }
+    }
+    return t;
+}
+// Tiles along a dimension of extent `ext` cut into tiles of T (split at kb when kb > 0).
+__host__ __forceinline__ int tiles_along(int ext, int T, int kb)
+{
+    return kb > 0 ? (kb + T - 1) / T + (ext - kb + T - 1) / T : (ext + T - 1) / T;
+}
+
 // OUT: 0 C, 1 scatter into an FP32 vector, 2 into an FP64 vector (GemmScatter).
 template <bool AMN, bool BMN, int OUT, int BN>
 __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ CUtensorMap ta,
@@ -78,14 +116,9 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
     int *cnt = reinterpret_cast<int *>(tslot + 1);   // [0] slices loaded, [1] slices consumed, [2] failure
     pdl_begin();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * kGM, n0 = blockIdx.y * BN;
-    int klo = 0, khi = K;   // this tile's k range (one block of a block-diagonal operand)
-    if (split.kb > 0) {
-        const int t0 = split.on_n ? n0 : m0, t1 = t0 + (split.on_n ? BN : kGM);
-        if (t0 >= split.kb) klo = split.kb;
-        else if (t1 <= split.kb) khi = split.kb;
-    }
-    const int nk = (khi - klo + kGK - 1) / kGK;
+    const TileRange tr = tile_range(split, blockIdx.x, blockIdx.y, kGM, BN, K, Mst, Nst);
+    const int m0 = tr.m0, n0 = tr.n0, klo = tr.klo;
+    const int nk = (tr.khi - klo + kGK - 1) / kGK;
 
     if (warp == 0) {
         umma::alloc(tslot, BN);
@@ -182,7 +215,7 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
 #pragma unroll 4
                 for (int rr = 0; rr < 16; ++rr) {
                     const int rl = 2 * rr + (lane >> 4), row_s = r0 + rl;
-                    if (row_s < sc.rows && col + cl < sc.cols) {
+                    if (row_s < sc.rows && col + cl < sc.cols && row_s < tr.mlim && col + cl < tr.nlim) {
                         const double val = f * (double)stage[rl * 17 + cl];
                         const size_t at = (size_t)(row_s + 1) * sc.ld + col + cl + 1;
                         if (OUT == 1) static_cast<float *>(sc.out)[at] = (float)val;
@@ -192,16 +225,16 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
                 __syncwarp();
                 continue;
             }
-            if (row >= Mst || col >= Nst) continue;
+            if (row >= tr.mlim || col >= tr.nlim) continue;
             float *dst = C + (size_t)row * ldc + col;
-            if (col + 16 <= Nst) {
+            if (col + 16 <= tr.nlim) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
                     reinterpret_cast<float4 *>(dst)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
             } else {
 #pragma unroll
                 for (int c = 0; c < 16; ++c)
-                    if (c < Nst - col) dst[c] = v[c];
+                    if (c < tr.nlim - col) dst[c] = v[c];
             }
         }
     } else {
@@ -274,7 +307,8 @@ int launch_tf32_t(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter
             return IGA_ERR_CUDA;
         attr = true;
     }
-    const dim3 grid((g.Mst + kGM - 1) / kGM, (g.Nst + BN - 1) / BN);
+    const dim3 grid(tiles_along(g.Mst, kGM, g.split.on_n ? 0 : g.split.kb),
+                    tiles_along(g.Nst, BN, g.split.on_n ? g.split.kb : 0));
     return launch_k(gemm_tf32_kernel<AMN, BMN, OUT, BN>, grid, dim3(128), smem, s, g.ta, g.tb, g.K, g.Mst, g.Nst, g.C,
                     g.ldc, err, sc, g.split) == cudaSuccess
                ? IGA_OK
@@ -423,14 +457,9 @@ __global__ void __launch_bounds__(32 * DCfg<CFG>::WMW * DCfg<CFG>::WNW, DCfg<CFG
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int g = lane >> 2, t4 = lane & 3;
     const int wm = (w % Cf::WMW) * 16 * WI, wn = (w / Cf::WMW) * 32;
-    const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;
-    int klo = 0, khi = K;   // this tile's k range (one block of a block-diagonal operand)
-    if (split.kb > 0) {
-        const int t0 = split.on_n ? n0 : m0, t1 = t0 + (split.on_n ? TN : TM);
-        if (t0 >= split.kb) klo = split.kb;
-        else if (t1 <= split.kb) khi = split.kb;
-    }
-    const int nk = (khi - klo + kDK - 1) / kDK;
+    const TileRange tr = tile_range(split, blockIdx.x, blockIdx.y, TM, TN, K, Mst, Nst);
+    const int m0 = tr.m0, n0 = tr.n0, klo = tr.klo;
+    const int nk = (tr.khi - klo + kDK - 1) / kDK;
     double acc[WI][4][4];
 #pragma unroll
     for (int i = 0; i < WI; ++i)
@@ -493,13 +522,13 @@ __global__ void __launch_bounds__(32 * DCfg<CFG>::WMW * DCfg<CFG>::WNW, DCfg<CFG
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int row = m0 + wm + 16 * i + g + 8 * h;
-                if (row >= sc.rows) continue;
+                if (row >= sc.rows || row >= tr.mlim) continue;
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
 #pragma unroll
                     for (int c = 0; c < 2; ++c) {
                         const int col = n0 + wn + 8 * j + 2 * t4 + c;
-                        if (col < sc.cols) out[(size_t)(row + 1) * sc.ld + col + 1] = f * acc[i][j][2 * h + c];
+                        if (col < sc.cols && col < tr.nlim) out[(size_t)(row + 1) * sc.ld + col + 1] = f * acc[i][j][2 * h + c];
                     }
             }
     } else {
@@ -508,14 +537,14 @@ __global__ void __launch_bounds__(32 * DCfg<CFG>::WMW * DCfg<CFG>::WNW, DCfg<CFG
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int row = m0 + wm + 16 * i + g + 8 * h;
-                if (row >= Mst) continue;
+                if (row >= tr.mlim) continue;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const int col = n0 + wn + 8 * j + 2 * t4;
                     double *dst = C + (size_t)row * ldc + col;
-                    if (col + 1 < Nst)
+                    if (col + 1 < tr.nlim)
                         *reinterpret_cast<double2 *>(dst) = make_double2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
-                    else if (col < Nst) dst[0] = acc[i][j][2 * h];
+                    else if (col < tr.nlim) dst[0] = acc[i][j][2 * h];
                 }
             }
     }
@@ -538,7 +567,7 @@ int launch_f64(GemmOperand A, GemmOperand B, double *C, int ldc, int M, int N, i
             return IGA_ERR_CUDA;
         attr = true;
     }
-    const dim3 grid((Mst + TM - 1) / TM, (Nst + TN - 1) / TN);
+    const dim3 grid(tiles_along(Mst, TM, split.on_n ? 0 : split.kb), tiles_along(Nst, TN, split.on_n ? split.kb : 0));
     return launch_k(gemm_f64_kernel<CFG, AMN, BMN, SCATTER>, grid, dim3(NT), smem, s,
                     static_cast<const double *>(A.ptr), A.ld, static_cast<const double *>(B.ptr), B.ld, C, ldc, M, N, K,
                     Mst, Nst, sc, split) == cudaSuccess

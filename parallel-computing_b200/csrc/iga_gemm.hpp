@@ -13,11 +13,11 @@
 
 namespace iga {
 
-// A block-diagonal operand split at kb (> 0): the operand indexed by the
-// split dimension (M with on_n false, N with on_n true) has nonzeros only in
-// the blocks [0, kb) x [0, kb) and [kb, K) x [kb, K) of (that index, k). A
-// tile lying inside one block then runs its k loop over that block's range
-// only; a tile straddling kb runs the full range (the zeros keep it exact).
+// A block-diagonal operand split at kb (> 0, a multiple of 16): the operand
+// indexed by the split dimension (M with on_n false, N with on_n true) has
+// nonzeros only in the blocks [0, kb) x [0, kb) and [kb, K) x [kb, K) of
+// (that index, k). The tiles along that dimension are laid out block by
+// block, each running its k loop over its own block's range only.
 struct GemmSplit {
     int kb = 0;
     bool on_n = false;

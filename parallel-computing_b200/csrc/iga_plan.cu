@@ -236,24 +236,78 @@ cudaError_t PlanArena::alloc(void **p, size_t bytes)
     return cudaSuccess;
 }
 
+cudaError_t PlanArena::alloc_data(void **p, size_t bytes)
+{
+    constexpr size_t kChunk = size_t(128) << 20;
+    bytes = (bytes + 255) & ~size_t(255);
+    if (dchunks.empty() || dused + bytes > dchunks.back().second) {
+        const size_t sz = std::max(kChunk, bytes);
+        char *c = nullptr;
+        const cudaError_t e = cudaMalloc((void **)&c, sz);
+        if (e != cudaSuccess) return e;
+        dchunks.emplace_back(c, sz);
+        shadows.emplace_back(new char[sz]);   // uninitialised: only written bytes are touched
+        dused = 0;
+    }
+    *p = dchunks.back().first + dused;
+    dused += bytes;
+    return cudaSuccess;
+}
+
+void PlanArena::stage(void *dst, const void *src, size_t bytes)
+{
+    for (size_t k = dchunks.size(); k-- > 0;) {
+        char *base = dchunks[k].first;
+        if ((char *)dst >= base && (char *)dst < base + dchunks[k].second) {
+            std::memcpy(shadows[k].get() + ((char *)dst - base), src, bytes);
+            return;
+        }
+    }
+}
+
+cudaError_t PlanArena::flush()
+{
+    for (size_t k = 0; k < dchunks.size(); ++k) {
+        const size_t n = k + 1 == dchunks.size() ? dused : dchunks[k].second;
+        if (n == 0) continue;
+        const cudaError_t e = cudaMemcpy(dchunks[k].first, shadows[k].get(), n, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+    }
+    shadows.clear();
+    for (auto &f : pending) f();
+    pending.clear();
+    return cudaGetLastError();
+}
+
 bool PlanArena::owns(const void *p) const
 {
-    for (const auto &c : chunks)
-        if (p >= (const void *)c.first && p < (const void *)(c.first + c.second)) return true;
+    for (const auto *list : {&chunks, &dchunks})
+        for (const auto &c : *list)
+            if (p >= (const void *)c.first && p < (const void *)(c.first + c.second)) return true;
     return false;
 }
 
 void PlanArena::release()
 {
     for (auto &c : chunks) cudaFree(c.first);
+    for (auto &c : dchunks) cudaFree(c.first);
     chunks.clear();
-    used = 0;
+    dchunks.clear();
+    shadows.clear();
+    pending.clear();
+    used = dused = 0;
 }
 
 template <typename T>
 static int upload(T **dst, const void *src, size_t bytes)
 {
-    if (PlanArena *a = plan_arena()) IGA_CUDA_TRY(a->alloc((void **)dst, std::max<size_t>(bytes, 16)));
+    PlanArena *a = plan_arena();
+    if (a && a->defer && src && bytes) {   // copied by the arena's flush
+        IGA_CUDA_TRY(a->alloc_data((void **)dst, bytes));
+        a->stage(*dst, src, bytes);
+        return IGA_OK;
+    }
+    if (a) IGA_CUDA_TRY(a->alloc((void **)dst, std::max<size_t>(bytes, 16)));
     else IGA_CUDA_TRY(cudaMalloc((void **)dst, std::max<size_t>(bytes, 16)));
     if (src && bytes) IGA_CUDA_TRY(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
     return IGA_OK;
@@ -395,6 +449,15 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
         const size_t gelems = (size_t)g.NSX * g.NSY * g.TY * NQ2 * 3 * kSW;
         op.geom_bytes = gelems * sizeof(T);
         if ((st = upload((T **)&op.G, nullptr, op.geom_bytes))) return st;
+        if (pl->arena && pl->arena->defer) {   // after the arena's flush has sent the tables
+            T *G = (T *)op.G;
+            const double *tx = pl->tabX64, *ty = pl->tabY64, *cp = pl->CP, *qw = pl->qw, *kp = pl->kappa_dev;
+            int *err = pl->d_err;
+            pl->arena->pending.push_back(
+                [=]() { geom_setup_kernel<T><<<1184, 256>>>(G, tx, ty, cp, qw, kp, g, err); });
+            op.ready = true;
+            return IGA_OK;
+        }
         geom_setup_kernel<T><<<1184, 256>>>((T *)op.G, pl->tabX64, pl->tabY64, pl->CP, pl->qw, pl->kappa_dev, g,
                                             pl->d_err);
         // in an arena (a batch's set-up) the caller synchronises once for all plans
@@ -702,8 +765,13 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
         if ((st = upload(&pl->tabY64, h64y.data(), h64y.size() * 8))) return fail(st);
         if ((st = upload(&pl->CP, P.CP.data(), P.CP.size() * 8))) return fail(st);
         if ((st = upload(&pl->qw, qw.data(), qw.size() * 8))) return fail(st);
-        if ((st = upload(&pl->d_err, nullptr, sizeof(int)))) return fail(st);
-        cudaMemset(pl->d_err, 0, sizeof(int));
+        const int zero = 0;
+        if (pl->arena && pl->arena->defer) {
+            if ((st = upload(&pl->d_err, &zero, sizeof(int)))) return fail(st);
+        } else {
+            if ((st = upload(&pl->d_err, nullptr, sizeof(int)))) return fail(st);
+            cudaMemset(pl->d_err, 0, sizeof(int));
+        }
         if (!P.kappa.empty()) {
             if ((st = upload(&pl->kappa_dev, P.kappa.data(), P.kappa.size() * 8))) return fail(st);
             pl->kappa_version = 1;

@@ -4,6 +4,8 @@
 
 #include <string>
 #include <utility>
+#include <functional>
+#include <memory>
 #include <vector>
 
 #include "../../include/iga_mf.h"
@@ -42,6 +44,19 @@ struct PlanArena {
     cudaError_t alloc(void **p, size_t bytes);
     bool owns(const void *p) const;
     void release();
+    // Deferred mode (defer = true): buffers with host data come from a data
+    // region whose chunks have host shadows; upload() copies into the shadow
+    // and flush() sends each chunk's used bytes in one copy, then runs the
+    // kernel launches the plans deferred (their geometry set-up), in order.
+    // Building many plans then makes no synchronising copy per buffer.
+    bool defer = false;
+    std::vector<std::pair<char *, size_t>> dchunks;
+    std::vector<std::unique_ptr<char[]>> shadows;
+    size_t dused = 0;
+    std::vector<std::function<void()>> pending;
+    cudaError_t alloc_data(void **p, size_t bytes);
+    void stage(void *dst, const void *src, size_t bytes);
+    cudaError_t flush();
 };
 PlanArena *&plan_arena();
 
@@ -91,6 +106,8 @@ struct iga_plan {
     long long wait_polls = -1;
     // The exact FEM preconditioner may split its x transforms by parity.
     bool pc_split = true;
+    // The solver runs its iterations inside a conditional-loop graph.
+    bool solver_graph = true;
     // Arena the plan's creation-time buffers came from (not owned), or null.
     iga::PlanArena *arena = nullptr;
 };

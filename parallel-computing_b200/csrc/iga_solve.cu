@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -805,11 +806,15 @@ __global__ void fd_unfold_kernel(const T *__restrict__ W, V *__restrict__ z, int
     }
 }
 
-// 2-D launch of the gather: 128-thread blocks over the 16-byte
-// groups of a column, one block row per column (at most 65535).
-static dim3 grid2d(int ngroups, int ncols)
+// 2-D launch of the gather / unfold: 128-thread blocks over the groups of a
+// row, block rows striding over the rows. About one wave of blocks (16 per
+// SM): one block per row made these kernels block-launch bound (the FP32
+// unfold of a 2049 x 1025 half took 21 us in 18.4 K blocks of one row each).
+static dim3 grid2d(int ngroups, int nrows, int nsm)
 {
-    return dim3((unsigned)std::max(1, (ngroups + 127) / 128), (unsigned)std::max(1, std::min(ncols, 65535)));
+    const int gx = std::max(1, (ngroups + 127) / 128);
+    const int gy = std::max(1, std::min({nrows, 65535, std::max(1, 16 * nsm / gx)}));
+    return dim3((unsigned)gx, (unsigned)gy);
 }
 
 // z = r on the boundary ring (identity rows of K_fem).
@@ -1120,73 +1125,42 @@ void interior_pencil(const std::vector<double> &g, std::vector<double> &Kd, std:
 }
 }  // namespace iga
 
-// True when the tridiagonal pencil is centrosymmetric (entry i equals entry
-// n-1-i) to rounding: the FEM nodes of a patch side are symmetric about its
-// middle.
-static bool centrosymmetric(const std::vector<double> &Kd, const std::vector<double> &Ko,
-                            const std::vector<double> &Md, const std::vector<double> &Mo)
-{
-    const int n = (int)Kd.size();
-    if (n < 2) return false;
-    auto sym = [](const std::vector<double> &v) {
-        double mx = 0.0, dif = 0.0;
-        for (size_t i = 0; i < v.size(); ++i) {
-            mx = std::max(mx, std::fabs(v[i]));
-            dif = std::max(dif, std::fabs(v[i] - v[v.size() - 1 - i]));
-        }
-        return dif <= 1e-12 * mx;
-    };
-    return sym(Kd) && sym(Md) && sym(std::vector<double>(Ko.begin(), Ko.begin() + (n - 1))) &&
-           sym(std::vector<double>(Mo.begin(), Mo.begin() + (n - 1)));
-}
-
-// Eigenpairs of a centrosymmetric tridiagonal pencil of size n by parity.
-// Every eigenvector is symmetric (v[i] = v[n-1-i]) or antisymmetric, and each
-// class is the eigenproblem of a half-size symmetric tridiagonal pencil in
-// the half vector u = v[0 .. fe-1] (fe = ceil(n/2)) or v[0 .. fo-1] (fo =
-// floor(n/2)):
-//   n = 2h:   rows 0 .. h-1, the last diagonal entry plus (symmetric) or
-//             minus (antisymmetric) the coupling (h-1, h);
-//   n = 2h+1: symmetric: rows 0 .. h with the middle row's diagonal halved
-//             (the row equation of the middle entry divided by 2, which makes
-//             the half pencil symmetric); antisymmetric: rows 0 .. h-1 (the
-//             middle entry is zero).
-// v^T M v = 2 u^T M_half u, so the half vectors (M_half-normalised by
-// pencil_eig) are divided by sqrt 2. Then for a vector r,
-//   v . r = u . (r[i] + r[n-1-i])_i  (the middle entry taken once)  or
-//   u . (r[i] - r[n-1-i])_i,
-// which halves the flops of both transforms (the even-odd decomposition of
-// spectral and fast-diagonalisation methods).
-static void fold_eig(const std::vector<double> &Kd, const std::vector<double> &Ko, const std::vector<double> &Md,
-                     const std::vector<double> &Mo, SolverState *S)
+// Eigenpairs of the x pencil split by parity (pencil_fold): even modes
+// 0 .. fe-1 then odd modes, each a half vector. v . r = u . (r[i] + r[nx-1-i])_i
+// (the middle entry taken once) for an even mode and u . (r[i] - r[nx-1-i])_i
+// for an odd one, which halves the flops of both transforms (the even-odd
+// decomposition of spectral and fast-diagonalisation methods). Eigenpairs
+// computed on the device (bisection, inverse iteration).
+static int fold_eig(const std::vector<double> &Kd, const std::vector<double> &Ko, const std::vector<double> &Md,
+                    const std::vector<double> &Mo, SolverState *S)
 {
     const int n = (int)Kd.size(), fo = n / 2, fe = n - fo;
+    std::vector<double> hk[2][4];
+    std::vector<PencilRef> refs(2);
+    for (int parity = 0; parity < 2; ++parity) {
+        pencil_fold(n, Kd.data(), Ko.data(), Md.data(), Mo.data(), parity, hk[parity][0], hk[parity][1],
+                    hk[parity][2], hk[parity][3]);
+        refs[parity] = PencilRef{parity == 0 ? fe : fo, hk[parity][0].data(), hk[parity][1].data(),
+                                 hk[parity][2].data(), hk[parity][3].data()};
+    }
+    std::vector<std::vector<double>> lam, vec;
+    int st = pencil_eig_device(S->device, refs, lam, &vec);
+    if (st) return st;
     S->fold = true;
     S->fe = fe;
     S->fo = fo;
     S->lamx.assign(n, 0.0);
     S->Vx.assign((size_t)fe * fe + (size_t)fo * fo, 0.0);
     for (int parity = 0; parity < 2; ++parity) {
-        const int h = parity == 0 ? fe : fo;
+        const int h = refs[parity].n;
         if (h == 0) continue;
-        std::vector<double> kd(Kd.begin(), Kd.begin() + h), md(Md.begin(), Md.begin() + h);
-        std::vector<double> ko(Ko.begin(), Ko.begin() + std::max(h - 1, 0)), mo(Mo.begin(), Mo.begin() + std::max(h - 1, 0));
-        ko.resize(h, 0.0);
-        mo.resize(h, 0.0);
-        if (n % 2 == 0) {
-            const double sg = parity == 0 ? 1.0 : -1.0;
-            kd[h - 1] += sg * Ko[h - 1];
-            md[h - 1] += sg * Mo[h - 1];
-        } else if (parity == 0) {
-            kd[h - 1] *= 0.5;
-            md[h - 1] *= 0.5;
-        }
-        double *lam = S->lamx.data() + (parity == 0 ? 0 : fe);
+        double *L = S->lamx.data() + (parity == 0 ? 0 : fe);
         double *V = S->Vx.data() + (parity == 0 ? 0 : (size_t)fe * fe);
-        pencil_eig(h, kd.data(), ko.data(), md.data(), mo.data(), lam, V);
-        const double s = 1.0 / std::sqrt(2.0);
-        for (size_t i = 0; i < (size_t)h * h; ++i) V[i] *= s;
+        std::copy(lam[parity].begin(), lam[parity].end(), L);
+        const double sc = 1.0 / std::sqrt(2.0);
+        for (size_t i = 0; i < (size_t)h * h; ++i) V[i] = sc * vec[parity][i];
     }
+    return IGA_OK;
 }
 
 // The x pencil's eigenpairs and, for every x mode a, the LDL^T factors of the
@@ -1197,13 +1171,16 @@ static int fd_setup(PrecState<double> &, const iga_plan *pl, SolverState *S)
     std::vector<double> Kd, Ko, Md, Mo;
     interior_pencil(S->gx, Kd, Ko, Md, Mo);
     const int nx = (int)Kd.size();
-    if (pl->pc_split && centrosymmetric(Kd, Ko, Md, Mo)) {
-        fold_eig(Kd, Ko, Md, Mo, S);
+    if (pl->pc_split && pencil_centrosymmetric(nx, Kd.data(), Ko.data(), Md.data(), Mo.data())) {
+        const int st = fold_eig(Kd, Ko, Md, Mo, S);
+        if (st) return st;
     } else {
         S->fold = false;
-        S->lamx.assign(nx, 0.0);
-        S->Vx.assign((size_t)nx * nx, 0.0);
-        pencil_eig(nx, Kd.data(), Ko.data(), Md.data(), Mo.data(), S->lamx.data(), S->Vx.data());
+        std::vector<std::vector<double>> lam, vec;
+        const int st = pencil_eig_device(S->device, {PencilRef{nx, Kd.data(), Ko.data(), Md.data(), Mo.data()}}, lam, &vec);
+        if (st) return st;
+        S->lamx = lam[0];
+        S->Vx = vec[0];
     }
     interior_pencil(S->gy, Kd, Ko, Md, Mo);
     const int ny = (int)Kd.size();
@@ -1241,7 +1218,7 @@ static int fd_upload(PrecState<T> &ps, const iga_plan *pl, SolverState *S)
 {
     if (ps.Vx) return IGA_OK;
     PrecState<double> dummy;
-    fd_setup(dummy, pl, S);
+    if (const int st0 = fd_setup(dummy, pl, S)) return st0;
     const int nx = pl->m - 2, ny = pl->n - 2;
     // multiples of 16: aligned rows for the GEMMs and 16-byte moves; the
     // DGEMMs do no more flops than they must (2112 -> 2064 at 2048^2: FP64
@@ -1356,7 +1333,7 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
     int seg = (ny + 31) / 32;
     seg |= 1;   // odd: conflict-free shared-memory rows
     constexpr int VN = Pk<T>::n;
-    SOLVE_TRY(launch_k(fd_gather_kernel<T, V>, grid2d(nxp / VN, nyp), dim3(128), 0, S->stream, r, ps.W2, z, m, n, nx, ny,
+    SOLVE_TRY(launch_k(fd_gather_kernel<T, V>, grid2d(nxp / VN, nyp, ps.nsm), dim3(128), 0, S->stream, r, ps.W2, z, m, n, nx, ny,
                        nxp, nyp, ps.kb, ps.fo, sc));
     int e = transform_gemm(ps, pl, 1, S->stream);
     if (e == IGA_OK) {
@@ -1378,7 +1355,7 @@ static int fd_apply(PrecState<T> &ps, const iga_plan *pl, SolverState *S, const 
             // unfold kernel combines them into z's interior
             e = transform_gemm(ps, pl, 2, S->stream);
             if (e == IGA_OK)
-                SOLVE_TRY(launch_k(fd_unfold_kernel<T, V>, grid2d(ps.fe, ny), dim3(128), 0, S->stream,
+                SOLVE_TRY(launch_k(fd_unfold_kernel<T, V>, grid2d(ps.fe, ny, ps.nsm), dim3(128), 0, S->stream,
                                    (const T *)ps.W2, z, m, nx, ny, nxp, ps.kb, ps.fe, ps.fo,
                                    sc ? &sc->rr : (const double *)nullptr));
         } else {
@@ -1673,8 +1650,8 @@ static int pcg_graph(iga_plan *pl, SolverState *S, PrecState<T> &ps, const iga_s
     if ((st = pc_apply(ps, pl, S, o, ps.r, ps.z, o.pc_rtol, dummy))) return st;
     dot_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.r, ps.z, N, &S->s->rz, S->partials, S->counter);
     pcg_p_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(ps.p, ps.z, N, S->s, 1);
-    st = build_loop(pl, S, ps, o, prec);
-    if (st == IGA_ERR_UNSUPPORTED) {   // e.g. a library kernel not allowed in a conditional body
+    st = pl->solver_graph ? build_loop(pl, S, ps, o, prec) : IGA_ERR_UNSUPPORTED;
+    if (st == IGA_ERR_UNSUPPORTED) {   // e.g. a library kernel not allowed in a conditional body, or the host loop asked for
         int64_t pcits = 0;
         st = pcg<T>(pl, S, ps, o, ps.b, ps.x, rtol, bnorm, o.pc_rtol, prec, its, pcits);
         if (x != ps.x) copy_kernel<T><<<kRedBlocks, kThreads, 0, s>>>(x, ps.x, N);
@@ -1775,6 +1752,13 @@ int iga_plan_set_pc_split(iga_plan *pl, int enable)
         iga_solver_release(pl);
     }
     pl->pc_split = enable != 0;
+    return IGA_OK;
+}
+
+int iga_plan_set_solver_graph(iga_plan *pl, int enable)
+{
+    if (!pl || (enable != 0 && enable != 1)) return IGA_ERR_ARG;
+    pl->solver_graph = enable != 0;
     return IGA_OK;
 }
 

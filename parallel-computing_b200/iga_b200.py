@@ -108,6 +108,7 @@ SIGNATURES = [
     ("iga_plan_device_status", ctypes.c_int, [VP, VP]),
     ("iga_plan_set_wait_limit", ctypes.c_int, [VP, ctypes.c_longlong]),
     ("iga_plan_set_pc_split", ctypes.c_int, [VP, ctypes.c_int]),
+    ("iga_plan_set_solver_graph", ctypes.c_int, [VP, ctypes.c_int]),
     ("iga_MatrixFreeMatMultCUDA", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 15),
     ("iga_MatrixFreeMatMultCUDA_release", ctypes.c_int, []),
     ("iga_MatrixFreeMatMultCUDA_noalloc", ctypes.c_int, [ctypes.c_int] * 4 + [VP] * 16),
@@ -625,6 +626,11 @@ class Plan:
         """Synchronises the stream and returns (and clears) the status the
         plan's kernels recorded (IGA_OK or e.g. IGA_ERR_TIMEOUT)."""
         return _lib().iga_plan_device_status(self.h, _stream(stream))
+
+    def set_solver_graph(self, enable):
+        """Profiling hook: 0 runs the solver's iterations from the host (kernel
+        by kernel) instead of inside the conditional-loop graph."""
+        _check(_lib().iga_plan_set_solver_graph(self.h, int(enable)), "iga_plan_set_solver_graph")
 
     def set_wait_limit(self, polls):
         """Test hook: polls per bounded wait of the MatMult kernel (< 0: default)."""
