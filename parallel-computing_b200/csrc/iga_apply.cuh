@@ -103,11 +103,42 @@ __host__ __device__ constexpr int apply_stages()
                                                  : (12288 / ApplyShape<P, T>::GBYTES > 8 ? 8 : 12288 / ApplyShape<P, T>::GBYTES);
 }
 
+// Whether a lane keeps its x-direction tables in registers (16 values at
+// p = 3) or reads them from shared memory: registers except where they are
+// the scarcer resource (FP64 p >= 4, FP64 on-the-fly geometry at p <= 2). In
+// registers they save 32 shared loads per element row of a p=3 FP64 strip
+// (12 instead of 13 warps per SM: 1.12x faster), and the warps of a CTA need
+// not share a column strip, so strips are dealt to warps one by one and every
+// SM gets work. The FP64 on-the-fly kernel at p = 3 keeps them in registers
+// at 8 warps per SM (244 registers, no spills; shared tables: 10 warps with
+// spills): 2048^2 673 -> 536 us, 1024^2 208 -> 149 us. At p = 2 the same
+// change was slower (2048^2 392 -> 435 us).
+template <int P, typename T, int GEOM>
+__host__ __device__ constexpr bool apply_txreg()
+{
+    return sizeof(T) == 4 || (GEOM == 0 ? P <= 3 : P == 3);
+}
+
+// Where the tables are not in registers they are either copied to shared
+// memory by a CTA that takes W strips of one column strip, or read by each
+// lane straight from global memory (its own entries, L1-resident: a strip's
+// tables are a few KB reused for every element row), which lets the kernel
+// deal strips to warps one by one and fill the SMs. Measured (B200, warm):
+// FP64 p=4 on-the-fly 1024^2 333 -> 302 us from global memory; FP64 p=4
+// precomputed 152.6 -> 164.8 us and p=5 (both geometry modes) 249 -> 278 /
+// 726 -> 890 us slower that way, so shared memory everywhere else.
+template <int P, typename T, int GEOM>
+__host__ __device__ constexpr bool apply_txshared()
+{
+    return !apply_txreg<P, T, GEOM>() && !(GEOM == 1 && P == 4);
+}
+
 template <int P, typename T, int GEOM, int NST>
 __host__ __device__ constexpr size_t apply_smem_bytes(int W)
 {
     using S = ApplyShape<P, T>;
-    return 256 + (size_t)W * NST * 8 + S::TABX * sizeof(T) + 128 + (GEOM == 0 ? (size_t)W * NST * S::GBYTES : 0) +
+    return 256 + (size_t)W * NST * 8 + (apply_txshared<P, T, GEOM>() ? S::TABX * sizeof(T) : 0) + 128 +
+           (GEOM == 0 ? (size_t)W * NST * S::GBYTES : 0) +
            (size_t)W * S::XR * S::XW * sizeof(T) * (GEOM == 1 ? 3 : 1) + (size_t)W * S::XR * S::TYW * sizeof(T);
 }
 
@@ -152,22 +183,6 @@ __host__ __device__ constexpr int apply_max_threads()
                           : (P <= 2 ? (GEOM ? 384 : 512) : P == 3 ? (GEOM ? 256 : 384) : 256);
 }
 
-// Whether a lane keeps its x-direction tables in registers (16 values at
-// p = 3) or reads them from shared memory: registers except where they are
-// the scarcer resource (FP64 p >= 4, FP64 on-the-fly geometry at p <= 2). In
-// registers they save 32 shared loads per element row of a p=3 FP64 strip
-// (12 instead of 13 warps per SM: 1.12x faster), and the warps of a CTA need
-// not share a column strip, so strips are dealt to warps one by one and every
-// SM gets work. The FP64 on-the-fly kernel at p = 3 keeps them in registers
-// at 8 warps per SM (244 registers, no spills; shared tables: 10 warps with
-// spills): 2048^2 673 -> 536 us, 1024^2 208 -> 149 us. At p = 2 the same
-// change was slower (2048^2 392 -> 435 us).
-template <int P, typename T, int GEOM>
-__host__ __device__ constexpr bool apply_txreg()
-{
-    return sizeof(T) == 4 || (GEOM == 0 ? P <= 3 : P == 3);
-}
-
 // One warp: strip (gx, gy). With tables in shared memory the CTA's warps
 // share the column strip gx (the CTA copies its tables once).
 template <int P, typename T, int GEOM, int NST>
@@ -186,7 +201,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     size_t off = 256 + (size_t)W * NST * 8;
     off = (off + 127) & ~size_t(127);
     T *tabXs = reinterpret_cast<T *>(smem + off);
-    off += S::TABX * sizeof(T);
+    if (apply_txshared<P, T, GEOM>()) off += S::TABX * sizeof(T);
     off = (off + 127) & ~size_t(127);
     T *Gs = reinterpret_cast<T *>(smem + off) + (size_t)w * NST * S::GE;
     if (GEOM == 0) off += (size_t)W * NST * S::GBYTES;
@@ -197,7 +212,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     T *yr = reinterpret_cast<T *>(smem + off) + (size_t)w * S::XR * S::TYW;     // y tables of upcoming rows
     uint64_t *wbar = bars + w * NST;
 
-    if constexpr (!TXREG) {   // x tables of this column strip, shared by the CTA's warps
+    if constexpr (apply_txshared<P, T, GEOM>()) {   // x tables of this column strip, shared by the CTA's warps
         const T *src = a.tabX + (size_t)gx * S::TABX;
         for (int i = threadIdx.y * 32 + lane; i < S::TABX; i += 32 * W) tabXs[i] = src[i];
         __syncthreads();
@@ -260,9 +275,11 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
 #pragma unroll
                 for (int il = 0; il < NB; ++il) txr[kind][j][il] = src[((kind * QH + j) * NB + il) * 32 + lane];
     }
+    const T *txg = a.tabX + (size_t)gx * S::TABX + lane;
     auto tx = [&](int kind, int j, int il) -> T {
         if constexpr (TXREG) return txr[kind][j][il];
-        else return tabXs[((kind * QH + j) * NB + il) * 32 + lane];
+        else if constexpr (apply_txshared<P, T, GEOM>()) return tabXs[((kind * QH + j) * NB + il) * 32 + lane];
+        else return __ldg(txg + ((kind * QH + j) * NB + il) * 32);
     };
 
     T xs0[NB][QH], xs1[NB][QH];     // x contracted with value / derivative tables, rows ey..ey+P
@@ -559,7 +576,7 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kern
 {
     pdl_begin();
     const int rows = min(a.gyn, a.g.NSY - a.gy0);   // strip rows of the window
-    if constexpr (apply_txreg<P, T, GEOM>()) {
+    if constexpr (!apply_txshared<P, T, GEOM>()) {
         const int sid = blockIdx.x * blockDim.y + threadIdx.y;
         const int gx = sid / rows;
         apply_tile<P, T, GEOM, NST>(a, a.x, a.y, gx, a.gy0 + (sid - gx * rows));
@@ -582,7 +599,7 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, 0>(), 1)
                        const int *__restrict__ active, const long long *__restrict__ offs, const T *__restrict__ xb,
                        T *__restrict__ yb)
 {
-    constexpr bool flat = apply_txreg<P, T, 0>();
+    constexpr bool flat = !apply_txshared<P, T, 0>();
     const int4 it = items[flat ? blockIdx.x * blockDim.y + threadIdx.y : blockIdx.x];
     if (it.x < 0 || !active[it.x]) return;   // uniform over the CTA unless flat (no CTA barrier then)
     const long long o = offs[it.x];

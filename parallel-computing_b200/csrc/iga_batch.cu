@@ -22,6 +22,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <string>
 #include <thread>
@@ -1639,7 +1640,8 @@ int setup_items(iga_batch *B, int pi)
             G.items[pi] = nullptr;
         }
         const int W = G.W[pi];
-        // the kernels' apply_txreg: FP32, or FP64 up to p = 3 (precomputed G)
+        // the kernels deal strips to warps unless their tables are in shared
+        // memory (apply_txshared: FP64 p >= 4 with precomputed G)
         const bool flat = pi == 1 || G.P <= 3;
         std::vector<int4> items;
         for (int i = 0; i < B->count; ++i) {
@@ -1716,28 +1718,50 @@ int create_batch(const iga_mesh_desc *meshes, int count, int precision, int devi
             set_error("iga_batch_create: coefficient kappa is not supported in batches");
             return fail(IGA_ERR_UNSUPPORTED);
         }
-        iga_opts o;
-        iga_opts_default(&o);
-        o.precision = precision;
-        o.geometry = IGA_GEOM_PRECOMPUTED;
-        o.sign = IGA_SIGN_SPD;
-        o.bc = IGA_BC_IDENTITY;
-        o.device = device;
-        int ty = rows && rows[i] > 0 ? rows[i] : tune_rows(tt, meshes[i].p, tprec, meshes[i].nElemY);
-        if (ty <= 0) ty = default_rows(meshes[i].p, meshes[i].nElemY);
-        o.rows_per_strip = std::max(ty, std::max(1, meshes[i].p));
-        iga_plan *pl = nullptr;
-        B->arena.defer = true;      // host data staged, sent once after the last plan
-        plan_arena() = &B->arena;   // few large allocations, no synchronisation per plan
-        const int st = iga_plan_create(&meshes[i], &o, &pl);
-        plan_arena() = nullptr;
-        if (st) {
-            set_error("iga_batch_create: problem " + std::to_string(i) + ": " + last_error());
-            return fail(st);
-        }
-        B->plans.push_back(pl);
-        B->off[i + 1] = B->off[i] + pl->nfunc;
     }
+    // The plans are built by host threads (mesh tables, strip layout: host
+    // work), all from the batch's arena in deferred mode: their host data is
+    // staged and sent in one copy after the last plan, their geometry set-up
+    // launched after that.
+    B->arena.defer = true;
+    std::vector<iga_plan *> built(count, nullptr);
+    std::vector<int> status(count, IGA_OK);
+    std::vector<std::string> message(count);
+    {
+        const unsigned nthr = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 16u));
+        std::atomic<int> next{0};
+        auto work = [&]() {
+            cudaSetDevice(device);
+            plan_arena() = &B->arena;
+            for (int i; (i = next.fetch_add(1)) < count;) {
+                iga_opts o;
+                iga_opts_default(&o);
+                o.precision = precision;
+                o.geometry = IGA_GEOM_PRECOMPUTED;
+                o.sign = IGA_SIGN_SPD;
+                o.bc = IGA_BC_IDENTITY;
+                o.device = device;
+                int ty = rows && rows[i] > 0 ? rows[i] : tune_rows(tt, meshes[i].p, tprec, meshes[i].nElemY);
+                if (ty <= 0) ty = default_rows(meshes[i].p, meshes[i].nElemY);
+                o.rows_per_strip = std::max(ty, std::max(1, meshes[i].p));
+                status[i] = iga_plan_create(&meshes[i], &o, &built[i]);
+                if (status[i]) message[i] = last_error();
+            }
+            plan_arena() = nullptr;
+        };
+        std::vector<std::thread> th;
+        for (unsigned w = 1; w < nthr; ++w) th.emplace_back(work);
+        work();
+        for (auto &t : th) t.join();
+    }
+    for (int i = 0; i < count; ++i)
+        if (built[i]) B->plans.push_back(built[i]);
+    for (int i = 0; i < count; ++i)
+        if (status[i]) {
+            set_error("iga_batch_create: problem " + std::to_string(i) + ": " + message[i]);
+            return fail(status[i]);
+        }
+    for (int i = 0; i < count; ++i) B->off[i + 1] = B->off[i] + B->plans[i]->nfunc;
     BT_TRY(B->arena.flush());   // the plans' tables and control points, then their geometry set-up
     B->arena.defer = false;
     B->ntot = B->off[count];

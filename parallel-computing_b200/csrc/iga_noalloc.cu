@@ -180,9 +180,9 @@ int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int 
     a.bc = d_ID ? IGA_BC_NONE : IGA_BC_REFERENCE;
     a.ID = d_ID;
     a.err = reinterpret_cast<int *>(base + Ly.off_err);
-    // tables in registers: strips dealt to warps one by one; else a CTA per W strips of a column
+    // strips dealt to warps one by one; with shared tables a CTA per W strips of a column
     const long long nstrips = (long long)g.NSX * g.NSY;
-    const dim3 grid = apply_txreg<P, double, 1>() ? dim3((unsigned)((nstrips + W - 1) / W))
+    const dim3 grid = !apply_txshared<P, double, 1>() ? dim3((unsigned)((nstrips + W - 1) / W))
                                                   : dim3(g.NSX, (g.NSY + W - 1) / W),
                block(32, W);
     kern<<<grid, block, smem, s>>>(a);

@@ -221,6 +221,7 @@ PlanArena *&plan_arena()
 
 cudaError_t PlanArena::alloc(void **p, size_t bytes)
 {
+    std::lock_guard<std::mutex> lock(mu);
     constexpr size_t kChunk = size_t(256) << 20;
     bytes = (bytes + 255) & ~size_t(255);
     if (chunks.empty() || used + bytes > chunks.back().second) {
@@ -238,6 +239,7 @@ cudaError_t PlanArena::alloc(void **p, size_t bytes)
 
 cudaError_t PlanArena::alloc_data(void **p, size_t bytes)
 {
+    std::lock_guard<std::mutex> lock(mu);
     constexpr size_t kChunk = size_t(128) << 20;
     bytes = (bytes + 255) & ~size_t(255);
     if (dchunks.empty() || dused + bytes > dchunks.back().second) {
@@ -256,13 +258,24 @@ cudaError_t PlanArena::alloc_data(void **p, size_t bytes)
 
 void PlanArena::stage(void *dst, const void *src, size_t bytes)
 {
-    for (size_t k = dchunks.size(); k-- > 0;) {
-        char *base = dchunks[k].first;
-        if ((char *)dst >= base && (char *)dst < base + dchunks[k].second) {
-            std::memcpy(shadows[k].get() + ((char *)dst - base), src, bytes);
-            return;
+    char *shadow = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (size_t k = dchunks.size(); k-- > 0;) {
+            char *base = dchunks[k].first;
+            if ((char *)dst >= base && (char *)dst < base + dchunks[k].second) {
+                shadow = shadows[k].get() + ((char *)dst - base);
+                break;
+            }
         }
     }
+    if (shadow) std::memcpy(shadow, src, bytes);   // disjoint ranges: no lock needed
+}
+
+void PlanArena::defer_launch(std::function<void()> f)
+{
+    std::lock_guard<std::mutex> lock(mu);
+    pending.push_back(std::move(f));
 }
 
 cudaError_t PlanArena::flush()
@@ -281,6 +294,7 @@ cudaError_t PlanArena::flush()
 
 bool PlanArena::owns(const void *p) const
 {
+    std::lock_guard<std::mutex> lock(mu);
     for (const auto *list : {&chunks, &dchunks})
         for (const auto &c : *list)
             if (p >= (const void *)c.first && p < (const void *)(c.first + c.second)) return true;
@@ -391,7 +405,7 @@ static int rows_for(int nex, int ney, const std::vector<WarpShape> &Ws, int nsm)
 
 static bool apply_flat(int P, int prec, int geom)
 {
-    return prec == IGA_FP32 || (geom == IGA_GEOM_PRECOMPUTED ? P <= 3 : P == 3);
+    return prec == IGA_FP32 || (geom == IGA_GEOM_PRECOMPUTED ? P <= 3 : (P == 3 || P == 4));
 }
 
 }  // namespace iga
@@ -453,8 +467,7 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
             T *G = (T *)op.G;
             const double *tx = pl->tabX64, *ty = pl->tabY64, *cp = pl->CP, *qw = pl->qw, *kp = pl->kappa_dev;
             int *err = pl->d_err;
-            pl->arena->pending.push_back(
-                [=]() { geom_setup_kernel<T><<<1184, 256>>>(G, tx, ty, cp, qw, kp, g, err); });
+            pl->arena->defer_launch([=]() { geom_setup_kernel<T><<<1184, 256>>>(G, tx, ty, cp, qw, kp, g, err); });
             op.ready = true;
             return IGA_OK;
         }
@@ -514,7 +527,7 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
         a.gyn = rows;
     }
     const long long nstrips = (long long)g.NSX * rows;
-    dim3 grid = apply_txreg<P, T, GEOM>() ? dim3((unsigned)((nstrips + W - 1) / W)) : dim3(g.NSX, (rows + W - 1) / W);
+    dim3 grid = !apply_txshared<P, T, GEOM>() ? dim3((unsigned)((nstrips + W - 1) / W)) : dim3(g.NSX, (rows + W - 1) / W);
     dim3 block(32, W);
     if (rows > 0) IGA_CUDA_TRY(launch_k(kern, grid, block, smem, s, a));
     if (win.gyn < 0) {

@@ -6,6 +6,7 @@
 #include <utility>
 #include <functional>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "../../include/iga_mf.h"
@@ -50,12 +51,14 @@ struct PlanArena {
     // kernel launches the plans deferred (their geometry set-up), in order.
     // Building many plans then makes no synchronising copy per buffer.
     bool defer = false;
+    mutable std::mutex mu;   // plans may be built by several host threads at once
     std::vector<std::pair<char *, size_t>> dchunks;
     std::vector<std::unique_ptr<char[]>> shadows;
     size_t dused = 0;
     std::vector<std::function<void()>> pending;
     cudaError_t alloc_data(void **p, size_t bytes);
     void stage(void *dst, const void *src, size_t bytes);
+    void defer_launch(std::function<void()> f);
     cudaError_t flush();
 };
 PlanArena *&plan_arena();
