@@ -429,6 +429,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
                 ueta = fma(d2[jl], xs0[jl][j], ueta);
             }
             T g00 = 0, g01 = 0, g11 = 0;
+            T vxi, veta;
             if constexpr (GEOM == 0) {
                 if constexpr (g_lane_major(NQ)) {
                     g00 = gv[3 * j];
@@ -460,17 +461,24 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
                     y_xi = fma(n2[jl], cs[1][1][jl][j], y_xi);
                     y_eta = fma(d2[jl], cs[1][0][jl][j], y_eta);
                 }
+                // G grad u = f adj(J) adj(J)^T grad u with adj(J) = [[y_eta,
+                // -x_eta], [-y_xi, x_xi]] and f = w kappa / det J: ten
+                // operations instead of forming G's three entries (thirteen)
+                vxi = veta = 0;
                 if (valid && ex < g.nex) {
                     T wgt = a.wq[qy * NQ + qx];
                     if (a.kappa) wgt *= a.kappa[((size_t)ey * g.nex + ex) * S::NQ2 + qy * NQ + qx];
                     const T f = wgt * recip(x_xi * y_eta - x_eta * y_xi);
-                    g00 = f * fma(x_eta, x_eta, y_eta * y_eta);
-                    g01 = -f * fma(x_xi, x_eta, y_xi * y_eta);
-                    g11 = f * fma(x_xi, x_xi, y_xi * y_xi);
+                    const T t0 = f * fma(y_eta, uxi, -(y_xi * ueta));
+                    const T t1 = f * fma(x_xi, ueta, -(x_eta * uxi));
+                    vxi = fma(y_eta, t0, -(x_eta * t1));
+                    veta = fma(x_xi, t1, -(y_xi * t0));
                 }
             }
-            const T vxi = fma(g00, uxi, g01 * ueta);
-            const T veta = fma(g01, uxi, g11 * ueta);
+            if constexpr (GEOM == 0) {
+                vxi = fma(g00, uxi, g01 * ueta);
+                veta = fma(g01, uxi, g11 * ueta);
+            }
 #pragma unroll
             for (int jl = 0; jl < NB; ++jl) {
                 acc0[jl][j] = fma(n2[jl], vxi, acc0[jl][j]);

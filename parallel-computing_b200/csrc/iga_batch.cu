@@ -1312,8 +1312,7 @@ int setup_fd(iga_batch *B)
 {
     if (B->fd_ready) return IGA_OK;
     struct Basis {
-        int n;
-        std::vector<double> lam, V;
+        int n = 0;   // free nodes of the grid
     };
     std::map<std::vector<double>, int> index;
     std::vector<std::vector<double>> grids;
@@ -1400,7 +1399,6 @@ int setup_fd(iga_batch *B)
     std::vector<int> hne(grids.size(), 0), hno(grids.size(), 0), fe_of(grids.size(), 0);
     std::vector<char> split(grids.size(), 0);
     std::vector<double> hU, hL(0);
-    std::vector<long long> lam_at(halves.size());
     for (size_t r = 0; r < halves.size(); ++r) {
         const Half &h = halves[r];
         const int hn = (int)h.kd.size();

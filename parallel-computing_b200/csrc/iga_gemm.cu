@@ -15,7 +15,7 @@ namespace iga {
 
 // ------------------------------------------------------------ TF32 on tcgen05
 // One CTA computes a 128 x 128 tile of C with the FP32 accumulator in 128
-// TMEM columns. Thread 0 of warp 0 feeds a ring of kGS stages with the
+// TMEM columns. Thread 0 of warp 0 feeds a ring of 3 or 4 stages with the
 // tensor-memory accelerator: per stage a 32-wide K slice of A (128 rows) and
 // of B (128 rows), 16 KiB each, in the canonical swizzled layouts of the UMMA
 // descriptors (K-major: 128-byte rows of 32 k values, 8-row groups 1 KiB
@@ -30,10 +30,15 @@ namespace iga {
 // The tile width BN is 128, or 64 where the 128-wide grid would leave SMs
 // idle (the 1040 x 1040 transforms of a 1024^2 patch: 81 tiles of 128 x 128
 // on 148 SMs, 153 of 128 x 64).
-constexpr int kGM = 128, kGK = 32, kGS = 3;
+constexpr int kGM = 128, kGK = 32;
 constexpr int kGTileA = kGM * kGK * 4;   // bytes of one A slice
+// Ring stages: 3 for 128-wide tiles (96 KiB, two CTAs per SM); 4 for 64-wide
+// ones (96 KiB as well), whose short k loops (the 1040^2 transforms: 17
+// slices) are bound by the copies' round trips, not the MMAs.
 template <int BN>
-constexpr int gemm_tf32_smem() { return 1024 + kGS * (kGTileA + BN * kGK * 4) + 256; }
+__host__ __device__ constexpr int gemm_tf32_stages() { return BN == 64 ? 4 : 3; }
+template <int BN>
+constexpr int gemm_tf32_smem() { return 1024 + gemm_tf32_stages<BN>() * (kGTileA + BN * kGK * 4) + 256; }
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
 {
@@ -106,6 +111,7 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
                                                         GemmScatter sc, GemmSplit split)
 {
     constexpr int kGTileB = BN * kGK * 4;
+    constexpr int kGS = gemm_tf32_stages<BN>();
     extern __shared__ unsigned char smem_raw[];
     unsigned char *sm =
         reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
