@@ -475,16 +475,21 @@ __global__ void __launch_bounds__(32 * kRowSeg, sizeof(T) == 4 ? 2 : 1) fd_rows_
     }
 }
 
-// Tensor-core tiles: FP64 through DMMA (mma.sync m8n8k4, FP64 accumulate),
+// Tensor-core tiles: FP64 through DMMA (mma.sync m16n8k8, FP64 accumulate),
 // FP32 through TF32 MMA (mma.sync m16n8k8, operands rounded to TF32 once when
 // staged, FP32 accumulate): the FP32 preconditioner only has to be a close
 // SPD approximation of K_fem^-1 (the flexible PCG and the FP64 refinement
 // absorb the difference).
-__device__ __forceinline__ void mma_tile(double (&d)[2], double a, double b)
+// FP64: D (16 x 8) += A (16 x 8) B (8 x 8); fragments (g = lane / 4, t = lane % 4)
+// a = A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g];
+// d = D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1] (the layout of the FP32 tile).
+__device__ __forceinline__ void mma_tile(double (&d)[4], const double (&a)[4], const double (&b)[2])
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(d[0]), "+d"(d[1])
-                 : "d"(a), "d"(b));
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 __device__ __forceinline__ void mma_tile(float (&d)[4], const float (&a)[4], const float (&b)[2])
@@ -594,10 +599,9 @@ __global__ void __launch_bounds__(128) fd_gemm_kernel(const FdProb<T> *__restric
     auto Aat = [&](int buf, int row, int k) -> T { return As[buf][A_KF ? row * LKF + k : k * LRF + row]; };
     auto Bat = [&](int buf, int k, int col) -> T { return Bs[buf][B_KF ? col * LKF + k : k * LRF + col]; };
 
-    constexpr bool F64 = sizeof(T) == 8;
-    constexpr int MB = F64 ? 4 : 2;      // row blocks of the warp tile (8 or 16 rows)
-    constexpr int RB = F64 ? 8 : 16;
-    constexpr int NACC = F64 ? 2 : 4;
+    constexpr int MB = 2;      // row blocks of 16 rows in the warp tile (m16n8k8 in both precisions)
+    constexpr int RB = 16;
+    constexpr int NACC = 4;
     T acc[MB][4][NACC];
 #pragma unroll
     for (int i = 0; i < MB; ++i)
@@ -618,24 +622,9 @@ __global__ void __launch_bounds__(128) fd_gemm_kernel(const FdProb<T> *__restric
     for (int kt = 0; kt < nk; ++kt) {
         const int buf = kt & 1;
         if (kt + 1 < nk) fetch((kt + 1) * kTK);
-        if constexpr (F64) {
 #pragma unroll
-            for (int kk = 0; kk < kTK; kk += 4) {
-                double av[4], bv[4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) av[i] = Aat(buf, wm + i * 8 + g, kk + t4);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) bv[j] = Bat(buf, kk + t4, wn + j * 8 + g);
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                        if (rv[i] && cv[j]) mma_tile(reinterpret_cast<double(&)[2]>(acc[i][j]), av[i], bv[j]);
-            }
-        } else {
-#pragma unroll
-            for (int kk = 0; kk < kTK; kk += 8) {
-                float av[2][4], bv[4][2];
+        for (int kk = 0; kk < kTK; kk += 8) {   // m16n8k8: FP64 DMMA or TF32
+                T av[2][4], bv[4][2];
 #pragma unroll
                 for (int i = 0; i < 2; ++i) {
                     const int r0 = wm + i * 16 + g;
@@ -653,14 +642,13 @@ __global__ void __launch_bounds__(128) fd_gemm_kernel(const FdProb<T> *__restric
                 for (int i = 0; i < 2; ++i)
 #pragma unroll
                     for (int j = 0; j < 4; ++j)
-                        if (rv[i] && cv[j]) mma_tile(reinterpret_cast<float(&)[4]>(acc[i][j]), av[i], bv[j]);
+                        if (rv[i] && cv[j]) mma_tile(acc[i][j], av[i], bv[j]);
             }
-        }
         if (kt + 1 < nk) stash(buf ^ 1);
         __syncthreads();
     }
-    // accumulator element c of block (i, j): row i*RB + g (+8 for c >= 2 in
-    // FP32), column j*8 + 2 t4 + (c & 1)
+    // accumulator element c of block (i, j): row i*RB + g (+8 for c >= 2),
+    // column j*8 + 2 t4 + (c & 1)
 #pragma unroll
     for (int i = 0; i < MB; ++i)
 #pragma unroll
