@@ -1350,7 +1350,7 @@ int setup_fd(iga_batch *B)
     std::vector<std::vector<double>> pencils(grids.size());   // Kd | Ko | Md | Mo of the free nodes
     struct Half {
         int grid, parity;   // parity -1: the whole pencil (not centrosymmetric)
-        std::vector<double> kd, ko, md, mo, V;
+        std::vector<double> kd, ko, md, mo;
     };
     std::vector<Half> halves;
     for (size_t k = 0; k < grids.size(); ++k) {
@@ -1369,37 +1369,38 @@ int setup_fd(iga_batch *B)
                 if (!h.kd.empty()) halves.push_back(std::move(h));
             }
         } else {
-            halves.push_back(Half{(int)k, -1, Kd, Ko, Md, Mo, {}});
+            halves.push_back(Half{(int)k, -1, Kd, Ko, Md, Mo});
         }
     }
     std::vector<PencilRef> refs;
     for (const Half &h : halves) refs.push_back(PencilRef{(int)h.kd.size(), h.kd.data(), h.ko.data(), h.md.data(), h.mo.data()});
-    std::vector<std::vector<double>> hlam, hvec;
+    std::vector<std::vector<double>> hlam;
+    double *dU = nullptr;            // the half vectors, left on the device
+    std::vector<long long> voff;     // offset of each half's block in dU
     {
-        const int st = pencil_eig_device(B->device, refs, hlam, &hvec);
+        const int st = pencil_eig_device(B->device, refs, hlam, nullptr, &dU, &voff);
         if (st) return st;
-        for (size_t r = 0; r < halves.size(); ++r) halves[r].V = std::move(hvec[r]);
     }
-    // half vectors and eigenvalues of all grids in one upload; the device
-    // expands them into every grid's full eigenvector matrix, its transpose
-    // and (MIXED) the FP32 copies, in one buffer per precision
+    // the half vectors stay on the device where they were computed (plus the
+    // eigenvalues, uploaded in mode order); the device expands them into every
+    // grid's full eigenvector matrix, its transpose and (MIXED) the FP32
+    // copies, in one buffer per precision
     std::vector<long long> lo_of(grids.size(), -1), ue_of(grids.size(), -1), uo_of(grids.size(), -1);
     std::vector<int> hne(grids.size(), 0), hno(grids.size(), 0), fe_of(grids.size(), 0);
     std::vector<char> split(grids.size(), 0);
-    std::vector<double> hU, hL(0);
+    std::vector<double> hL(0);
     for (size_t r = 0; r < halves.size(); ++r) {
         const Half &h = halves[r];
         const int hn = (int)h.kd.size();
         if (h.parity <= 0) {   // even half or whole pencil: first in mode order
-            ue_of[h.grid] = (long long)hU.size();
+            ue_of[h.grid] = voff[r];
             hne[h.grid] = hn;
             fe_of[h.grid] = hn;
             split[h.grid] = h.parity == 0;
         } else {
-            uo_of[h.grid] = (long long)hU.size();
+            uo_of[h.grid] = voff[r];
             hno[h.grid] = hn;
         }
-        hU.insert(hU.end(), h.V.begin(), h.V.end());
     }
     // eigenvalues in mode order per grid: even half, then odd half
     for (size_t k = 0; k < grids.size(); ++k) {
@@ -1409,10 +1410,13 @@ int setup_fd(iga_batch *B)
                 if (halves[r].grid == (int)k && (halves[r].parity == parity || (parity == 0 && halves[r].parity < 0)))
                     hL.insert(hL.end(), hlam[r].begin(), hlam[r].end());
     }
-    double *dU = nullptr, *dL = nullptr;
+    double *dL = nullptr;
     {
         int st;
-        if ((st = bupload(&dU, hU)) || (st = bupload(&dL, hL))) return st;
+        if ((st = bupload(&dL, hL))) {
+            cudaFree(dU);
+            return st;
+        }
     }
     const bool mixed = B->precision == IGA_MIXED;
     // every sub-array starts on a 16-byte boundary (the FP32 padded copies

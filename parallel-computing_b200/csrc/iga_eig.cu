@@ -175,8 +175,13 @@ double pencil_upper_bound(int n, const double *Kd, const double *Ko, const doubl
 }
 
 int pencil_eig_device(int device, const std::vector<PencilRef> &P, std::vector<std::vector<double>> &lam,
-                      std::vector<std::vector<double>> *vec)
+                      std::vector<std::vector<double>> *vec, double **dvec, std::vector<long long> *voff)
 {
+    if (dvec) {
+        *dvec = nullptr;
+        vec = nullptr;
+        if (voff) voff->assign(P.size(), -1);
+    }
     lam.assign(P.size(), {});
     if (vec) vec->assign(P.size(), {});
     std::vector<EigSet> sets;
@@ -239,20 +244,27 @@ int pencil_eig_device(int device, const std::vector<PencilRef> &P, std::vector<s
     eig_bisect_kernel<<<blocks, threads>>>(ds, (int)sets.size(), total, d, d + total, d + 2 * total, d + 3 * total, dl);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
     std::vector<double> hv;
-    if (vec) {
+    if (vec || dvec) {
         if ((e = cudaMalloc((void **)&dw, sizeof(double) * 8 * (size_t)nmax * (size_t)total)) != cudaSuccess ||
             (e = cudaMalloc((void **)&dv, sizeof(double) * (size_t)vtotal)) != cudaSuccess)
             return fail(e);
         eig_vec_kernel<<<blocks, threads>>>(ds, (int)sets.size(), total, nmax, d, d + total, d + 2 * total,
                                             d + 3 * total, dl, dw, dv);
         if ((e = cudaGetLastError()) != cudaSuccess) return fail(e);
-        hv.resize((size_t)vtotal);
-        if ((e = cudaMemcpy(hv.data(), dv, sizeof(double) * (size_t)vtotal, cudaMemcpyDeviceToHost)) != cudaSuccess)
-            return fail(e);
+        if (vec) {
+            hv.resize((size_t)vtotal);
+            if ((e = cudaMemcpy(hv.data(), dv, sizeof(double) * (size_t)vtotal, cudaMemcpyDeviceToHost)) != cudaSuccess)
+                return fail(e);
+        }
     }
     std::vector<double> hl((size_t)total);
     if ((e = cudaMemcpy(hl.data(), dl, sizeof(double) * (size_t)total, cudaMemcpyDeviceToHost)) != cudaSuccess)
         return fail(e);
+    double *keep = nullptr;
+    if (dvec) {   // the caller takes the vectors' buffer
+        keep = dv;
+        dv = nullptr;
+    }
     release();
     size_t q = 0, qv = 0;
     for (size_t k = 0; k < P.size(); ++k) {
@@ -260,6 +272,25 @@ int pencil_eig_device(int device, const std::vector<PencilRef> &P, std::vector<s
         if (n <= 0) continue;
         lam[k].assign(hl.begin() + q, hl.begin() + q + n);
         q += n;
+        if (dvec) {
+            if (voff) (*voff)[k] = (long long)qv;
+            const double ctol = 1e-5 * lam[k][n - 1];
+            bool cluster = false;
+            for (int a = 0; a + 1 < n && !cluster; ++a) cluster = lam[k][a + 1] - lam[k][a] < ctol;
+            if (cluster) {   // as below, then over the device copy
+                std::vector<double> V((size_t)n * n);
+                pencil_eigvecs(n, P[k].Kd, P[k].Ko, P[k].Md, P[k].Mo, lam[k].data(), V.data(), 1);
+                cudaSetDevice(device);
+                e = cudaMemcpy(keep + qv, V.data(), sizeof(double) * V.size(), cudaMemcpyHostToDevice);
+                cudaSetDevice(prev);
+                if (e != cudaSuccess) {
+                    cudaFree(keep);
+                    set_error(std::string("device eigenpairs: ") + cudaGetErrorString(e));
+                    return IGA_ERR_CUDA;
+                }
+            }
+            qv += (size_t)n * n;
+        }
         if (vec) {
             std::vector<double> &V = (*vec)[k];
             V.assign(hv.begin() + qv, hv.begin() + qv + (size_t)n * n);
@@ -273,12 +304,13 @@ int pencil_eig_device(int device, const std::vector<PencilRef> &P, std::vector<s
             if (cluster) pencil_eigvecs(n, P[k].Kd, P[k].Ko, P[k].Md, P[k].Mo, lam[k].data(), V.data(), 1);
         }
     }
+    if (dvec) *dvec = keep;
     return IGA_OK;
 }
 
 int pencil_eigvals_device(int device, const std::vector<PencilRef> &P, std::vector<std::vector<double>> &lam)
 {
-    return pencil_eig_device(device, P, lam, nullptr);
+    return pencil_eig_device(device, P, lam, nullptr, nullptr, nullptr);
 }
 
 }  // namespace iga

@@ -32,8 +32,12 @@ int pencil_eigvals_device(int device, const std::vector<PencilRef> &P, std::vect
 // component i of vector a at a n + i), both computed on `device` (inverse
 // iteration one thread per eigenpair; pencils with coincident eigenvalues
 // get their vectors from pencil_eigvecs on the host).
+// With dvec set, the vectors stay on the device instead: *dvec receives the
+// buffer (all pencils' n x n blocks, the caller frees it) and (*voff)[k] the
+// offset of pencil k's block; vec is then ignored.
 int pencil_eig_device(int device, const std::vector<PencilRef> &P, std::vector<std::vector<double>> &lam,
-                      std::vector<std::vector<double>> *vec);
+                      std::vector<std::vector<double>> *vec, double **dvec = nullptr,
+                      std::vector<long long> *voff = nullptr);
 
 // Parity split of a centrosymmetric pencil (entry i equals entry n-1-i, to
 // rounding): every eigenvector is symmetric (v[i] = v[n-1-i]) or

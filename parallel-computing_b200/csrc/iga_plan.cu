@@ -31,16 +31,32 @@ __global__ void geom_setup_kernel(T *__restrict__ G, const double *__restrict__ 
     const long long total = (long long)g.NSX * g.NSY * g.TY * NQ2 * kSW;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)(t % kSW);
-        long long r = t / kSW;
-        const int qp = (int)(r % NQ2);
-        r /= NQ2;
+        // Point u of the step block, in the order the block is stored, so that
+        // consecutive threads write consecutive words: lane-major layouts
+        // (g_lane_major) [qy][lane = 2c + h][j] (qx = h QH + j), else
+        // [qy][qx][column]. (At p = 3 the column-fastest order scattered the
+        // lane-major writes 12 words apart: 2048^2 G64 + G32 18.4 ms.)
+        const int u = (int)(t % (NQ2 * kSW));
+        long long r = t / (NQ2 * kSW);
+        int c, qx, qy;
+        if (g_lane_major(NQ)) {
+            const int QH = NQ / 2;
+            qy = u / (32 * QH);
+            const int rem = u - qy * 32 * QH, lane = rem / QH, j = rem - lane * QH;
+            c = lane >> 1;
+            qx = (lane & 1) * QH + j;
+        } else {
+            c = u % kSW;
+            const int qp = u / kSW;
+            qx = qp % NQ;
+            qy = qp / NQ;
+        }
+        const int qp = qy * NQ + qx;
         const int s = (int)(r % g.TY);
         r /= g.TY;
         const int gy = (int)(r % g.NSY);
         const int gx = (int)(r / g.NSY);
         const int ex = kSW * gx + c, ey = g.TY * gy + s;
-        const int qx = qp % NQ, qy = qp / NQ;
         double g00 = 0, g01 = 0, g11 = 0;
         if (ex < g.nex && ey < g.ney) {
             double x_xi = 0, x_eta = 0, y_xi = 0, y_eta = 0;
