@@ -4,11 +4,14 @@ Bar: FP64 results within 1e-12 relative (max-norm, relative to the largest
 entry) of the reference's own element code (golden vectors) and of the oracle;
 FP32 within 2e-5 relative. Repeated applies are bitwise identical.
 """
+import ctypes
+import os
+
 import numpy as np
 import pytest
 
-from iga_testlib import (distorted, golden_mesh, load_binding, splitmix_uniform, unit_square_mesh, window,
-                         window_rows)
+from iga_testlib import (REF_CPU_LIB, _p, distorted, golden_mesh, load_binding, splitmix_uniform, unit_square_mesh,
+                         window, window_rows)
 
 pytestmark = pytest.mark.gpu
 TOL64 = 1e-12
@@ -213,3 +216,37 @@ def test_full_size_c2_properties(torch_cuda, ib, orc):
     plan.apply(lin, y)
     torch.cuda.synchronize()
     assert float(y.abs().max()) < 1e-12
+
+
+def test_c1_hundred_matmults_equal_assembled_matvec(torch_cuda, ib, orc, gold):
+    """p = 2, 64x64 elements: 100 matrix-free MatMults (the reference's
+    MatMulMF, matrix_free/mult_mf.cpp:75) on seeded x with the Dirichlet
+    entries zeroed, each against the assembled-matrix MatMult. The reference's own
+    assembled matvec (ref_assembled_matvec of its compiled element code) is
+    the checker where that library is present, the oracle everywhere; the 100
+    applies run back to back on one plan and one stream."""
+    torch = torch_cuda
+    name = "c1"
+    M = golden_mesh(gold, name)
+    Dir = gold[f"{name}_Dir"]
+    plan = ib.Plan(M, IEN=gold[f"{name}_IEN"], ID=gold[f"{name}_ID"], Dir=Dir)
+    nf = plan.nfunc
+    X = np.stack([splitmix_uniform(k, -1.0, 1.0, nf) for k in range(100)])
+    X[:, Dir] = 0.0
+    xd = torch.from_numpy(X).cuda()
+    yd = torch.full_like(xd, float("nan"))
+    for k in range(100):
+        plan.apply(xd[k], yd[k])
+    torch.cuda.synchronize()
+    Y = yd.cpu().numpy()
+    ref_lib = ctypes.CDLL(REF_CPU_LIB) if os.path.exists(REF_CPU_LIB) else None
+    Mr = {k: np.ascontiguousarray(gold[f"{name}_{k}"]) for k in ("CP", "IEN", "ID", "Dir", "C1", "C2", "h1", "h2")}
+    for k in range(100):
+        assert rel(Y[k], orc.apply_mf(M, X[k])) < TOL64
+        if ref_lib is not None:
+            yk = np.zeros(nf)
+            ref_lib.ref_assembled_matvec(M["p"], M["q"], M["nex"], M["ney"], _p(Mr["CP"]), _p(Mr["IEN"]),
+                                         _p(Mr["ID"]), _p(Mr["Dir"]), len(Mr["Dir"]), _p(Mr["C1"]), _p(Mr["C2"]),
+                                         _p(Mr["h1"]), _p(Mr["h2"]), _p(X[k]), _p(yk))
+            assert rel(Y[k], yk) < TOL64
+    plan.close()
