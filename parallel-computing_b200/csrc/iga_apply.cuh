@@ -88,7 +88,7 @@ struct ApplyShape {
     static constexpr int XR = 8;                        // x / CP rows in flight per warp
     static constexpr int XW = 24;                       // >= SW + P, padded
     static constexpr int NBP = tab_nbp(NB, (int)sizeof(T));   // y-table row length
-    static constexpr int TYW = 2 * NQ * NBP;            // one element row's y tables
+    static constexpr int TYW = tab_row_len(NB, NQ, (int)sizeof(T));   // one element row's y tables
     static_assert(GBYTES % 16 == 0, "bulk copy size must be a multiple of 16 bytes");
     static_assert(kSW + P <= XW, "row buffer too narrow");
 };
@@ -264,9 +264,27 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
 
     // This lane's x-direction tables, [kind][j][il][lane] per column strip
     // (apply_txreg: registers, loaded straight from global memory; else the
-    // CTA's shared copy).
-    T txr[TXREG ? 2 : 1][TXREG ? QH : 1][TXREG ? NB : 1];
-    if constexpr (TXREG) {
+    // CTA's shared copy). The FP32 precomputed-geometry kernel at p <= 3
+    // (PAIR) keeps them as (derivative, value) pairs and forms both kinds of
+    // every 1-D contraction with one packed f32x2 FMA (sm_100). Measured
+    // (B200, FP32, cold L2): p=2 2048^2 157 -> 146 us, p=3 181 -> 175 us; at
+    // p = 4, 5 the pairs' registers spill (83 -> 97 us, 144 -> 216 us), and
+    // the on-the-fly kernels were slower too (p=3 1024^2 87 -> 101 us), so
+    // those keep scalar FMAs (reading paired y tables up to p = 4: on-the-fly
+    // p=3 1024^2 87 -> 85 us, p=2 62.4 -> 60.4 us).
+    constexpr bool TPAIR = tab_paired(NB, (int)sizeof(T));
+    constexpr bool PAIR = TPAIR && GEOM == 0 && P <= 3;
+    static_assert(!PAIR || TXREG, "FP32 x tables live in registers");
+    T txr[TXREG && !PAIR ? 2 : 1][TXREG && !PAIR ? QH : 1][TXREG && !PAIR ? NB : 1];
+    float2 tpr[PAIR ? QH : 1][PAIR ? NB : 1];
+    if constexpr (PAIR) {
+        const T *src = a.tabX + (size_t)gx * S::TABX;
+#pragma unroll
+        for (int j = 0; j < QH; ++j)
+#pragma unroll
+            for (int il = 0; il < NB; ++il)
+                tpr[j][il] = make_float2(src[((QH + j) * NB + il) * 32 + lane], src[(j * NB + il) * 32 + lane]);
+    } else if constexpr (TXREG) {
         const T *src = a.tabX + (size_t)gx * S::TABX;
 #pragma unroll
         for (int kind = 0; kind < 2; ++kind)
@@ -282,11 +300,16 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         else return __ldg(txg + ((kind * QH + j) * NB + il) * 32);
     };
 
-    T xs0[NB][QH], xs1[NB][QH];     // x contracted with value / derivative tables, rows ey..ey+P
-    T acc0[NB][QH], acc1[NB][QH];   // y-transposed partial sums for control-point rows ey..ey+P
-    T cs[2][2][GEOM == 1 ? NB : 1][QH];   // GEOM 1: CP coordinates contracted likewise
+    constexpr int NR = PAIR ? 1 : NB;
+    T xs0[NR][QH], xs1[NR][QH];     // x contracted with value / derivative tables, rows ey..ey+P
+    T acc0[NR][QH], acc1[NR][QH];   // y-transposed partial sums for control-point rows ey..ey+P
+    T cs[2][2][GEOM == 1 && !PAIR ? NB : 1][QH];   // GEOM 1: CP coordinates contracted likewise
+    // PAIR: X = (xs1, xs0), A = (acc0, acc1), CX = (cs[0][1], cs[0][0]), CY = (cs[1][1], cs[1][0])
+    float2 X[PAIR ? NB : 1][QH], A[PAIR ? NB : 1][QH];
+    float2 CX[PAIR && GEOM == 1 ? NB : 1][QH], CY[PAIR && GEOM == 1 ? NB : 1][QH];
 
-    auto contract_row = [&](int k, T (&r0)[QH], T (&r1)[QH], int slot_geom) {
+    // x contraction of control-point row k into state row `slot` (0 .. P)
+    auto contract_row = [&](int k, int slot) {
         cp_async_wait<D - 1>();
         __syncwarp();
         const T *src = xr + (k % S::XR) * S::XW;
@@ -304,47 +327,79 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         }
         __syncwarp();
         fetch_row(k + D);
-#pragma unroll
-        for (int j = 0; j < QH; ++j) {
-            T s0 = 0, s1 = 0;
-#pragma unroll
-            for (int il = 0; il < NB; ++il) {
-                s0 = fma(tx(0, j, il), xv[il], s0);
-                s1 = fma(tx(1, j, il), xv[il], s1);
-            }
-            r0[j] = s0;
-            r1[j] = s1;
-        }
-        if constexpr (GEOM == 1) {
+        if constexpr (PAIR) {
 #pragma unroll
             for (int j = 0; j < QH; ++j) {
-                T a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+                float2 s2 = __fmul2_rn(tpr[j][0], make_float2(xv[0], xv[0]));
+#pragma unroll
+                for (int il = 1; il < NB; ++il) s2 = __ffma2_rn(tpr[j][il], make_float2(xv[il], xv[il]), s2);
+                X[slot][j] = s2;
+            }
+            if constexpr (GEOM == 1) {
+#pragma unroll
+                for (int j = 0; j < QH; ++j) {
+                    float2 ax = __fmul2_rn(tpr[j][0], make_float2(px[0], px[0]));
+                    float2 ay = __fmul2_rn(tpr[j][0], make_float2(py[0], py[0]));
+#pragma unroll
+                    for (int il = 1; il < NB; ++il) {
+                        ax = __ffma2_rn(tpr[j][il], make_float2(px[il], px[il]), ax);
+                        ay = __ffma2_rn(tpr[j][il], make_float2(py[il], py[il]), ay);
+                    }
+                    CX[slot][j] = ax;
+                    CY[slot][j] = ay;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < QH; ++j) {
+                T s0 = 0, s1 = 0;
 #pragma unroll
                 for (int il = 0; il < NB; ++il) {
-                    a0 = fma(tx(0, j, il), px[il], a0);
-                    a1 = fma(tx(1, j, il), px[il], a1);
-                    b0 = fma(tx(0, j, il), py[il], b0);
-                    b1 = fma(tx(1, j, il), py[il], b1);
+                    s0 = fma(tx(0, j, il), xv[il], s0);
+                    s1 = fma(tx(1, j, il), xv[il], s1);
                 }
-                cs[0][0][slot_geom][j] = a0;
-                cs[0][1][slot_geom][j] = a1;
-                cs[1][0][slot_geom][j] = b0;
-                cs[1][1][slot_geom][j] = b1;
+                xs0[slot][j] = s0;
+                xs1[slot][j] = s1;
+            }
+            if constexpr (GEOM == 1) {
+#pragma unroll
+                for (int j = 0; j < QH; ++j) {
+                    T a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+#pragma unroll
+                    for (int il = 0; il < NB; ++il) {
+                        a0 = fma(tx(0, j, il), px[il], a0);
+                        a1 = fma(tx(1, j, il), px[il], a1);
+                        b0 = fma(tx(0, j, il), py[il], b0);
+                        b1 = fma(tx(1, j, il), py[il], b1);
+                    }
+                    cs[0][0][slot][j] = a0;
+                    cs[0][1][slot][j] = a1;
+                    cs[1][0][slot][j] = b0;
+                    cs[1][1][slot][j] = b1;
+                }
             }
         }
     };
 
     auto store = [&](int R, int C, T v) { store_point<T>(g, x, y, a.ID, a.sign, a.bc, R, C, v); };
     T *frame = a.frame + (size_t)(gx * g.NSY + gy) * g.FS;
-    auto write_row = [&](int lr, const T (&r0)[QH], const T (&r1)[QH]) {
+    // finishes control-point row ey0 + lr from state row 0 of the partial sums
+    auto write_row = [&](int lr) {
         T out[NB];
 #pragma unroll
         for (int il = 0; il < NB; ++il) {
             T s = 0;
+            if constexpr (PAIR) {   // the derivative-table and value-table sums, then their total
+                float2 s2 = __fmul2_rn(tpr[0][il], A[0][0]);
 #pragma unroll
-            for (int j = 0; j < QH; ++j) {
-                s = fma(tx(1, j, il), r0[j], s);
-                s = fma(tx(0, j, il), r1[j], s);
+                for (int j = 1; j < QH; ++j) s2 = __ffma2_rn(tpr[j][il], A[0][j], s2);
+                s = s2.x + s2.y;
+            } else {
+#pragma unroll
+                for (int j = 0; j < QH; ++j) {
+                    s = fma(tx(1, j, il), acc0[0][j], s);
+                    s = fma(tx(0, j, il), acc1[0][j], s);
+                }
             }
             out[il] = s + __shfl_xor_sync(0xffffffffu, s, 1);   // both qx halves, same order on both lanes
         }
@@ -375,17 +430,56 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
 
     // Prologue: rows ey0 .. ey0+P-1.
 #pragma unroll
-    for (int r = 0; r < P; ++r) contract_row(r, xs0[r], xs1[r], GEOM == 1 ? r : 0);
+    for (int r = 0; r < P; ++r) contract_row(r, r);
 #pragma unroll
     for (int r = 0; r < NB; ++r)
 #pragma unroll
-        for (int q = 0; q < QH; ++q) acc0[r][q] = acc1[r][q] = 0;
+        for (int q = 0; q < QH; ++q) {
+            if constexpr (PAIR) A[r][q] = make_float2(0.f, 0.f);
+            else acc0[r][q] = acc1[r][q] = 0;
+        }
+    // state rows r+1 -> r (the next element row); the partial sums of row P restart
+    auto shift_rows = [&](bool inputs) {
+#pragma unroll
+        for (int r = 0; r < P; ++r)
+#pragma unroll
+            for (int q = 0; q < QH; ++q) {
+                if constexpr (PAIR) {
+                    A[r][q] = A[r + 1][q];
+                    if (inputs) {
+                        X[r][q] = X[r + 1][q];
+                        if constexpr (GEOM == 1) {
+                            CX[r][q] = CX[r + 1][q];
+                            CY[r][q] = CY[r + 1][q];
+                        }
+                    }
+                } else {
+                    acc0[r][q] = acc0[r + 1][q];
+                    acc1[r][q] = acc1[r + 1][q];
+                    if (inputs) {
+                        xs0[r][q] = xs0[r + 1][q];
+                        xs1[r][q] = xs1[r + 1][q];
+                        if constexpr (GEOM == 1) {
+                            cs[0][0][r][q] = cs[0][0][r + 1][q];
+                            cs[0][1][r][q] = cs[0][1][r + 1][q];
+                            cs[1][0][r][q] = cs[1][0][r + 1][q];
+                            cs[1][1][r][q] = cs[1][1][r + 1][q];
+                        }
+                    }
+                }
+            }
+#pragma unroll
+        for (int q = 0; q < QH; ++q) {
+            if constexpr (PAIR) A[P][q] = make_float2(0.f, 0.f);
+            else acc0[P][q] = acc1[P][q] = 0;
+        }
+    };
 
     bool ok = true;
     int failed_step = 0;
     for (int s = 0; s < nsteps; ++s) {
         const int ey = ey0 + s;
-        contract_row(s + P, xs0[P], xs1[P], GEOM == 1 ? P : 0);
+        contract_row(s + P, P);
         const int slot = s % NST;
         const T *Gst = Gs + (size_t)slot * S::GE;
         if (GEOM == 0) {
@@ -398,22 +492,49 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         const T *ty = yr + ((s + P) % S::XR) * S::TYW;   // landed with x row s + P
         constexpr bool MID = mid_shared(NQ, (int)sizeof(T));
         constexpr int QJ = MID ? QH - 1 : QH;   // slots of this lane half's own columns
-        // y tables (value n2, derivative d2) of quadrature row qy
-        auto load_tab = [&](int qy, T (&n2)[NB], T (&d2)[NB]) {
-            // rows of NBP entries, 16-byte aligned in the ring: vector loads
-            constexpr int V = 16 / sizeof(T), NBP = S::NBP;
-            using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
-            const VT *va = reinterpret_cast<const VT *>(ty + qy * NBP);
-            const VT *vb = reinterpret_cast<const VT *>(ty + (NQ + qy) * NBP);
+        // y tables of quadrature row qy: value n2 and derivative d2, or their
+        // pairs nd (PAIR)
+        struct YRow {
+            T n2[PAIR ? 1 : NB], d2[PAIR ? 1 : NB];
+            float2 nd[PAIR ? NB : 1];
+        };
+        auto load_tab = [&](int qy, YRow &t) {
+            if constexpr (PAIR) {   // rows of NB pairs padded to 16 bytes: two pairs per vector load
+                const float4 *v = reinterpret_cast<const float4 *>(ty + qy * tab_nbp2(NB));
 #pragma unroll
-            for (int v = 0; v < NBP / V; ++v) {
-                const VT ua = va[v], ub = vb[v];
-                const T *pa = reinterpret_cast<const T *>(&ua), *pb = reinterpret_cast<const T *>(&ub);
+                for (int u = 0; 2 * u < NB; ++u) {
+                    const float4 q = v[u];
+                    t.nd[2 * u] = make_float2(q.x, q.y);
+                    if (2 * u + 1 < NB) t.nd[2 * u + 1] = make_float2(q.z, q.w);
+                }
+            } else if constexpr (TPAIR) {   // the same rows, split into the two kinds
+                const float4 *v = reinterpret_cast<const float4 *>(ty + qy * tab_nbp2(NB));
 #pragma unroll
-                for (int e = 0; e < V; ++e) {
-                    if (v * V + e < NB) {
-                        n2[v * V + e] = pa[e];
-                        d2[v * V + e] = pb[e];
+                for (int u = 0; 2 * u < NB; ++u) {
+                    const float4 q = v[u];
+                    t.n2[2 * u] = q.x;
+                    t.d2[2 * u] = q.y;
+                    if (2 * u + 1 < NB) {
+                        t.n2[2 * u + 1] = q.z;
+                        t.d2[2 * u + 1] = q.w;
+                    }
+                }
+            } else {
+                // rows of NBP entries, 16-byte aligned in the ring: vector loads
+                constexpr int V = 16 / sizeof(T), NBP = S::NBP;
+                using VT = typename std::conditional<sizeof(T) == 8, double2, float4>::type;
+                const VT *va = reinterpret_cast<const VT *>(ty + qy * NBP);
+                const VT *vb = reinterpret_cast<const VT *>(ty + (NQ + qy) * NBP);
+#pragma unroll
+                for (int v = 0; v < NBP / V; ++v) {
+                    const VT ua = va[v], ub = vb[v];
+                    const T *pa = reinterpret_cast<const T *>(&ua), *pb = reinterpret_cast<const T *>(&ub);
+#pragma unroll
+                    for (int e = 0; e < V; ++e) {
+                        if (v * V + e < NB) {
+                            t.n2[v * V + e] = pa[e];
+                            t.d2[v * V + e] = pb[e];
+                        }
                     }
                 }
             }
@@ -421,12 +542,20 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         // quadrature point (qy, qx) in slot j: gradient of u, times G, back
         // onto the slot's y-transposed partial sums (valid false: adds zero)
         // gv: this lane's G values of row qy (lane-major G), else read here
-        auto qpoint = [&](int qy, int qx, int j, bool valid, const T (&n2)[NB], const T (&d2)[NB], const T *gv) {
+        auto qpoint = [&](int qy, int qx, int j, bool valid, const YRow &t, const T *gv) {
             T uxi = 0, ueta = 0;
+            if constexpr (PAIR) {   // (n2 . xs1, d2 . xs0) together
+                float2 u2 = __fmul2_rn(t.nd[0], X[0][j]);
 #pragma unroll
-            for (int jl = 0; jl < NB; ++jl) {
-                uxi = fma(n2[jl], xs1[jl][j], uxi);
-                ueta = fma(d2[jl], xs0[jl][j], ueta);
+                for (int jl = 1; jl < NB; ++jl) u2 = __ffma2_rn(t.nd[jl], X[jl][j], u2);
+                uxi = u2.x;
+                ueta = u2.y;
+            } else {
+#pragma unroll
+                for (int jl = 0; jl < NB; ++jl) {
+                    uxi = fma(t.n2[jl], xs1[jl][j], uxi);
+                    ueta = fma(t.d2[jl], xs0[jl][j], ueta);
+                }
             }
             T g00 = 0, g01 = 0, g11 = 0;
             T vxi, veta;
@@ -454,12 +583,25 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
                 }
             } else {
                 T x_xi = 0, x_eta = 0, y_xi = 0, y_eta = 0;
+                if constexpr (PAIR) {
+                    float2 cx = __fmul2_rn(t.nd[0], CX[0][j]), cy = __fmul2_rn(t.nd[0], CY[0][j]);
 #pragma unroll
-                for (int jl = 0; jl < NB; ++jl) {
-                    x_xi = fma(n2[jl], cs[0][1][jl][j], x_xi);
-                    x_eta = fma(d2[jl], cs[0][0][jl][j], x_eta);
-                    y_xi = fma(n2[jl], cs[1][1][jl][j], y_xi);
-                    y_eta = fma(d2[jl], cs[1][0][jl][j], y_eta);
+                    for (int jl = 1; jl < NB; ++jl) {
+                        cx = __ffma2_rn(t.nd[jl], CX[jl][j], cx);
+                        cy = __ffma2_rn(t.nd[jl], CY[jl][j], cy);
+                    }
+                    x_xi = cx.x;
+                    x_eta = cx.y;
+                    y_xi = cy.x;
+                    y_eta = cy.y;
+                } else {
+#pragma unroll
+                    for (int jl = 0; jl < NB; ++jl) {
+                        x_xi = fma(t.n2[jl], cs[0][1][jl][j], x_xi);
+                        x_eta = fma(t.d2[jl], cs[0][0][jl][j], x_eta);
+                        y_xi = fma(t.n2[jl], cs[1][1][jl][j], y_xi);
+                        y_eta = fma(t.d2[jl], cs[1][0][jl][j], y_eta);
+                    }
                 }
                 // G grad u = f adj(J) adj(J)^T grad u with adj(J) = [[y_eta,
                 // -x_eta], [-y_xi, x_xi]] and f = w kappa / det J: ten
@@ -479,17 +621,23 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
                 vxi = fma(g00, uxi, g01 * ueta);
                 veta = fma(g01, uxi, g11 * ueta);
             }
+            if constexpr (PAIR) {   // (acc0 += n2 vxi, acc1 += d2 veta) together
+                const float2 v2 = make_float2(vxi, veta);
 #pragma unroll
-            for (int jl = 0; jl < NB; ++jl) {
-                acc0[jl][j] = fma(n2[jl], vxi, acc0[jl][j]);
-                acc1[jl][j] = fma(d2[jl], veta, acc1[jl][j]);
+                for (int jl = 0; jl < NB; ++jl) A[jl][j] = __ffma2_rn(t.nd[jl], v2, A[jl][j]);
+            } else {
+#pragma unroll
+                for (int jl = 0; jl < NB; ++jl) {
+                    acc0[jl][j] = fma(t.n2[jl], vxi, acc0[jl][j]);
+                    acc1[jl][j] = fma(t.d2[jl], veta, acc1[jl][j]);
+                }
             }
         };
 
 #pragma unroll
         for (int qy = 0; qy < NQ; ++qy) {
-            T n2[NB], d2[NB];
-            load_tab(qy, n2, d2);
+            YRow t;
+            load_tab(qy, t);
             // this lane's G values of row qy for its own columns: 3 QJ contiguous
             // values (lane-major G rows), widest aligned loads
             constexpr int GVN = (g_lane_major(NQ) || g_mid_lane_major(NQ, (int)sizeof(T))) ? 3 * QJ : 1;
@@ -510,16 +658,16 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
 #pragma unroll
             for (int j = 0; j < QJ; ++j) {
                 const int qx = h * QH + j;   // only h = 1's last slot can lie past NQ
-                qpoint(qy, qx, j, (NQ % 2 == 0 || j + 1 < QH) || qx < NQ, n2, d2, gv);
+                qpoint(qy, qx, j, (NQ % 2 == 0 || j + 1 < QH) || qx < NQ, t, gv);
             }
         }
         if constexpr (MID) {   // middle column QH - 1: half h takes rows qy = 2 t + h
 #pragma unroll
-            for (int t = 0; t < QH; ++t) {
-                const int qy = min(2 * t + h, NQ - 1);
-                T n2[NB], d2[NB];
-                load_tab(qy, n2, d2);
-                qpoint(qy, QH - 1, QH - 1, 2 * t + h < NQ, n2, d2, nullptr);
+            for (int tq = 0; tq < QH; ++tq) {
+                const int qy = min(2 * tq + h, NQ - 1);
+                YRow t;
+                load_tab(qy, t);
+                qpoint(qy, QH - 1, QH - 1, 2 * tq + h < NQ, t, nullptr);
             }
         }
         if (GEOM == 0) {
@@ -530,24 +678,8 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
                 bulk_g2s(Gs + (size_t)slot * S::GE, Gstrip + (size_t)(s + NST) * S::GE, S::GBYTES, &wbar[slot]);
             }
         }
-        write_row(s, acc0[0], acc1[0]);
-#pragma unroll
-        for (int r = 0; r < P; ++r)
-#pragma unroll
-            for (int q = 0; q < QH; ++q) {
-                xs0[r][q] = xs0[r + 1][q];
-                xs1[r][q] = xs1[r + 1][q];
-                acc0[r][q] = acc0[r + 1][q];
-                acc1[r][q] = acc1[r + 1][q];
-                if constexpr (GEOM == 1) {
-                    cs[0][0][r][q] = cs[0][0][r + 1][q];
-                    cs[0][1][r][q] = cs[0][1][r + 1][q];
-                    cs[1][0][r][q] = cs[1][0][r + 1][q];
-                    cs[1][1][r][q] = cs[1][1][r + 1][q];
-                }
-            }
-#pragma unroll
-        for (int q = 0; q < QH; ++q) acc0[P][q] = acc1[P][q] = 0;
+        write_row(s);
+        shift_rows(true);
     }
     if (!ok) {
         if (lane == 0) atomicExch(a.err, 8 /* IGA_ERR_TIMEOUT */);
@@ -562,14 +694,8 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     // Rows above the last element row: partial sums for rows ey_last+1 .. ey_last+P.
 #pragma unroll
     for (int r = 0; r < P; ++r) {
-        write_row(nsteps + r, acc0[0], acc1[0]);
-#pragma unroll
-        for (int rr = 0; rr < P; ++rr)
-#pragma unroll
-            for (int q = 0; q < QH; ++q) {
-                acc0[rr][q] = acc0[rr + 1][q];
-                acc1[rr][q] = acc1[rr + 1][q];
-            }
+        write_row(nsteps + r);
+        shift_rows(false);
     }
     cp_async_wait<0>();
 }

@@ -140,6 +140,24 @@ __host__ __device__ constexpr int tab_nbp(int NB, int esz)
     return (NB * esz) % 16 == 0 ? NB : ((NB * esz + 15) / 16 * 16) / esz;
 }
 
+// FP32 y tables up to p = 4 hold (value, derivative) pairs side by side, one
+// row of NB pairs per qy padded to whole 16-byte words: the operands of packed
+// f32x2 FMAs where the apply kernel uses them, and no more vector loads per
+// row than two padded rows elsewhere (p=4 unchanged; at p = 5 the paired rows
+// were slower, 144 -> 157 us at 1024^2); the others keep separate rows per
+// kind. Entries of one element row: tab_row_len(NB, NQ, esz).
+__host__ __device__ constexpr bool tab_paired(int NB, int esz) { return esz == 4 && NB <= 5; }
+__host__ __device__ constexpr int tab_nbp2(int NB) { return (2 * NB * 4 + 15) / 16 * 16 / 4; }
+__host__ __device__ constexpr int tab_row_len(int NB, int NQ, int esz)
+{
+    return tab_paired(NB, esz) ? NQ * tab_nbp2(NB) : 2 * NQ * tab_nbp(NB, esz);
+}
+// Offset of entry (kind, qy, jl) within an element row of y tables.
+__host__ __device__ constexpr int tab_y_index(int NB, int NQ, int esz, int kind, int qy, int jl)
+{
+    return tab_paired(NB, esz) ? qy * tab_nbp2(NB) + 2 * jl + kind : (kind * NQ + qy) * tab_nbp(NB, esz) + jl;
+}
+
 // ---------------------------------------------------------------- strips
 // Element columns per warp strip (two lanes per element column).
 constexpr int kSW = 16;

@@ -448,13 +448,13 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
                         if (ex < P.nex && qx < NQ) v = (kind ? tx.der : tx.val)[((size_t)ex * NQ + qx) * NB + il];
                         hx[((((size_t)gx * 2 + kind) * QH + j) * NB + il) * 32 + lane] = (T)v;
                     }
-    const int NBP = tab_nbp(NB, (int)sizeof(T));   // y-table rows padded to 16 bytes
-    std::vector<T> hy((size_t)P.ney * 2 * NQ * NBP, T(0));
+    const int TYW = tab_row_len(NB, NQ, (int)sizeof(T));   // rows padded to 16 bytes
+    std::vector<T> hy((size_t)P.ney * TYW, T(0));
     for (int ey = 0; ey < P.ney; ++ey)
         for (int kind = 0; kind < 2; ++kind)
             for (int qy = 0; qy < NQ; ++qy)
                 for (int jl = 0; jl < NB; ++jl)
-                    hy[(((size_t)ey * 2 + kind) * NQ + qy) * NBP + jl] =
+                    hy[(size_t)ey * TYW + tab_y_index(NB, NQ, (int)sizeof(T), kind, qy, jl)] =
                         (T)(kind ? ty.der : ty.val)[((size_t)ey * NQ + qy) * NB + jl];
     int st;
     if ((st = upload((T **)&op.tabX, hx.data(), hx.size() * sizeof(T)))) return st;
