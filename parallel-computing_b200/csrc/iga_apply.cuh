@@ -260,7 +260,6 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
         cp_async_commit();
     };
     constexpr int D = S::XR - 1;
-    for (int k = 0; k < D; ++k) fetch_row(k);
 
     // This lane's x-direction tables, [kind][j][il][lane] per column strip
     // (apply_txreg: registers, loaded straight from global memory; else the
@@ -295,10 +294,15 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     }
     const T *txg = a.tabX + (size_t)gx * S::TABX + lane;
     auto tx = [&](int kind, int j, int il) -> T {
-        if constexpr (TXREG) return txr[kind][j][il];
+        if constexpr (PAIR) return kind ? tpr[j][il].x : tpr[j][il].y;
+        else if constexpr (TXREG) return txr[kind][j][il];
         else if constexpr (apply_txshared<P, T, GEOM>()) return tabXs[((kind * QH + j) * NB + il) * 32 + lane];
         else return __ldg(txg + ((kind * QH + j) * NB + il) * 32);
     };
+    // Everything above reads only the plan's constant tables and geometry;
+    // x (an earlier grid's output) and every write come after the wait.
+    pdl_wait();
+    for (int k = 0; k < D; ++k) fetch_row(k);
 
     constexpr int NR = PAIR ? 1 : NB;
     T xs0[NR][QH], xs1[NR][QH];     // x contracted with value / derivative tables, rows ey..ey+P
@@ -708,7 +712,7 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
 template <int P, typename T, int GEOM, int NST>
 __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kernel(ApplyParams<T> a)
 {
-    pdl_begin();
+    pdl_launch();   // apply_tile waits for the preceding grid once its constant operands are in flight
     const int rows = min(a.gyn, a.g.NSY - a.gy0);   // strip rows of the window
     if constexpr (!apply_txshared<P, T, GEOM>()) {
         const int sid = blockIdx.x * blockDim.y + threadIdx.y;

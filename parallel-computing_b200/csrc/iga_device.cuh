@@ -23,6 +23,14 @@ __device__ __forceinline__ void pdl_begin()
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// The two halves of pdl_begin() for kernels that first fetch operands no
+// earlier grid writes (tables, geometry, eigenvectors) and set up shared
+// memory and tensor memory while the preceding grid drains: pdl_launch() at
+// the start, pdl_wait() before the first read of data an earlier grid
+// produced and before the first global write. pdl_wait() is per thread.
+__device__ __forceinline__ void pdl_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Host side: while pdl_capture() is true on this thread (the solver's loop
 // capture), launch_k() launches with a programmatic stream serialisation
 // attribute, so that stream capture records programmatic edges; otherwise

@@ -108,7 +108,7 @@ template <bool AMN, bool BMN, int OUT, int BN>
 __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ CUtensorMap ta,
                                                         const __grid_constant__ CUtensorMap tb, int K, int Mst, int Nst,
                                                         float *__restrict__ C, int ldc, int *__restrict__ err,
-                                                        GemmScatter sc, GemmSplit split)
+                                                        GemmScatter sc, GemmSplit split, int const_op)
 {
     constexpr int kGTileB = BN * kGK * 4;
     constexpr int kGS = gemm_tf32_stages<BN>();
@@ -120,7 +120,10 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
     uint64_t *empty = full + kGS, *done = empty + kGS;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 1);
     int *cnt = reinterpret_cast<int *>(tslot + 1);   // [0] slices loaded, [1] slices consumed, [2] failure
-    pdl_begin();
+    // Tensor memory, barriers and (const_op) the first stages of the operand
+    // no earlier grid writes are set up before the wait for the preceding
+    // grid; the other operand's loads and every global write come after it.
+    pdl_launch();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const TileRange tr = tile_range(split, blockIdx.x, blockIdx.y, kGM, BN, K, Mst, Nst);
     const int m0 = tr.m0, n0 = tr.n0, klo = tr.klo;
@@ -145,6 +148,30 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
     const uint32_t tmem = *tslot;
 
     if (warp == 0 && lane == 0) {   // copy thread
+        auto load_a = [&](int s, int k0) {
+            unsigned char *a = As + s * kGTileA;
+            if (AMN) {
+                for (int j = 0; j < kGM / 32; ++j) tma_load_2d(a + j * 4096, &ta, m0 + 32 * j, k0, &full[s]);
+            } else {
+                tma_load_2d(a, &ta, k0, m0, &full[s]);
+            }
+        };
+        auto load_b = [&](int s, int k0) {
+            unsigned char *b = Bs + s * kGTileB;
+            if (BMN) {
+                for (int j = 0; j < BN / 32; ++j) tma_load_2d(b + j * 4096, &tb, n0 + 32 * j, k0, &full[s]);
+            } else {
+                tma_load_2d(b, &tb, k0, n0, &full[s]);
+            }
+        };
+        // stages 0 .. npre-1: the constant operand now, the other after the wait
+        const int npre = const_op ? min(nk, kGS) : 0;
+        for (int kt = 0; kt < npre; ++kt) {
+            mbar_arrive_expect_tx(&full[kt], kGTileA + kGTileB);
+            if (const_op == 1) load_a(kt, klo + kt * kGK);
+            else load_b(kt, klo + kt * kGK);
+        }
+        pdl_wait();
         int kt = 0;
         for (; kt < nk; ++kt) {
             const int s = kt % kGS;
@@ -152,19 +179,10 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
                 cnt[2] = 1;
                 break;
             }
-            mbar_arrive_expect_tx(&full[s], kGTileA + kGTileB);
             const int k0 = klo + kt * kGK;
-            unsigned char *a = As + s * kGTileA, *b = Bs + s * kGTileB;
-            if (AMN) {
-                for (int j = 0; j < kGM / 32; ++j) tma_load_2d(a + j * 4096, &ta, m0 + 32 * j, k0, &full[s]);
-            } else {
-                tma_load_2d(a, &ta, k0, m0, &full[s]);
-            }
-            if (BMN) {
-                for (int j = 0; j < BN / 32; ++j) tma_load_2d(b + j * 4096, &tb, n0 + 32 * j, k0, &full[s]);
-            } else {
-                tma_load_2d(b, &tb, k0, n0, &full[s]);
-            }
+            if (kt >= npre) mbar_arrive_expect_tx(&full[s], kGTileA + kGTileB);
+            if (kt >= npre || const_op != 1) load_a(s, k0);
+            if (kt >= npre || const_op != 2) load_b(s, k0);
         }
         cnt[0] = kt;
     } else if (warp == 1 && lane == 0) {   // MMA thread
@@ -194,6 +212,7 @@ __global__ void __launch_bounds__(128) gemm_tf32_kernel(const __grid_constant__ 
     }
     __syncwarp();
     const bool ok = !__syncthreads_or(!mbar_wait_bounded(done, 0));   // uniform over the CTA
+    pdl_wait();   // (long since passed by the copy thread) before this thread's global reads and writes
     const bool failed = !ok || cnt[2] || cnt[1] < nk;
     if (!failed) {
         umma::fence_after_sync();
@@ -316,7 +335,7 @@ int launch_tf32_t(const GemmTF32 &g, cudaStream_t s, int *err, const GemmScatter
     const dim3 grid(tiles_along(g.Mst, kGM, g.split.on_n ? 0 : g.split.kb),
                     tiles_along(g.Nst, BN, g.split.on_n ? g.split.kb : 0));
     return launch_k(gemm_tf32_kernel<AMN, BMN, OUT, BN>, grid, dim3(128), smem, s, g.ta, g.tb, g.K, g.Mst, g.Nst, g.C,
-                    g.ldc, err, sc, g.split) == cudaSuccess
+                    g.ldc, err, sc, g.split, g.const_op) == cudaSuccess
                ? IGA_OK
                : IGA_ERR_CUDA;
 }

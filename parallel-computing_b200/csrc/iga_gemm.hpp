@@ -40,6 +40,10 @@ struct GemmTF32 {
     int ldc = 0;
     int bn = 128;                  // output tile width (128, or 64 for small products)
     GemmSplit split;               // block-diagonal operand, if any
+    // 1 (A) or 2 (B): an operand that no kernel launched on the same stream
+    // writes (the eigenvectors), whose first tiles a launch with a programmatic
+    // dependency may fetch before the preceding grid has finished; 0: none
+    int const_op = 0;
     bool ready = false;
 };
 

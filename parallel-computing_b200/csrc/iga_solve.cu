@@ -611,7 +611,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32)
 fd_tri_kernel(T *__restrict__ W, const T *__restrict__ Lf, const T *__restrict__ Dv, int nx, int ny, int nyp, int seg,
               DevScalars *sc)
 {
-    pdl_begin();
+    pdl_launch();
     extern __shared__ __align__(16) unsigned char tri_smem[];
     __shared__ uint64_t bar[kTriMaxWarps];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -626,18 +626,29 @@ fd_tri_kernel(T *__restrict__ W, const T *__restrict__ Lf, const T *__restrict__
     }
     uint32_t phase = 0;
     const int b0 = lane * seg, b1 = min(b0 + seg, ny);
-    for (int a = blockIdx.x * nw + wid; a < nx; a += gridDim.x * nw) {
+    const uint32_t bytes = (uint32_t)nyp * (uint32_t)sizeof(T);
+    const int a0 = blockIdx.x * nw + wid;
+    // the first mode's factors (constant) are requested before the wait for
+    // the preceding grid, its column of W after it
+    if (STAGED && lane == 0 && a0 < nx) {
+        mbar_arrive_expect_tx(&bar[wid], 3u * bytes);
+        bulk_g2s(lb, Lf + (size_t)a0 * nyp, bytes, &bar[wid]);
+        bulk_g2s(db, Dv + (size_t)a0 * nyp, bytes, &bar[wid]);
+    }
+    pdl_wait();
+    for (int a = a0; a < nx; a += gridDim.x * nw) {
         T *wg = W + (size_t)a * nyp;
         const T *lg = Lf + (size_t)a * nyp, *dg = Dv + (size_t)a * nyp;
         T *wp;
         const T *lp, *dp;
         if constexpr (STAGED) {
             if (lane == 0) {
-                const uint32_t bytes = (uint32_t)nyp * (uint32_t)sizeof(T);
-                mbar_arrive_expect_tx(&bar[wid], 3u * bytes);
+                if (a != a0) {
+                    mbar_arrive_expect_tx(&bar[wid], 3u * bytes);
+                    bulk_g2s(lb, lg, bytes, &bar[wid]);
+                    bulk_g2s(db, dg, bytes, &bar[wid]);
+                }
                 bulk_g2s(wb, wg, bytes, &bar[wid]);
-                bulk_g2s(lb, lg, bytes, &bar[wid]);
-                bulk_g2s(db, dg, bytes, &bar[wid]);
             }
             if (!mbar_wait_bounded(&bar[wid], phase)) {
                 if (lane == 0) sc->err = 1;
@@ -1209,8 +1220,11 @@ static int prepare_gemms(PrecState<float> &ps)
     int st = gemm_tf32_prepare(ps.g1, GemmOperand{ps.Vx, nxp, false}, GemmOperand{ps.W2, nxp, false}, ps.W1, nyp, nxp,
                                nyp, nxp, nxp, nyp, GemmSplit{ps.kb, false});
     if (st) return st;
-    return gemm_tf32_prepare(ps.g2, GemmOperand{ps.W1, nyp, true}, GemmOperand{ps.Vx, nxp, true}, ps.W2, nxp, nyp, nxp,
-                             nxp, nyp, nxp, GemmSplit{ps.kb, true});
+    ps.g1.const_op = 1;   // Vx
+    st = gemm_tf32_prepare(ps.g2, GemmOperand{ps.W1, nyp, true}, GemmOperand{ps.Vx, nxp, true}, ps.W2, nxp, nyp, nxp,
+                           nxp, nyp, nxp, GemmSplit{ps.kb, true});
+    ps.g2.const_op = 2;   // Vx
+    return st;
 }
 
 template <typename T>
