@@ -9,6 +9,7 @@
 #include <mutex>
 #include <string>
 #include <tuple>
+#include <thread>
 #include <vector>
 
 #include "iga_apply.cuh"
@@ -21,16 +22,20 @@ namespace iga {
 // Precomputed geometry (the mult_sf path): G = w kappa det(J) J^-1 J^-T at
 // every quadrature point, in the order apply_kernel streams it:
 // [strip][row][qy][qx][3][column of the strip]. Padding elements get G = 0.
-template <typename T>
-__global__ void geom_setup_kernel(T *__restrict__ G, const double *__restrict__ tabX64,
-                                  const double *__restrict__ tabY64, const double *__restrict__ CP,
-                                  const double *__restrict__ qw, const double *__restrict__ kappa, StripGrid g,
-                                  int *err)
+// Quadrature points (padding included) of a strip grid's G.
+__host__ __device__ __forceinline__ long long geom_points(const StripGrid &g)
+{
+    return (long long)g.NSX * g.NSY * g.TY * (g.P + 1) * (g.P + 1) * kSW;
+}
+
+// G at point t of grid g, into G64 and / or G32 (either may be null).
+__device__ __forceinline__ void geom_point(double *__restrict__ G64, float *__restrict__ G32,
+                                           const double *__restrict__ tabX64, const double *__restrict__ tabY64,
+                                           const double *__restrict__ CP, const double *__restrict__ qw,
+                                           const double *__restrict__ kappa, const StripGrid &g, int *err, long long t)
 {
     const int P = g.P, NB = P + 1, NQ = P + 1, NQ2 = NQ * NQ;
-    const long long total = (long long)g.NSX * g.NSY * g.TY * NQ2 * kSW;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
-         t += (long long)gridDim.x * blockDim.x) {
+    {
         // Point u of the step block, in the order the block is stored, so that
         // consecutive threads write consecutive words: lane-major layouts
         // (g_lane_major) [qy][lane = 2c + h][j] (qx = h QH + j), else
@@ -83,10 +88,61 @@ __global__ void geom_setup_kernel(T *__restrict__ G, const double *__restrict__ 
             g01 = -f * (x_xi * x_eta + y_xi * y_eta);
             g11 = f * (x_xi * x_xi + y_xi * y_xi);
         }
-        T *Gs = G + (((size_t)gx * g.NSY + gy) * g.TY + s) * NQ2 * 3 * kSW;
-        Gs[g_index(NQ, (int)sizeof(T), qy, qx, 0, c)] = (T)g00;
-        Gs[g_index(NQ, (int)sizeof(T), qy, qx, 1, c)] = (T)g01;
-        Gs[g_index(NQ, (int)sizeof(T), qy, qx, 2, c)] = (T)g11;
+        const size_t base = (((size_t)gx * g.NSY + gy) * g.TY + s) * NQ2 * 3 * kSW;
+        if (G64) {
+            double *Gs = G64 + base;
+            Gs[g_index(NQ, 8, qy, qx, 0, c)] = g00;
+            Gs[g_index(NQ, 8, qy, qx, 1, c)] = g01;
+            Gs[g_index(NQ, 8, qy, qx, 2, c)] = g11;
+        }
+        if (G32) {
+            float *Gs = G32 + base;
+            Gs[g_index(NQ, 4, qy, qx, 0, c)] = (float)g00;
+            Gs[g_index(NQ, 4, qy, qx, 1, c)] = (float)g01;
+            Gs[g_index(NQ, 4, qy, qx, 2, c)] = (float)g11;
+        }
+    }
+}
+
+template <typename T>
+__global__ void geom_setup_kernel(T *__restrict__ G, const double *__restrict__ tabX64,
+                                  const double *__restrict__ tabY64, const double *__restrict__ CP,
+                                  const double *__restrict__ qw, const double *__restrict__ kappa, StripGrid g,
+                                  int *err)
+{
+    const long long total = geom_points(g);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x)
+        geom_point(sizeof(T) == 8 ? (double *)(void *)G : nullptr, sizeof(T) == 4 ? (float *)(void *)G : nullptr,
+                   tabX64, tabY64, CP, qw, kappa, g, err, t);
+}
+
+// Every job of a batch's plans in one launch: the CTA finds the job of the
+// first point of its 256-point block once (jobs hold at least 2 x 32 x 9 x
+// 16 points, so a block straddles at most one boundary) and each thread
+// steps to the next job if its point lies past that one's start.
+__global__ void geom_jobs_kernel(const GeomJob *__restrict__ jobs, int njobs, long long total)
+{
+    __shared__ int js;
+    for (long long b0 = (long long)blockIdx.x * blockDim.x; b0 < total; b0 += (long long)gridDim.x * blockDim.x) {
+        if (threadIdx.x == 0) {
+            int lo = 0, hi = njobs - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (jobs[mid].t0 <= b0) lo = mid;
+                else hi = mid - 1;
+            }
+            js = lo;
+        }
+        __syncthreads();
+        const long long t = b0 + threadIdx.x;
+        int j = js;
+        __syncthreads();
+        if (t < total) {
+            if (j + 1 < njobs && t >= jobs[j + 1].t0) ++j;
+            const GeomJob &J = jobs[j];
+            geom_point(J.G64, J.G32, J.tx, J.ty, J.cp, J.qw, J.kappa, J.g, J.err, t - J.t0);
+        }
     }
 }
 
@@ -288,10 +344,25 @@ void PlanArena::stage(void *dst, const void *src, size_t bytes)
     if (shadow) std::memcpy(shadow, src, bytes);   // disjoint ranges: no lock needed
 }
 
-void PlanArena::defer_launch(std::function<void()> f)
+static bool same_grid(const StripGrid &a, const StripGrid &b)
+{
+    return a.m == b.m && a.n == b.n && a.nex == b.nex && a.ney == b.ney && a.TY == b.TY && a.NSX == b.NSX &&
+           a.NSY == b.NSY && a.P == b.P;
+}
+
+void PlanArena::defer_geom(const GeomJob &j)
 {
     std::lock_guard<std::mutex> lock(mu);
-    pending.push_back(std::move(f));
+    for (size_t k = geom.size(); k-- > 0;) {   // the plan's other precision, added just before by the same thread
+        GeomJob &o = geom[k];
+        if (o.cp == j.cp && o.tx == j.tx && o.kappa == j.kappa && same_grid(o.g, j.g) && !(o.G64 && j.G64) &&
+            !(o.G32 && j.G32)) {
+            if (j.G64) o.G64 = j.G64;
+            if (j.G32) o.G32 = j.G32;
+            return;
+        }
+    }
+    geom.push_back(j);
 }
 
 cudaError_t PlanArena::flush()
@@ -302,9 +373,28 @@ cudaError_t PlanArena::flush()
         const cudaError_t e = cudaMemcpy(dchunks[k].first, shadows[k].get(), n, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return e;
     }
+    // the host shadows are released by a thread of their own (unmapping a few
+    // hundred MB takes milliseconds the caller need not wait for)
+    std::thread([sh = std::move(shadows)]() mutable { sh.clear(); }).detach();
     shadows.clear();
-    for (auto &f : pending) f();
-    pending.clear();
+    if (!geom.empty()) {
+        long long t = 0;
+        for (GeomJob &j : geom) {
+            j.t0 = t;
+            t += geom_points(j.g);
+        }
+        GeomJob *dj = nullptr;
+        cudaError_t e = alloc((void **)&dj, geom.size() * sizeof(GeomJob));
+        if (e == cudaSuccess) e = cudaMemcpy(dj, geom.data(), geom.size() * sizeof(GeomJob), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+        int nsm = 148, dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            nsm = 148;
+        const long long blocks = std::min<long long>((t + 255) / 256, 8LL * nsm);
+        geom_jobs_kernel<<<(unsigned)blocks, 256>>>(dj, (int)geom.size(), t);
+        geom.clear();
+    }
     return cudaGetLastError();
 }
 
@@ -324,7 +414,7 @@ void PlanArena::release()
     chunks.clear();
     dchunks.clear();
     shadows.clear();
-    pending.clear();
+    geom.clear();
     used = dused = 0;
 }
 
@@ -480,10 +570,17 @@ static int build_operator(iga_plan *pl, OperatorData &op, const Patch &P, const 
         op.geom_bytes = gelems * sizeof(T);
         if ((st = upload((T **)&op.G, nullptr, op.geom_bytes))) return st;
         if (pl->arena && pl->arena->defer) {   // after the arena's flush has sent the tables
-            T *G = (T *)op.G;
-            const double *tx = pl->tabX64, *ty = pl->tabY64, *cp = pl->CP, *qw = pl->qw, *kp = pl->kappa_dev;
-            int *err = pl->d_err;
-            pl->arena->defer_launch([=]() { geom_setup_kernel<T><<<1184, 256>>>(G, tx, ty, cp, qw, kp, g, err); });
+            GeomJob j;
+            if (sizeof(T) == 8) j.G64 = (double *)op.G;
+            else j.G32 = (float *)op.G;
+            j.tx = pl->tabX64;
+            j.ty = pl->tabY64;
+            j.cp = pl->CP;
+            j.qw = pl->qw;
+            j.kappa = pl->kappa_dev;
+            j.g = g;
+            j.err = pl->d_err;
+            pl->arena->defer_geom(j);
             op.ready = true;
             return IGA_OK;
         }
@@ -707,10 +804,10 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     if (opts.geometry != IGA_GEOM_PRECOMPUTED && opts.geometry != IGA_GEOM_ON_THE_FLY) return IGA_ERR_ARG;
     if (opts.sign != IGA_SIGN_REFERENCE && opts.sign != IGA_SIGN_SPD) return IGA_ERR_ARG;
     if (opts.bc != IGA_BC_REFERENCE && opts.bc != IGA_BC_IDENTITY && opts.bc != IGA_BC_NONE) return IGA_ERR_ARG;
-    Patch P;
+    Patch Pb;
     MeshDescView v{d->p, d->q, d->nElemX, d->nElemY, d->CP, d->weights, d->C1, d->C2, d->IEN, d->ID, d->Dir,
                    d->nDir, d->kappa};
-    std::string err = build_patch(v, P);
+    std::string err = build_patch(v, Pb);
     if (!err.empty()) {
         set_error(err);
         return (err.find("requires") != std::string::npos || err.find("must be in") != std::string::npos)
@@ -722,6 +819,8 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, opts.device);
 
     iga_plan *pl = new iga_plan();
+    pl->patch = std::move(Pb);   // the plan keeps the patch; no copy of its control points
+    const Patch &P = pl->patch;
     pl->p = P.p;
     pl->nex = P.nex;
     pl->ney = P.ney;
@@ -734,7 +833,6 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     pl->bc = opts.bc;
     pl->device = opts.device;
     pl->arena = plan_arena();
-    pl->patch = P;
     // Rows per strip, per operator: a MIXED plan's FP64 and FP32 operators
     // have their own G layouts, so each gets the strip height that fills the
     // SMs best with its own warps per CTA (or the caller's rows_per_strip).

@@ -32,6 +32,18 @@ struct OperatorData {
 
 struct SolverState;   // defined by the solver translation unit
 
+// One plan's precomputed-geometry set-up inside a batch's single launch:
+// G in FP64 and / or FP32 (null: not wanted) on strip grid g from the plan's
+// FP64 tables and control points; t0 = the job's first point in the launch.
+struct GeomJob {
+    double *G64 = nullptr;
+    float *G32 = nullptr;
+    const double *tx = nullptr, *ty = nullptr, *cp = nullptr, *qw = nullptr, *kappa = nullptr;
+    StripGrid g;
+    int *err = nullptr;
+    long long t0 = 0;
+};
+
 // Device memory of many plans carved out of a few large allocations. A batch
 // creates hundreds of small plans; with one cudaMalloc per table and a device
 // synchronisation per plan their set-up cost far more than the solves.
@@ -48,17 +60,19 @@ struct PlanArena {
     // Deferred mode (defer = true): buffers with host data come from a data
     // region whose chunks have host shadows; upload() copies into the shadow
     // and flush() sends each chunk's used bytes in one copy, then runs the
-    // kernel launches the plans deferred (their geometry set-up), in order.
+    // plans' geometry set-up (one launch over all of them).
     // Building many plans then makes no synchronising copy per buffer.
     bool defer = false;
     mutable std::mutex mu;   // plans may be built by several host threads at once
     std::vector<std::pair<char *, size_t>> dchunks;
     std::vector<std::unique_ptr<char[]>> shadows;
     size_t dused = 0;
-    std::vector<std::function<void()>> pending;
+    // deferred geometry set-up: one job per plan (a MIXED plan's two
+    // precisions on the same strips share one), all run by one launch in flush()
+    std::vector<GeomJob> geom;
     cudaError_t alloc_data(void **p, size_t bytes);
     void stage(void *dst, const void *src, size_t bytes);
-    void defer_launch(std::function<void()> f);
+    void defer_geom(const GeomJob &j);
     cudaError_t flush();
 };
 PlanArena *&plan_arena();
