@@ -309,39 +309,97 @@ cudaError_t PlanArena::alloc(void **p, size_t bytes)
     return cudaSuccess;
 }
 
+static size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// The last chunk takes no more allocations; once its bytes are all written
+// the copy thread (started with the first sealed chunk) sends it.
+void PlanArena::seal_last(bool start_copier)
+{
+    if (dchunks.empty() || dchunks.back()->sealed) return;
+    dchunks.back()->sealed = true;
+    if (start_copier && !copier.joinable()) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        copier = std::thread(&PlanArena::copy_loop, this, dev);
+    }
+    cv.notify_all();
+}
+
+void PlanArena::copy_loop(int device)
+{
+    cudaSetDevice(device);
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+        DataChunk *ready = nullptr;
+        for (auto &c : dchunks)
+            if (c->sealed && !c->taken && c->staged == c->used) {
+                ready = c.get();
+                break;
+            }
+        if (ready) {
+            ready->taken = true;
+            lk.unlock();
+            const cudaError_t e =
+                ready->used ? cudaMemcpy(ready->dev, ready->host.get(), ready->used, cudaMemcpyHostToDevice) : cudaSuccess;
+            ready->host.reset();   // a copy from pageable memory has finished reading it on return
+            lk.lock();
+            if (e != cudaSuccess && copy_err == cudaSuccess) copy_err = e;
+            continue;
+        }
+        if (copier_stop) break;
+        cv.wait(lk);
+    }
+}
+
+void PlanArena::stop_copier()
+{
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        copier_stop = true;
+        cv.notify_all();
+    }
+    if (copier.joinable()) copier.join();
+    copier_stop = false;
+}
+
 cudaError_t PlanArena::alloc_data(void **p, size_t bytes)
 {
     std::lock_guard<std::mutex> lock(mu);
-    constexpr size_t kChunk = size_t(128) << 20;
-    bytes = (bytes + 255) & ~size_t(255);
-    if (dchunks.empty() || dused + bytes > dchunks.back().second) {
-        const size_t sz = std::max(kChunk, bytes);
-        char *c = nullptr;
-        const cudaError_t e = cudaMalloc((void **)&c, sz);
+    constexpr size_t kChunk = size_t(16) << 20;
+    bytes = round256(bytes);
+    if (dchunks.empty() || dchunks.back()->used + bytes > dchunks.back()->size) {
+        seal_last(true);
+        auto c = std::make_unique<DataChunk>();
+        c->size = std::max(kChunk, bytes);
+        const cudaError_t e = cudaMalloc((void **)&c->dev, c->size);
         if (e != cudaSuccess) return e;
-        dchunks.emplace_back(c, sz);
-        shadows.emplace_back(new char[sz]);   // uninitialised: only written bytes are touched
-        dused = 0;
+        c->host.reset(new char[c->size]);   // uninitialised: only written bytes are touched
+        dchunks.push_back(std::move(c));
     }
-    *p = dchunks.back().first + dused;
-    dused += bytes;
+    DataChunk &c = *dchunks.back();
+    *p = c.dev + c.used;
+    c.used += bytes;
     return cudaSuccess;
 }
 
 void PlanArena::stage(void *dst, const void *src, size_t bytes)
 {
-    char *shadow = nullptr;
+    DataChunk *c = nullptr;
     {
         std::lock_guard<std::mutex> lock(mu);
         for (size_t k = dchunks.size(); k-- > 0;) {
-            char *base = dchunks[k].first;
-            if ((char *)dst >= base && (char *)dst < base + dchunks[k].second) {
-                shadow = shadows[k].get() + ((char *)dst - base);
+            DataChunk *d = dchunks[k].get();
+            if ((char *)dst >= d->dev && (char *)dst < d->dev + d->size) {
+                c = d;
                 break;
             }
         }
     }
-    if (shadow) std::memcpy(shadow, src, bytes);   // disjoint ranges: no lock needed
+    if (!c) return;
+    std::memcpy(c->host.get() + ((char *)dst - c->dev), src, bytes);   // disjoint ranges: no lock needed
+    std::lock_guard<std::mutex> lock(mu);
+    c->staged += round256(bytes);
+    if (c->sealed && c->staged == c->used) cv.notify_all();
 }
 
 static bool same_grid(const StripGrid &a, const StripGrid &b)
@@ -367,16 +425,30 @@ void PlanArena::defer_geom(const GeomJob &j)
 
 cudaError_t PlanArena::flush()
 {
-    for (size_t k = 0; k < dchunks.size(); ++k) {
-        const size_t n = k + 1 == dchunks.size() ? dused : dchunks[k].second;
-        if (n == 0) continue;
-        const cudaError_t e = cudaMemcpy(dchunks[k].first, shadows[k].get(), n, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) return e;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        seal_last(false);
     }
-    // the host shadows are released by a thread of their own (unmapping a few
-    // hundred MB takes milliseconds the caller need not wait for)
-    std::thread([sh = std::move(shadows)]() mutable { sh.clear(); }).detach();
-    shadows.clear();
+    stop_copier();   // it sends every complete chunk before it stops
+    for (auto &c : dchunks)   // chunks no copy thread took (a single one, or none started)
+        if (!c->taken) {
+            c->taken = true;
+            const cudaError_t e = c->used ? cudaMemcpy(c->dev, c->host.get(), c->used, cudaMemcpyHostToDevice) : cudaSuccess;
+            if (e != cudaSuccess && copy_err == cudaSuccess) copy_err = e;
+        }
+    if (copy_err != cudaSuccess) {
+        const cudaError_t e = copy_err;
+        copy_err = cudaSuccess;
+        return e;
+    }
+    // the remaining host shadows are released by a thread of their own
+    // (unmapping them takes milliseconds the caller need not wait for)
+    {
+        std::vector<std::unique_ptr<char[]>> sh;
+        for (auto &c : dchunks)
+            if (c->host) sh.push_back(std::move(c->host));
+        if (!sh.empty()) std::thread([sh = std::move(sh)]() mutable { sh.clear(); }).detach();
+    }
     if (!geom.empty()) {
         long long t = 0;
         for (GeomJob &j : geom) {
@@ -401,21 +473,22 @@ cudaError_t PlanArena::flush()
 bool PlanArena::owns(const void *p) const
 {
     std::lock_guard<std::mutex> lock(mu);
-    for (const auto *list : {&chunks, &dchunks})
-        for (const auto &c : *list)
-            if (p >= (const void *)c.first && p < (const void *)(c.first + c.second)) return true;
+    for (const auto &c : chunks)
+        if (p >= (const void *)c.first && p < (const void *)(c.first + c.second)) return true;
+    for (const auto &c : dchunks)
+        if (p >= (const void *)c->dev && p < (const void *)(c->dev + c->size)) return true;
     return false;
 }
 
 void PlanArena::release()
 {
+    stop_copier();
     for (auto &c : chunks) cudaFree(c.first);
-    for (auto &c : dchunks) cudaFree(c.first);
+    for (auto &c : dchunks) cudaFree(c->dev);
     chunks.clear();
     dchunks.clear();
-    shadows.clear();
     geom.clear();
-    used = dused = 0;
+    used = 0;
 }
 
 template <typename T>

@@ -6,7 +6,9 @@
 #include <utility>
 #include <functional>
 #include <memory>
+#include <condition_variable>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../../include/iga_mf.h"
@@ -58,15 +60,30 @@ struct PlanArena {
     bool owns(const void *p) const;
     void release();
     // Deferred mode (defer = true): buffers with host data come from a data
-    // region whose chunks have host shadows; upload() copies into the shadow
-    // and flush() sends each chunk's used bytes in one copy, then runs the
-    // plans' geometry set-up (one launch over all of them).
-    // Building many plans then makes no synchronising copy per buffer.
+    // region of chunks with host shadows; upload() copies into the shadow.
+    // A chunk that is full and completely written is sent to the device by a
+    // copy thread while the plans are still being built (a copy from pageable
+    // memory runs at about 11 GB/s however many threads issue it, so it is
+    // overlapped with the plans' host work rather than split); flush() sends
+    // the rest, then runs the plans' geometry set-up (one launch over all of
+    // them). Building many plans then makes no synchronising copy per buffer.
     bool defer = false;
     mutable std::mutex mu;   // plans may be built by several host threads at once
-    std::vector<std::pair<char *, size_t>> dchunks;
-    std::vector<std::unique_ptr<char[]>> shadows;
-    size_t dused = 0;
+    struct DataChunk {
+        char *dev = nullptr;
+        std::unique_ptr<char[]> host;   // the shadow
+        size_t size = 0, used = 0, staged = 0;   // bytes allocated / written into the shadow
+        bool sealed = false;            // no further allocations
+        bool taken = false;             // copied (or being copied)
+    };
+    std::vector<std::unique_ptr<DataChunk>> dchunks;
+    std::condition_variable cv;
+    std::thread copier;
+    bool copier_stop = false;
+    cudaError_t copy_err = cudaSuccess;
+    void seal_last(bool start_copier);   // with mu held
+    void copy_loop(int device);
+    void stop_copier();
     // deferred geometry set-up: one job per plan (a MIXED plan's two
     // precisions on the same strips share one), all run by one launch in flush()
     std::vector<GeomJob> geom;
