@@ -133,13 +133,54 @@ __host__ __device__ constexpr bool apply_txshared()
     return !apply_txreg<P, T, GEOM>() && !(GEOM == 1 && P == 4);
 }
 
+// The FP64 on-the-fly kernel at p = 5 (255 registers, spilling) keeps one
+// CTA per column strip: dealt from the flat grid its spills grew (608 ->
+// 880 B a thread) and it ran 187 -> 255 us at 512^2.
+template <int P, typename T, int GEOM>
+__host__ __device__ constexpr bool apply_percolumn()
+{
+    return apply_txshared<P, T, GEOM>() && GEOM == 1 && P == 5;
+}
+
+// Shared memory of a CTA of W warps: barriers, then each warp's G ring, x
+// (and control-point) rows and y-table rows, then (apply_txshared) ntab
+// slots of column-strip x tables, 128-byte aligned.
 template <int P, typename T, int GEOM, int NST>
-__host__ __device__ constexpr size_t apply_smem_bytes(int W)
+__host__ __device__ constexpr size_t apply_tab_offset(int W)
 {
     using S = ApplyShape<P, T>;
-    return 256 + (size_t)W * NST * 8 + (apply_txshared<P, T, GEOM>() ? S::TABX * sizeof(T) : 0) + 128 +
-           (GEOM == 0 ? (size_t)W * NST * S::GBYTES : 0) +
-           (size_t)W * S::XR * S::XW * sizeof(T) * (GEOM == 1 ? 3 : 1) + (size_t)W * S::XR * S::TYW * sizeof(T);
+    return (((256 + (size_t)W * NST * 8 + 127) & ~size_t(127)) + (GEOM == 0 ? (size_t)W * NST * S::GBYTES : 0) +
+            (size_t)W * S::XR * S::XW * sizeof(T) * (GEOM == 1 ? 3 : 1) + (size_t)W * S::XR * S::TYW * sizeof(T) +
+            127) &
+           ~size_t(127);
+}
+
+template <int P, typename T, int GEOM, int NST>
+__host__ __device__ constexpr size_t apply_smem_bytes(int W, int ntab = 1)
+{
+    return apply_tab_offset<P, T, GEOM, NST>(W) +
+           (apply_txshared<P, T, GEOM>() ? (size_t)ntab * ApplyShape<P, T>::TABX * sizeof(T) : 0);
+}
+
+// The CTA's x-table slots in shared memory (apply_txshared kernels).
+template <int P, typename T, int GEOM, int NST>
+__device__ __forceinline__ T *apply_tab_slots()
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    return reinterpret_cast<T *>(smem + apply_tab_offset<P, T, GEOM, NST>(blockDim.y));
+}
+
+// Copies the x tables of column strips gx0 .. gx0 + n - 1 into the slots (all
+// threads of the CTA; the caller synchronises).
+template <int P, typename T, int GEOM, int NST>
+__device__ __forceinline__ void apply_load_tabs(const T *__restrict__ tabX, int gx0, int n, T *slots)
+{
+    constexpr int TABX = ApplyShape<P, T>::TABX;
+    const int t = threadIdx.y * 32 + threadIdx.x, nt = 32 * blockDim.y;
+    for (int k = 0; k < n; ++k) {
+        const T *src = tabX + (size_t)(gx0 + k) * TABX;
+        for (int i = t; i < TABX; i += nt) slots[(size_t)k * TABX + i] = src[i];
+    }
 }
 
 template <typename T>
@@ -183,11 +224,11 @@ __host__ __device__ constexpr int apply_max_threads()
                           : (P <= 2 ? (GEOM ? 384 : 512) : P == 3 ? (GEOM ? 256 : 384) : 256);
 }
 
-// One warp: strip (gx, gy). With tables in shared memory the CTA's warps
-// share the column strip gx (the CTA copies its tables once).
+// One warp: strip (gx, gy). tab_slot: the slot of the CTA's shared memory
+// holding the column strip's x tables (apply_txshared), loaded by the caller.
 template <int P, typename T, int GEOM, int NST>
 __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__restrict__ x, T *__restrict__ y, const int gx,
-                                           const int gy)
+                                           const int gy, const int tab_slot)
 {
     using S = ApplyShape<P, T>;
     constexpr int NB = S::NB, NQ = S::NQ, QH = S::QH;
@@ -200,9 +241,6 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     size_t off = 256 + (size_t)W * NST * 8;
     off = (off + 127) & ~size_t(127);
-    T *tabXs = reinterpret_cast<T *>(smem + off);
-    if (apply_txshared<P, T, GEOM>()) off += S::TABX * sizeof(T);
-    off = (off + 127) & ~size_t(127);
     T *Gs = reinterpret_cast<T *>(smem + off) + (size_t)w * NST * S::GE;
     if (GEOM == 0) off += (size_t)W * NST * S::GBYTES;
     T *xr = reinterpret_cast<T *>(smem + off) + (size_t)w * S::XR * S::XW;
@@ -211,12 +249,9 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     if (GEOM == 1) off += (size_t)W * S::XR * S::XW * 2 * sizeof(T);
     T *yr = reinterpret_cast<T *>(smem + off) + (size_t)w * S::XR * S::TYW;     // y tables of upcoming rows
     uint64_t *wbar = bars + w * NST;
+    // (addressed from the shared array itself, so that the compiler emits shared loads)
+    const T *tabXs = reinterpret_cast<const T *>(smem + apply_tab_offset<P, T, GEOM, NST>(W)) + (size_t)tab_slot * S::TABX;
 
-    if constexpr (apply_txshared<P, T, GEOM>()) {   // x tables of this column strip, shared by the CTA's warps
-        const T *src = a.tabX + (size_t)gx * S::TABX;
-        for (int i = threadIdx.y * 32 + lane; i < S::TABX; i += 32 * W) tabXs[i] = src[i];
-        __syncthreads();
-    }
     if (gx >= g.NSX || gy >= g.NSY) return;
     const int ex0 = kSW * gx, ey0 = g.TY * gy;
     const int nsteps = min(g.TY, g.ney - ey0);
@@ -704,24 +739,37 @@ __device__ __forceinline__ void apply_tile(const ApplyParams<T> &a, const T *__r
     cp_async_wait<0>();
 }
 
-// Strips to warps: with tables in registers any warp takes any strip, warp
-// k of the 1-D grid strip k in column-major order (gx outer), so the grid
-// covers NSX * NSY strips with no partly idle CTAs; with shared tables the
-// CTA is one column strip gx = blockIdx.x and its warps take consecutive
-// strips of it.
+// Strips to warps: warp k of the 1-D grid takes strip k in column-major
+// order (gx outer), so the grid covers NSX * rows strips with no partly idle
+// CTAs and the strip height can make the strip count fill the SMs. With the
+// tables in shared memory (apply_txshared) the CTA copies the tables of the
+// column strips its warps' strips lie in: two slots, as the launch keeps W - 1
+// <= rows. (One CTA per column strip, W strips of it each, left 20 of 148
+// SMs idle for the FP64 p=4 operator on a 1024-wide patch: 64 columns.)
 template <int P, typename T, int GEOM, int NST>
 __global__ void __launch_bounds__(apply_max_threads<P, T, GEOM>(), 1) apply_kernel(ApplyParams<T> a)
 {
     pdl_launch();   // apply_tile waits for the preceding grid once its constant operands are in flight
     const int rows = min(a.gyn, a.g.NSY - a.gy0);   // strip rows of the window
-    if constexpr (!apply_txshared<P, T, GEOM>()) {
-        const int sid = blockIdx.x * blockDim.y + threadIdx.y;
-        const int gx = sid / rows;
-        apply_tile<P, T, GEOM, NST>(a, a.x, a.y, gx, a.gy0 + (sid - gx * rows));
-    } else {
+    if constexpr (apply_percolumn<P, T, GEOM>()) {   // CTA = W strips of column strip blockIdx.x
+        apply_load_tabs<P, T, GEOM, NST>(a.tabX, blockIdx.x, 1, apply_tab_slots<P, T, GEOM, NST>());
+        __syncthreads();
         const int r = blockIdx.y * blockDim.y + threadIdx.y;
-        apply_tile<P, T, GEOM, NST>(a, a.x, a.y, blockIdx.x, r < rows ? a.gy0 + r : a.g.NSY);
+        apply_tile<P, T, GEOM, NST>(a, a.x, a.y, blockIdx.x, r < rows ? a.gy0 + r : a.g.NSY, 0);
+        return;
     }
+    const int s0 = blockIdx.x * blockDim.y, sid = s0 + threadIdx.y;   // strips: NSX * NSY < 2^31
+    const int gx = sid / rows;
+    int slot = 0;
+    if constexpr (apply_txshared<P, T, GEOM>()) {
+        const int total = a.g.NSX * rows;
+        const int gx_lo = s0 / rows, gx_hi = (min(s0 + (int)blockDim.y, total) - 1) / rows;
+        apply_load_tabs<P, T, GEOM, NST>(a.tabX, gx_lo, gx_hi - gx_lo + 1, apply_tab_slots<P, T, GEOM, NST>());
+        __syncthreads();
+        if (sid >= total) return;
+        slot = gx - gx_lo;
+    }
+    apply_tile<P, T, GEOM, NST>(a, a.x, a.y, gx, a.gy0 + (sid - gx * rows), slot);
 }
 
 // Many independent patches in one launch, with that problem's parameters
@@ -741,7 +789,11 @@ __global__ void __launch_bounds__(apply_max_threads<P, T, 0>(), 1)
     const int4 it = items[flat ? blockIdx.x * blockDim.y + threadIdx.y : blockIdx.x];
     if (it.x < 0 || !active[it.x]) return;   // uniform over the CTA unless flat (no CTA barrier then)
     const long long o = offs[it.x];
-    apply_tile<P, T, 0, NST>(params[it.x], xb + o, yb + o, it.y, flat ? it.z : it.z * blockDim.y + threadIdx.y);
+    if constexpr (!flat) {   // the item's column strip, slot 0
+        apply_load_tabs<P, T, 0, NST>(params[it.x].tabX, it.y, 1, apply_tab_slots<P, T, 0, NST>());
+        __syncthreads();
+    }
+    apply_tile<P, T, 0, NST>(params[it.x], xb + o, yb + o, it.y, flat ? it.z : it.z * blockDim.y + threadIdx.y, 0);
 }
 
 // Sums the frames of the strips covering each seam control point, strip

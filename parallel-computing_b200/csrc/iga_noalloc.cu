@@ -140,13 +140,13 @@ int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int 
 {
     using namespace iga;
     int W = apply_max_threads<P, double, 1>() / 32;
-    while (W > 1 && apply_smem_bytes<P, double, 1, 2>(W) > 220 * 1024) --W;
-    const size_t smem = apply_smem_bytes<P, double, 1, 2>(W);
+    while (W > 1 && apply_smem_bytes<P, double, 1, 2>(W, 2) > 220 * 1024) --W;
+    const size_t smem_max = apply_smem_bytes<P, double, 1, 2>(W, 2);
     auto kern = apply_kernel<P, double, 1, 2>;
     {
         std::lock_guard<std::mutex> lk(g_mu);
         if (!g_attr[dev][P]) {
-            const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
             if (e != cudaSuccess) {
                 set_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
                 return IGA_ERR_CUDA;
@@ -180,12 +180,14 @@ int launch(int dev, unsigned char *base, const Layout &Ly, int TY, int nex, int 
     a.bc = d_ID ? IGA_BC_NONE : IGA_BC_REFERENCE;
     a.ID = d_ID;
     a.err = reinterpret_cast<int *>(base + Ly.off_err);
-    // strips dealt to warps one by one; with shared tables a CTA per W strips of a column
+    // strips dealt to warps one by one; with shared tables the CTA's strips
+    // lie in at most two column strips (W - 1 <= NSY)
+    constexpr bool percol = apply_percolumn<P, double, 1>();
+    if (apply_txshared<P, double, 1>() && !percol) W = std::max(1, std::min(W, g.NSY + 1));
     const long long nstrips = (long long)g.NSX * g.NSY;
-    const dim3 grid = !apply_txshared<P, double, 1>() ? dim3((unsigned)((nstrips + W - 1) / W))
-                                                  : dim3(g.NSX, (g.NSY + W - 1) / W),
+    const dim3 grid = percol ? dim3(g.NSX, (g.NSY + W - 1) / W) : dim3((unsigned)((nstrips + W - 1) / W)),
                block(32, W);
-    kern<<<grid, block, smem, s>>>(a);
+    kern<<<grid, block, apply_smem_bytes<P, double, 1, 2>(W, !percol && g.NSY % W ? 2 : 1), s>>>(a);
     cudaError_t e = cudaPeekAtLastError();
     const long long nseam = (long long)(g.NSX - 1) * P * g.n + (long long)(g.NSY - 1) * P * g.m;
     if (e == cudaSuccess && nseam > 0) {

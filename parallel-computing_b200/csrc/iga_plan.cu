@@ -520,7 +520,7 @@ static int warps_for_t()
 {
     constexpr int NST = apply_stages<P, T>();
     for (int W = apply_max_threads<P, T, GEOM>() / 32; W >= 1; --W)
-        if (apply_smem_bytes<P, T, GEOM, NST>(W) <= kSmemBudget) return W;
+        if (apply_smem_bytes<P, T, GEOM, NST>(W, 2) <= kSmemBudget) return W;
     return 1;
 }
 
@@ -582,10 +582,10 @@ static int rows_for(int nex, int ney, const std::vector<WarpShape> &Ws, int nsm)
     return best;
 }
 
-static bool apply_flat(int P, int prec, int geom)
-{
-    return prec == IGA_FP32 || (geom == IGA_GEOM_PRECOMPUTED ? P <= 3 : (P == 3 || P == 4));
-}
+// The single-plan kernel deals strips to warps one by one in every
+// configuration (shared x tables included) but the FP64 on-the-fly p = 5
+// one (apply_percolumn).
+static bool apply_flat(int P, int prec, int geom) { return !(P == 5 && prec == IGA_FP64 && geom == IGA_GEOM_ON_THE_FLY); }
 
 }  // namespace iga
 
@@ -698,22 +698,28 @@ static int launch_apply_t(iga_plan *pl, const OperatorData &op, const T *x, T *y
     a.err = pl->d_err;
     a.ID = win.ID;
     if (pl->wait_polls >= 0) a.wait_polls = pl->wait_polls;
-    const int W = op.warps;
-    const size_t smem = apply_smem_bytes<P, T, GEOM, NST>(W);
     auto kern = apply_kernel<P, T, GEOM, NST>;
-    static bool attr_set = false;   // per template instance
+    static bool attr_set = false;   // per template instance: the most any launch below asks for
     if (!attr_set) {
-        IGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        IGA_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)apply_smem_bytes<P, T, GEOM, NST>(op.warps, 2)));
         attr_set = true;
     }
     const StripGrid &g = op.grid;
     const int rows = win.gyn >= 0 ? std::min(win.gyn, g.NSY - win.gy0) : g.NSY;
+    // shared x tables: a CTA's strips lie in at most two column strips when
+    // W - 1 <= rows, in one when W divides rows (one slot: the shared memory
+    // of the one-column layout, which matters where a kernel's spills live
+    // in L1: FP64 on-the-fly p=5 512^2 189 -> 257 us with a second slot)
+    constexpr bool percol = apply_percolumn<P, T, GEOM>();
+    const int W = apply_txshared<P, T, GEOM>() && !percol ? std::max(1, std::min(op.warps, rows + 1)) : op.warps;
+    const size_t smem = apply_smem_bytes<P, T, GEOM, NST>(W, !percol && rows % W ? 2 : 1);
     if (win.gyn >= 0) {
         a.gy0 = win.gy0;
         a.gyn = rows;
     }
     const long long nstrips = (long long)g.NSX * rows;
-    dim3 grid = !apply_txshared<P, T, GEOM>() ? dim3((unsigned)((nstrips + W - 1) / W)) : dim3(g.NSX, (rows + W - 1) / W);
+    const dim3 grid = percol ? dim3(g.NSX, (rows + W - 1) / W) : dim3((unsigned)((nstrips + W - 1) / W));
     dim3 block(32, W);
     if (rows > 0) IGA_CUDA_TRY(launch_k(kern, grid, block, smem, s, a));
     if (win.gyn < 0) {
