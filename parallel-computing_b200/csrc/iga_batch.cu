@@ -1718,7 +1718,9 @@ int create_batch(const iga_mesh_desc *meshes, int count, int precision, int devi
     std::vector<int> status(count, IGA_OK);
     std::vector<std::string> message(count);
     {
-        const unsigned nthr = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), 16u));
+        // host threads building plans: one core is left to the arena's copy thread
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const unsigned nthr = hw > 2 ? std::min(hw - 1, 16u) : 1u;
         std::atomic<int> next{0};
         auto work = [&]() {
             cudaSetDevice(device);

@@ -371,8 +371,16 @@ cudaError_t PlanArena::alloc_data(void **p, size_t bytes)
         seal_last(true);
         auto c = std::make_unique<DataChunk>();
         c->size = std::max(kChunk, bytes);
-        const cudaError_t e = cudaMalloc((void **)&c->dev, c->size);
-        if (e != cudaSuccess) return e;
+        if (dblocks.empty() || dblock_used + c->size > dblocks.back().second) {   // device memory in 128 MB blocks
+            const size_t sz = std::max(size_t(128) << 20, c->size);
+            char *b = nullptr;
+            const cudaError_t e = cudaMalloc((void **)&b, sz);
+            if (e != cudaSuccess) return e;
+            dblocks.emplace_back(b, sz);
+            dblock_used = 0;
+        }
+        c->dev = dblocks.back().first + dblock_used;
+        dblock_used += c->size;
         c->host.reset(new char[c->size]);   // uninitialised: only written bytes are touched
         dchunks.push_back(std::move(c));
     }
@@ -475,8 +483,8 @@ bool PlanArena::owns(const void *p) const
     std::lock_guard<std::mutex> lock(mu);
     for (const auto &c : chunks)
         if (p >= (const void *)c.first && p < (const void *)(c.first + c.second)) return true;
-    for (const auto &c : dchunks)
-        if (p >= (const void *)c->dev && p < (const void *)(c->dev + c->size)) return true;
+    for (const auto &c : dblocks)
+        if (p >= (const void *)c.first && p < (const void *)(c.first + c.second)) return true;
     return false;
 }
 
@@ -484,9 +492,11 @@ void PlanArena::release()
 {
     stop_copier();
     for (auto &c : chunks) cudaFree(c.first);
-    for (auto &c : dchunks) cudaFree(c->dev);
+    for (auto &c : dblocks) cudaFree(c.first);
     chunks.clear();
     dchunks.clear();
+    dblocks.clear();
+    dblock_used = 0;
     geom.clear();
     used = 0;
 }

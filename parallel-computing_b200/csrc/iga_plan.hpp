@@ -77,6 +77,8 @@ struct PlanArena {
         bool taken = false;             // copied (or being copied)
     };
     std::vector<std::unique_ptr<DataChunk>> dchunks;
+    std::vector<std::pair<char *, size_t>> dblocks;   // the device memory the chunks are carved from
+    size_t dblock_used = 0;
     std::condition_variable cv;
     std::thread copier;
     bool copier_stop = false;
