@@ -1915,6 +1915,7 @@ int iga_batch_destroy(iga_batch *B)
 {
     if (!B) return IGA_OK;
     cudaSetDevice(B->device);
+    B->arena.stop_copier();   // its queued copies read the plans' control points
     cudaDeviceSynchronize();
     if (B->graph) cudaGraphExecDestroy(B->graph);
     for (iga_plan *pl : B->plans) iga_plan_destroy(pl);

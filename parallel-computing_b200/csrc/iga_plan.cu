@@ -325,6 +325,27 @@ void PlanArena::seal_last(bool start_copier)
     cv.notify_all();
 }
 
+void PlanArena::drop_copies(const void *lo, const void *hi)
+{
+    std::unique_lock<std::mutex> lk(mu);
+    auto inside = [&](const void *p) { return p >= lo && p < hi; };
+    direct.erase(std::remove_if(direct.begin(), direct.end(), [&](const DirectCopy &d) { return inside(d.src); }),
+                 direct.end());
+    cv.wait(lk, [&] { return !copying || !inside(copying); });
+}
+
+void PlanArena::defer_copy(void *dst, const void *src, size_t bytes)
+{
+    std::lock_guard<std::mutex> lock(mu);
+    direct.push_back(DirectCopy{dst, src, bytes});
+    if (!copier.joinable()) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        copier = std::thread(&PlanArena::copy_loop, this, dev);
+    }
+    cv.notify_all();
+}
+
 void PlanArena::copy_loop(int device)
 {
     cudaSetDevice(device);
@@ -343,6 +364,18 @@ void PlanArena::copy_loop(int device)
                 ready->used ? cudaMemcpy(ready->dev, ready->host.get(), ready->used, cudaMemcpyHostToDevice) : cudaSuccess;
             ready->host.reset();   // a copy from pageable memory has finished reading it on return
             lk.lock();
+            if (e != cudaSuccess && copy_err == cudaSuccess) copy_err = e;
+            continue;
+        }
+        if (!direct.empty()) {
+            const DirectCopy d = direct.back();
+            direct.pop_back();
+            copying = d.src;
+            lk.unlock();
+            const cudaError_t e = cudaMemcpy(d.dst, d.src, d.bytes, cudaMemcpyHostToDevice);
+            lk.lock();
+            copying = nullptr;
+            cv.notify_all();
             if (e != cudaSuccess && copy_err == cudaSuccess) copy_err = e;
             continue;
         }
@@ -437,7 +470,7 @@ cudaError_t PlanArena::flush()
         std::lock_guard<std::mutex> lock(mu);
         seal_last(false);
     }
-    stop_copier();   // it sends every complete chunk before it stops
+    stop_copier();   // it sends every complete chunk and queued copy before it stops
     for (auto &c : dchunks)   // chunks no copy thread took (a single one, or none started)
         if (!c->taken) {
             c->taken = true;
@@ -491,6 +524,7 @@ bool PlanArena::owns(const void *p) const
 void PlanArena::release()
 {
     stop_copier();
+    direct.clear();
     for (auto &c : chunks) cudaFree(c.first);
     for (auto &c : dblocks) cudaFree(c.first);
     chunks.clear();
@@ -514,6 +548,20 @@ static int upload(T **dst, const void *src, size_t bytes)
     else IGA_CUDA_TRY(cudaMalloc((void **)dst, std::max<size_t>(bytes, 16)));
     if (src && bytes) IGA_CUDA_TRY(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
     return IGA_OK;
+}
+
+// Like upload() for host data that lives as long as the plan (its patch):
+// in deferred mode the arena's copy thread copies it straight from there.
+template <typename T>
+static int upload_persistent(T **dst, const void *src, size_t bytes)
+{
+    PlanArena *a = plan_arena();
+    if (a && a->defer && src && bytes) {
+        IGA_CUDA_TRY(a->alloc((void **)dst, bytes));
+        a->defer_copy(*dst, src, bytes);
+        return IGA_OK;
+    }
+    return upload(dst, src, bytes);
 }
 
 // cudaFree unless the buffer belongs to the plan's arena.
@@ -979,7 +1027,7 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
         gauss01(NQ, qx.data(), qw.data());
         if ((st = upload(&pl->tabX64, h64x.data(), h64x.size() * 8))) return fail(st);
         if ((st = upload(&pl->tabY64, h64y.data(), h64y.size() * 8))) return fail(st);
-        if ((st = upload(&pl->CP, P.CP.data(), P.CP.size() * 8))) return fail(st);
+        if ((st = upload_persistent(&pl->CP, P.CP.data(), P.CP.size() * 8))) return fail(st);
         if ((st = upload(&pl->qw, qw.data(), qw.size() * 8))) return fail(st);
         const int zero = 0;
         if (pl->arena && pl->arena->defer) {
@@ -1014,6 +1062,8 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
 int iga_plan_destroy(iga_plan *pl)
 {
     if (!pl) return IGA_OK;
+    if (pl->arena && !pl->patch.CP.empty())   // a copy thread may still read the control points
+        pl->arena->drop_copies(pl->patch.CP.data(), pl->patch.CP.data() + pl->patch.CP.size());
     cudaSetDevice(pl->device);
     cudaDeviceSynchronize();
     free_op(pl, pl->op64);

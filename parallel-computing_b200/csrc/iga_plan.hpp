@@ -83,6 +83,20 @@ struct PlanArena {
     std::thread copier;
     bool copier_stop = false;
     cudaError_t copy_err = cudaSuccess;
+    // Copies from host memory that outlives the flush (a plan's own control
+    // points) into buffers of the plain region, done by the copy thread
+    // without staging: defer_copy() queues one.
+    struct DirectCopy {
+        void *dst;
+        const void *src;
+        size_t bytes;
+    };
+    std::vector<DirectCopy> direct;
+    const void *copying = nullptr;   // source of the direct copy in progress
+    void defer_copy(void *dst, const void *src, size_t bytes);
+    // Forgets the queued copies from [lo, hi) and waits for one in progress
+    // (a plan destroyed before the flush).
+    void drop_copies(const void *lo, const void *hi);
     void seal_last(bool start_copier);   // with mu held
     void copy_loop(int device);
     void stop_copier();
