@@ -100,6 +100,7 @@ struct PlanArena {
     void seal_last(bool start_copier);   // with mu held
     void copy_loop(int device);
     void stop_copier();
+    ~PlanArena() { stop_copier(); }
     // deferred geometry set-up: one job per plan (a MIXED plan's two
     // precisions on the same strips share one), all run by one launch in flush()
     std::vector<GeomJob> geom;
