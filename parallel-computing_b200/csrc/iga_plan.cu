@@ -609,6 +609,13 @@ int warps_for(int P, int prec, int geom)
 struct WarpShape {
     int W;
     bool flat;
+    // also try the strip heights whose CTA count fills whole waves of SMs:
+    // the FP64 precomputed operators at p >= 4, which are held back by each
+    // SM's own progress rather than by HBM (p=4 1024^2: 57 rows, 144 CTAs,
+    // 146.4 -> 140.3 us; p=5: 38 rows, 238 -> 230 us), where the p=3
+    // headline at 82% of HBM gained nothing from it (40 or 50 rows: 312 /
+    // 314 us)
+    bool waves = false;
 };
 
 static double strip_cost(int NSX, int ney, int TY, WarpShape ws, int nsm)
@@ -623,7 +630,15 @@ static double strip_cost(int NSX, int ney, int TY, WarpShape ws, int nsm)
 static int rows_for(int nex, int ney, const std::vector<WarpShape> &Ws, int nsm)
 {
     const int NSX = (nex + kSW - 1) / kSW;
-    static const int cands[] = {64, 56, 48, 40, 32, 28, 24, 20, 16};
+    std::vector<int> cands = {64, 56, 48, 40, 32, 28, 24, 20, 16};
+    for (const WarpShape &ws : Ws)
+        if (ws.waves && ws.flat)
+            for (int k = 1; k <= 16; ++k) {
+                const long long nsy = (long long)k * nsm * ws.W / NSX;   // strip rows of k full waves
+                if (nsy < 1) continue;
+                const int TY = (int)((ney + nsy - 1) / nsy);
+                if (TY >= 16 && TY <= 64 && std::find(cands.begin(), cands.end(), TY) == cands.end()) cands.push_back(TY);
+            }
     std::vector<double> best_w(Ws.size(), 1e300);
     for (size_t k = 0; k < Ws.size(); ++k)
         for (int TY : cands) best_w[k] = std::min(best_w[k], strip_cost(NSX, ney, TY, Ws[k], nsm));
@@ -975,7 +990,8 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     // SMs best with its own warps per CTA (or the caller's rows_per_strip).
     auto rows_of = [&](int prec) {
         if (opts.rows_per_strip > 0) return opts.rows_per_strip;
-        return rows_for(P.nex, P.ney, {{warps_for(P.p, prec, opts.geometry), apply_flat(P.p, prec, opts.geometry)}},
+        return rows_for(P.nex, P.ney, {{warps_for(P.p, prec, opts.geometry), apply_flat(P.p, prec, opts.geometry),
+                                         prec == IGA_FP64 && opts.geometry == IGA_GEOM_PRECOMPUTED && P.p >= 4}},
                         nsm);
     };
     auto make_grid = [&](int TY) {
