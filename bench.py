@@ -385,9 +385,16 @@ def time_batch(ib, torch, stream, barrier, max_over_ranks):
     # FP32 sweep tolerance: 3e-4 needs three sweeps here, like 1e-5, with fewer
     # FP32 iterations per sweep
     for name, prec, kw in (("fp64", ib.FP64, {}), ("fp32_refine", ib.MIXED, {"sweep_rtol": 3e-4})):
-        t0 = time.perf_counter()
-        batch = ib.Batch(meshes, precision=prec, tune_file=ib.TUNE_FILE)
-        setup = time.perf_counter() - t0
+        # set-up is host-bound and the host is shared: the median of three
+        # creations (the samples are reported too)
+        setups = []
+        for rep in range(3):
+            t0 = time.perf_counter()
+            batch = ib.Batch(meshes, precision=prec, tune_file=ib.TUNE_FILE)
+            setups.append(time.perf_counter() - t0)
+            if rep < 2:
+                batch.close()
+        setup = statistics.median(setups)
         x = torch.zeros_like(b)
         batch.solve(b, x, **kw)   # warm-up: graph capture and instantiation
         times, st, its = [], None, None
@@ -401,6 +408,7 @@ def time_batch(ib, torch, stream, barrier, max_over_ranks):
             times.append(max_over_ranks(e0.elapsed_time(e1) / 1e3))
         sec = statistics.median(times)
         out[name] = {"seconds": sec, "solves_per_s": 256 / sec, "setup_seconds": setup,
+                     "setup_seconds_samples": [round(v, 4) for v in setups],
                      "converged": st.converged, "max_iterations": st.max_iterations,
                      "mean_iterations": float(its.mean()), "max_sweeps": st.max_sweeps, "max_relres": st.max_relres,
                      **({"sweep_rtol": kw["sweep_rtol"]} if kw else {})}
