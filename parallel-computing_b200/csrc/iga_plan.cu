@@ -610,11 +610,12 @@ struct WarpShape {
     int W;
     bool flat;
     // also try the strip heights whose CTA count fills whole waves of SMs:
-    // the FP64 precomputed operators at p >= 4, which are held back by each
-    // SM's own progress rather than by HBM (p=4 1024^2: 57 rows, 144 CTAs,
-    // 146.4 -> 140.3 us; p=5: 38 rows, 238 -> 230 us), where the p=3
-    // headline at 82% of HBM gained nothing from it (40 or 50 rows: 312 /
-    // 314 us)
+    // the kernels with shared x tables dealt from a flat grid (FP64
+    // precomputed p >= 4, FP64 on-the-fly p = 1, 2), which are held back by
+    // each SM's own progress rather than by HBM (p=4 1024^2: 57 rows, 144
+    // CTAs, 146.4 -> 140.3 us; p=5: 38 rows, 238 -> 230 us; on-the-fly p=2
+    // 1024^2 105.5 -> 101.4 us, p=1 50.1 -> 48.1 us), where the p=3 headline
+    // at 82% of HBM gained nothing from it (40 or 50 rows: 312 / 314 us)
     bool waves = false;
 };
 
@@ -990,8 +991,9 @@ int iga_plan_create(const iga_mesh_desc *d, const iga_opts *opts_in, iga_plan **
     // SMs best with its own warps per CTA (or the caller's rows_per_strip).
     auto rows_of = [&](int prec) {
         if (opts.rows_per_strip > 0) return opts.rows_per_strip;
+        const bool shared_flat = prec == IGA_FP64 && (opts.geometry == IGA_GEOM_PRECOMPUTED ? P.p >= 4 : P.p <= 2);
         return rows_for(P.nex, P.ney, {{warps_for(P.p, prec, opts.geometry), apply_flat(P.p, prec, opts.geometry),
-                                         prec == IGA_FP64 && opts.geometry == IGA_GEOM_PRECOMPUTED && P.p >= 4}},
+                                         shared_flat}},
                         nsm);
     };
     auto make_grid = [&](int TY) {
